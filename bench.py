@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark of the sinc-DVR orbital right-hand side on B200.
+
+Metric: orbital-RHS evaluations per second.  One evaluation (one "step") is a
+mean-field build -- pair densities, Toeplitz/FFT Coulomb solves, twoematel,
+reducedpot from the 2-RDM tally -- followed by one actreduced00 on the same
+orbitals (MCTDH.SRC/derivs.f90:629-852 with the SINCDVR project operators).
+
+Workload B (default): two Z=1 nuclei at z=+-0.75 bohr, 41^3 grid, spacing 0.25,
+10 orbitals, complex128, seeded synthetic orbitals/tally/density matrices.
+
+  python bench.py [--gpus N --steps K --warmup W]      # this implementation
+  python bench.py --impl reference [...]               # CPU reference restatement
+
+Multi-GPU: independent replicas (the path has no exchange step); value is the
+sum over ranks, timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "v1-1_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "orbital-RHS evals/s"
+UNIT = "evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="B")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_config(w, l2="flushed (256 MiB write between timed steps)"):
+    return {
+        "workload": f"{w.name}: {w.note}, {w.numpoints}^3 grid, spacing {w.spacing}, "
+                    f"{w.nspf} orbitals, nuclei Z={list(w.nuccharges)} at centershift {list(map(list, w.centershift))}",
+        "numpoints": w.numpoints, "nspf": w.nspf, "pairs": w.nspf * (w.nspf + 1) // 2,
+        "l2": l2, "parallelism": "replicas",
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (oracle restatement), used for --impl reference and cpu_baseline
+# ---------------------------------------------------------------------------
+def cpu_reference_eval(w, threads):
+    """One orbital-RHS evaluation with the CPU restatement of the reference.
+    Returns (seconds, description)."""
+    sys.path.insert(0, str(REPO))
+    from oracle import sinc_oracle as orc
+    from sincgpu import inputs as inp
+    sysm = orc.SincSystem(w.numpoints, w.spacing, w.centershift, w.nuccharges)
+    phi = inp.seeded_orbitals(w.numpoints, w.spacing, w.nspf, seed=1)
+    tally = inp.seeded_tally(w.nspf, seed=2)
+    den = inp.seeded_hermitian_psd(w.nspf, seed=3)
+    inv = orc.invmatsmooth(den)
+    t0 = time.perf_counter()
+    _, red = sysm.call_twoe_matel00(phi, phi, workers=threads)
+    rp = orc.get_reducedpot(red, tally)
+    orc.actreduced00(sysm, phi, phi, den, inv, rp)
+    return time.perf_counter() - t0
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from sincgpu.inputs import WORKLOADS
+    w = WORKLOADS[args.config]
+    threads = os.cpu_count() or 1
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_reference_eval(w, threads)
+    ts = [cpu_reference_eval(w, threads) for _ in range(max(1, min(args.steps, 3)))]
+    t = float(np.median(ts))
+    v = 1.0 / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
+        "steps": len(ts), "warmup": min(args.warmup, 1), "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+        "data": "synthetic", "config": workload_config(w, l2="n/a (CPU)"),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{len(ts)} full orbital-RHS evaluations (median), numpy/scipy restatement "
+                                   f"of the reference on {threads} host threads; the Fortran reference has "
+                                   f"no compiler in this image"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# this implementation
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, world, local = dist_env()
+    import torch
+    from sincgpu import SincProject
+    from sincgpu.inputs import WORKLOADS, seeded_orbitals, seeded_tally, seeded_hermitian_psd, regularized_inverse
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    w = WORKLOADS[args.config]
+    n, G = w.nspf, w.G
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    proj = SincProject(w.numpoints, w.spacing, w.centershift, w.nuccharges, n, device=local)
+    proj.set_stream(stream.cuda_stream)
+
+    phi_h = seeded_orbitals(w.numpoints, w.spacing, n, seed=1 + rank)
+    tally_h = seeded_tally(n, seed=2)
+    den_h = seeded_hermitian_psd(n, seed=3)
+    inv_h = regularized_inverse(den_h)
+
+    def dev_from_fortran(a):
+        return torch.from_numpy(np.ascontiguousarray(a.T)).to(dev)
+
+    phi = dev_from_fortran(phi_h)
+    tally = dev_from_fortran(tally_h)
+    den = dev_from_fortran(den_h)
+    inv = dev_from_fortran(inv_h)
+    red = torch.empty((n, n, G), dtype=torch.complex128, device=dev)
+    mat = torch.empty((n, n, n, n), dtype=torch.complex128, device=dev)
+    out = torch.empty((n, G), dtype=torch.complex128, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        proj.orbital_rhs_dev(phi, tally, den, inv, red, out, twoematel=mat)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- timed region (device events per step, L2 flushed between steps) ----
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = SincProject.launch_count()
+    for a, b in evs:
+        flush.zero_()
+        a.record(stream)
+        step()
+        b.record(stream)
+    torch.cuda.synchronize()
+    launches = SincProject.launch_count() - l0
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    clk = clocks.stop()
+    t_local = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+    total_ms = float(t_local.item())
+    ms_step = total_ms / args.steps
+    value = world * args.steps / (total_ms / 1e3)
+
+    # ---- per-kernel times (profiled pass, same stream) for the roofline ----
+    proj.profile(True)
+    nprof = min(20, args.steps)
+    for _ in range(nprof):
+        flush.zero_()
+        step()
+    prof = proj.profile_read()
+    proj.profile(False)
+    roofline = make_roofline(w, prof, nprof, dev)
+
+    # ---- end to end through the host-array C entry (pinned host buffers) ----
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(proj, w, phi_h, tally_h, den_h, inv_h, args, stream, world, dist)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "complex128", "data": "synthetic (seeded orbitals, tally, density matrix)",
+        "config": workload_config(w), "clocks": clk, "gpu_launches": int(launches),
+        "launches_per_step": launches / args.steps, "fft_length": proj.fft_length,
+        "roofline": roofline, "stage_ms_per_step": {k: v[0] / nprof for k, v in prof.items()},
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        t = cpu_reference_eval(w, threads)
+        line["cpu_baseline"] = {"value": 1.0 / t, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": "1 full orbital-RHS evaluation of the same workload with the "
+                                          "numpy/scipy restatement of the reference"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    proj.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def make_roofline(w, prof, nprof, dev):
+    """Dominant kernel of the step with its algorithmic bytes or flops per launch."""
+    import torch
+    if not prof:
+        return None
+    name, (ms, nl) = max(prof.items(), key=lambda kv: kv[1][0])
+    per_launch_ms = ms / nl
+    n, G, N = w.nspf, w.G, w.numpoints
+    U = n * (n + 1) // 2
+    peaks = {}
+    try:
+        peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    hbm_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
+    launches_per_step = nl / nprof
+    if name in ("rp_gemm", "twoe_gemm", "ke_xy", "ke_z"):
+        # FP64 contraction: achieved FLOP/s against an in-run cuBLAS DGEMM
+        a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+        torch.matmul(a, a)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            torch.matmul(a, a)
+        e1.record()
+        torch.cuda.synchronize()
+        dgemm = 5 * 2 * 8192 ** 3 / (e0.elapsed_time(e1) / 1e3) / 1e12
+        flops = {"rp_gemm": 2.0 * G * 2 * U * 2 * n * n, "twoe_gemm": 2.0 * G * (2 * U) ** 2,
+                 "ke_xy": 2 * 2 * 2.0 * N ** 3 * N * n, "ke_z": 2 * 2.0 * N ** 3 * N * n}[name] / launches_per_step
+        ach = flops / (per_launch_ms / 1e3) / 1e12
+        return {"kernel": name, "bound": "tensor", "achieved": ach, "peak": dgemm, "unit": "TFLOP/s",
+                "frac": ach / dgemm, "traffic": None, "launch_ms": per_launch_ms,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64; the measured-peaks file has no FP64 figure)"}
+    P = {41: 81, 21: 42, 81: 162}.get(N, 2 * N)
+    bytes_per_pair = {
+        "coul_fwd_x": 16.0 * (2 * N ** 3 + N * N * P),
+        "coul_fwd_y": 16.0 * (N * N * P + N * P * P),
+        "coul_z": 16.0 * (2 * N * P * P) + 16.0 * P ** 3,
+        "coul_inv_y": 16.0 * (N * P * P + N * N * P),
+        "coul_inv_x": 16.0 * (N * N * P + N ** 3),
+    }
+    if name in bytes_per_pair:
+        by = bytes_per_pair[name] * U / launches_per_step
+    elif name == "rhs_redpot":
+        by = 16.0 * G * (n * n + 3 * n)
+    else:
+        by = 16.0 * G * n * 2
+    ach = by / (per_launch_ms / 1e3) / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+            "frac": ach / hbm, "traffic": None, "launch_ms": per_launch_ms, "peak_source": hbm_src}
+
+
+def run_e2e(proj, w, phi_h, tally_h, den_h, inv_h, args, stream, world, dist):
+    import torch
+    n, G = w.nspf, w.G
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a.T)).pin_memory()  # noqa: E731
+    phi_p, tally_p, den_p, inv_p = pin(phi_h), pin(tally_h), pin(den_h), pin(inv_h)
+    out_p = torch.empty((n, G), dtype=torch.complex128).pin_memory()
+    mat_p = torch.empty((n, n, n, n), dtype=torch.complex128).pin_memory()
+    from sincgpu.capi import _call, _ptr
+    import ctypes as C
+
+    def call():
+        _call("sincgpu_orbital_rhs", proj._h, _ptr(phi_p), _ptr(tally_p), _ptr(den_p), _ptr(inv_p),
+              0.0, -1.0, 0.0, _ptr(mat_p), _ptr(out_p))
+
+    for _ in range(3):
+        call()
+    steps = max(10, args.steps // 3)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    h2d = 16 * (G * n + n ** 4 + 2 * n * n)
+    d2h = 16 * (G * n + n ** 4)
+    return {"value": world * steps / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "steps": steps, "ms_per_step": ms / steps,
+            "path": "sincgpu_orbital_rhs (host arrays, pinned) through the C ABI"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,179 @@
+/*
+ * sincgpu -- B200 (sm_100a) implementation of the LBNL-AMO-MCTDHF polyatomic
+ * sinc-DVR orbital right-hand side, behind a plain C ABI.
+ *
+ * Conventions
+ *   - Every array is a Fortran array passed by address: column-major, the grid
+ *     index x fastest (x + N*y + N*N*z), then the orbital index.
+ *   - "complex" arrays are complex*16: interleaved (re, im) doubles.  Their
+ *     element count below is in complex numbers.
+ *   - Orbital indices in argument lists are 1-based, as in the Fortran caller.
+ *   - Every function returns SINCGPU_OK (0) or an error code; the message of the
+ *     last failure on the calling thread is available from sincgpu_last_error().
+ *     The library never aborts the process; the Fortran shim turns a non-zero
+ *     status into the reference's abort (OFLWR ... CFLST).
+ *   - Functions without the _dev suffix take HOST arrays (they upload, compute
+ *     and download before returning).  _dev functions take DEVICE pointers and
+ *     enqueue on the context stream; call sincgpu_synchronize() before reading
+ *     results on the host.
+ *   - A context is not re-entrant: callers serialise calls on one context.
+ *
+ * Citations are to the reference project (MCTDH.SRC/...).
+ */
+#ifndef SINCGPU_H
+#define SINCGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SINCGPU_OK 0
+#define SINCGPU_EINVAL 1   /* bad argument */
+#define SINCGPU_ECUDA 2    /* CUDA runtime failure */
+#define SINCGPU_ENOMEM 3   /* device allocation failed */
+#define SINCGPU_ESTATE 4   /* call made in the wrong state */
+#define SINCGPU_ETIMEOUT 5 /* bounded device wait expired */
+#define SINCGPU_ERANGE 6   /* size outside the supported range */
+
+typedef struct sincgpu_ctx sincgpu_ctx;
+
+/* Message of the last failure on this thread ("" if none). */
+const char* sincgpu_last_error(void);
+int sincgpu_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Set-up
+ * ------------------------------------------------------------------------- */
+
+/* Builds the project state on the device: 1-D kinetic vector (SINCDVR/SineDVR.f90:11-44,
+ * init_sinc_new.f90:441-464), the inverse-kinetic Coulomb kernel threed_two
+ * (SINCDVR/tooth.f90:12-231, sincproject.f90:119-188), the nuclear potential
+ * (sincproject.f90:190-250) and nucrepulsion (sinc_extraproject.f90:288-300).
+ * Replaces the get_twoe_new part of init_project (init_sinc_new.f90:533).
+ *   centershift(3,numcenters) in units of spacing/2; flags bit0: single-precision
+ *   sqrt in the far-field nuclear potential (sincproject.f90:220 without -r8);
+ *   bit1: notwoflag (zero Coulomb kernel, sincproject.f90:330-332). */
+int sincgpu_create(sincgpu_ctx** ctx, int numpoints, double spacing, int numcenters,
+                   const int* centershift, const double* nuccharges, int numspf, int toothnbig,
+                   int toothnsmall, int flags, int device);
+
+/* Same, but takes threed_two(-N:N-1,-N:N-1,-N:N-1) (complex, real valued) and
+ * pot(totpoints) already built by the Fortran init_project. */
+int sincgpu_create_from_tables(sincgpu_ctx** ctx, int numpoints, double spacing, int numspf,
+                               const double* threed_two, const double* pot, int device);
+
+int sincgpu_destroy(sincgpu_ctx* ctx);
+
+/* Copies back tempcoulomb(1-N:N-1)^3 = threed_two on that range (real),
+ * pot(totpoints), kevect(1-N:N-1) and nucrepulsion.  Any pointer may be NULL. */
+int sincgpu_get_tables(sincgpu_ctx* ctx, double* tempcoulomb, double* pot, double* kevect,
+                       double* nucrepulsion);
+
+/* Padded FFT length P (>= 2N-1) used for the Toeplitz convolution. */
+int sincgpu_fft_length(sincgpu_ctx* ctx);
+
+/* Tuning knobs: "coul_chunk" (pairs per Coulomb pass sequence, 0 = auto). */
+int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
+
+int sincgpu_synchronize(sincgpu_ctx* ctx);
+
+/* Makes the context enqueue on a caller-owned cudaStream_t (passed as void*).
+ * The caller keeps the stream alive for the life of the context. */
+int sincgpu_set_stream(sincgpu_ctx* ctx, void* stream);
+
+/* Number of kernels this library has launched in the process so far. */
+long long sincgpu_launch_count(void);
+
+/* Per-kernel CUDA-event timing on the context stream (off by default).
+ * sincgpu_profile_read synchronises, returns the accumulated milliseconds and
+ * launch counts per stage (indices: 0 coul_fwd_x, 1 coul_fwd_y, 2 coul_z,
+ * 3 coul_inv_y, 4 coul_inv_x, 5 twoe_gemm, 6 twoe_finish, 7 rp_w, 8 rp_gemm,
+ * 9 ke_xy, 10 ke_z, 11 rhs_mix, 12 rhs_redpot, 13 rhs_proj, 14 ci, 15 other)
+ * and resets them. */
+int sincgpu_profile(sincgpu_ctx* ctx, int enable);
+int sincgpu_profile_read(sincgpu_ctx* ctx, double* ms, long long* launches, int nstage);
+
+/* Page-locks a caller's host array so that host-array entry points copy at full
+ * PCIe/C2C speed.  Optional. */
+int sincgpu_host_register(void* ptr, long long bytes);
+int sincgpu_host_unregister(void* ptr);
+
+/* ---------------------------------------------------------------------------
+ * Drop-ins for the SINCDVR project interface (host arrays)
+ * ------------------------------------------------------------------------- */
+
+/* call_twoe_matel00 (SINCDVR/coreproject.f90:945-1194; caller MCTDH.SRC/matel.f90:95-96):
+ *   twoereduced(x,a,b) = sum_y threed_two(x-y) inspfs10(y,a) conj(inspfs20(y,b))
+ *   twoematel(a1,b1,a2,b2) = sum_x inspfs10(x,a1) conj(inspfs20(x,b1)) twoereduced(x,a2,b2)
+ * inspfs10/20(totpoints,numspf), twoematel(numspf^4), twoereduced(totpoints,numspf,numspf).
+ * lowspf/highspf must span all orbitals (single-rank build).  When inspfs10 and
+ * inspfs20 are the same array the hermitian pair symmetry halves the work. */
+int sincgpu_call_twoe_matel00(sincgpu_ctx* ctx, int lowspf, int highspf, const double* inspfs10,
+                              const double* inspfs20, double* twoematel, double* twoereduced);
+
+/* op_tinv (SINCDVR/coreproject.f90:250-539, serial path): twoereduced(:,i) =
+ * threed_two (*) twoeden03(:,i), i=1..allsize.  circsize only has to divide allsize
+ * (it selects batching in the reference and does not change the result). */
+int sincgpu_op_tinv(sincgpu_ctx* ctx, const double* twoeden03, double* twoereduced, int allsize,
+                    int circsize);
+
+/* mult_ke (SINCDVR/coreproject.f90:2104-2116): in/out(totpoints,howmany). */
+int sincgpu_mult_ke(sincgpu_ctx* ctx, const double* in, double* out, int howmany);
+
+/* mult_reducedpot (SINCDVR/coreproject.f90:1200-1235):
+ * outspfs(:,i) = sum_k reducedpot(:,k,i) inspfs(:,k), i = firstspf..lastspf;
+ * reducedpot(totpoints,numspf,firstspf:lastspf), outspfs(totpoints,firstspf:lastspf). */
+int sincgpu_mult_reducedpot(sincgpu_ctx* ctx, int firstspf, int lastspf, const double* inspfs,
+                            double* outspfs, const double* reducedpot);
+
+/* get_reducedpot0 (MCTDH.SRC/mean.f90:503-588): reducedpot(G,n^2) =
+ * twoereduced(G,n^2) x reducedpottally(n^2,n^2). */
+int sincgpu_get_reducedpot(sincgpu_ctx* ctx, const double* twoereduced,
+                           const double* reducedpottally, double* reducedpot);
+
+/* actreduced00 (MCTDH.SRC/derivs.f90:629-852) for numr=1, no frozen core, length
+ * gauge: out = (1-P) timefac [KE + pot + ztdpot z + W] (inspfs denmat) invdenmat,
+ * where W is the mult_reducedpot term on inspfs.  denmat/invdenmat(numspf,numspf). */
+int sincgpu_actreduced00(sincgpu_ctx* ctx, int dentimeflag, const double* inspfs,
+                         const double* projspfs, const double* denmat, const double* invdenmat,
+                         const double* reducedpot, double timefac_re, double timefac_im,
+                         int projflag, double ztdpot, double* outspfs);
+
+/* ---------------------------------------------------------------------------
+ * Device-resident forms (device pointers, context stream)
+ * ------------------------------------------------------------------------- */
+int sincgpu_twoe_matel_dev(sincgpu_ctx* ctx, const double* phi1, const double* phi2,
+                           double* twoematel, double* twoereduced);
+int sincgpu_mult_ke_dev(sincgpu_ctx* ctx, const double* in, double* out, int howmany);
+int sincgpu_mult_reducedpot_dev(sincgpu_ctx* ctx, const double* inspfs, double* outspfs,
+                                const double* reducedpot);
+/* Mean-field build from orbitals and a 2-RDM tally: Coulomb pair solves,
+ * twoematel and reducedpot (MCTDH.SRC/matel.f90:72-111 + mean.f90:484-590). */
+int sincgpu_mean_field_dev(sincgpu_ctx* ctx, const double* phi, const double* reducedpottally,
+                           double* twoematel, double* reducedpot);
+int sincgpu_actreduced_dev(sincgpu_ctx* ctx, int dentimeflag, const double* inspfs,
+                           const double* projspfs, const double* denmat, const double* invdenmat,
+                           const double* reducedpot, double timefac_re, double timefac_im,
+                           int projflag, double ztdpot, double* outspfs);
+
+/* One orbital-RHS evaluation = mean-field build (Coulomb pair solves, twoematel,
+ * reducedpot from the 2-RDM tally) + actreduced00 with projspfs = inspfs,
+ * dentimeflag = projflag = 1 (MCTDH.SRC/derivs.f90:629-852).  Device pointers;
+ * reducedpot(totpoints,n,n) receives the reduced potentials; twoematel may be NULL. */
+int sincgpu_orbital_rhs_dev(sincgpu_ctx* ctx, const double* phi, const double* reducedpottally,
+                            const double* denmat, const double* invdenmat, double timefac_re,
+                            double timefac_im, double ztdpot, double* twoematel,
+                            double* reducedpot, double* outspfs);
+
+/* Host-array form of the same evaluation: only phi, the tally and the two n x n
+ * matrices go up and only outspfs (and twoematel, if non-NULL) come back; the
+ * reduced potentials stay on the device.  A Fortran driver replaces the sequence
+ * twoe_matel + get_reducedpot + actreduced0 with this call. */
+int sincgpu_orbital_rhs(sincgpu_ctx* ctx, const double* phi, const double* reducedpottally,
+                        const double* denmat, const double* invdenmat, double timefac_re,
+                        double timefac_im, double ztdpot, double* twoematel, double* outspfs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SINCGPU_H */

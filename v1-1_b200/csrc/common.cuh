@@ -1,0 +1,73 @@
+// Shared helpers for the sinc-DVR orbital-RHS CUDA library (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#define SINCGPU_OK 0
+#define SINCGPU_EINVAL 1
+#define SINCGPU_ECUDA 2
+#define SINCGPU_ENOMEM 3
+#define SINCGPU_ESTATE 4
+#define SINCGPU_ETIMEOUT 5
+#define SINCGPU_ERANGE 6
+
+namespace sincgpu {
+
+// Records the message of the last failure for sincgpu_last_error().
+void set_error(const char* fmt, ...);
+
+#define SG_CUDA(call)                                                                  \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) {                                                           \
+      ::sincgpu::set_error("%s:%d: %s: %s", __FILE__, __LINE__, #call,                 \
+                           cudaGetErrorString(e_));                                    \
+      return SINCGPU_ECUDA;                                                            \
+    }                                                                                  \
+  } while (0)
+
+#define SG_CHECK(cond, code, ...)                                                      \
+  do {                                                                                 \
+    if (!(cond)) {                                                                     \
+      ::sincgpu::set_error(__VA_ARGS__);                                               \
+      return (code);                                                                   \
+    }                                                                                  \
+  } while (0)
+
+#define SG_TRY(expr)                                                                   \
+  do {                                                                                 \
+    int r_ = (expr);                                                                   \
+    if (r_ != SINCGPU_OK) return r_;                                                   \
+  } while (0)
+
+// Counts kernel launches of this library (sincgpu_launch_count).
+void count_launch();
+
+// Kernel launch check: catches configuration errors right after launch.
+#define SG_LAUNCHED()            \
+  do {                           \
+    ::sincgpu::count_launch();   \
+    SG_CUDA(cudaGetLastError()); \
+  } while (0)
+
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a*conj(b)
+  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) {
+  return make_double2(a.x - b.x, a.y - b.y);
+}
+__host__ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__host__ __device__ __forceinline__ double2 cscale(double2 a, double s) {
+  return make_double2(a.x * s, a.y * s);
+}
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace sincgpu

@@ -1,0 +1,132 @@
+// Device-resident state of one sinc-DVR system (the GPU counterpart of the
+// SINCDVR project module state, SINCDVR/sincproject.f90:4-43).
+#pragma once
+#include <cuda_runtime.h>
+#include <vector>
+#include "common.cuh"
+#include "fft_engine.cuh"
+
+namespace sincgpu {
+
+struct Workspace {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t need);  // grows (cudaMalloc) when needed
+  void release();
+};
+
+// Per-kernel CUDA-event timing (off by default; sincgpu_profile).
+enum Stage {
+  ST_COUL_FWD_X = 0, ST_COUL_FWD_Y, ST_COUL_Z, ST_COUL_INV_Y, ST_COUL_INV_X,
+  ST_TWOE_GEMM, ST_TWOE_FINISH, ST_RP_W, ST_RP_GEMM, ST_KE_XY, ST_KE_Z,
+  ST_RHS_MIX, ST_RHS_REDPOT, ST_RHS_PROJ, ST_CI, ST_OTHER, ST_COUNT
+};
+
+struct Prof {
+  bool on = false;
+  struct Rec { int stage; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  double ms[ST_COUNT] = {};
+  long long launches[ST_COUNT] = {};
+};
+
+struct Ctx {
+  // ---- problem parameters -------------------------------------------------
+  int N = 0;             // points per axis (numpoints == gridpoints, nbox=1)
+  long long G = 0;       // totpoints = N^3
+  int nspf = 0;          // orbitals
+  double spacing = 0.0;
+  int numcenters = 0;
+  std::vector<int> centershift;     // 3*numcenters
+  std::vector<double> nuccharges;
+  double nucrepulsion = 0.0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+
+  // ---- FFT plan for the padded Toeplitz grid ------------------------------
+  FftPlan plan{};
+  int P = 0;             // padded axis length, P >= 2N-1, 7-smooth
+  int tx = 0;            // column-tile width of the y/z passes
+
+  // ---- device tables --------------------------------------------------------
+  double* d_kevect = nullptr;   // K(d), d in [1-N, N-1]           (2N-1)
+  double* d_ketile = nullptr;   // K(j-l) padded S x S for the DMMA KE kernels
+  int ke_stride = 0;            // S (row stride of d_ketile)
+  double* d_pot = nullptr;      // nuclear potential              (G)
+  double* d_zdip = nullptr;     // z coordinate of each point      (G)
+  double* d_tcoul = nullptr;    // threed_two on [1-N,N-1]^3 (real) ((2N-1)^3)
+  double2* d_khat = nullptr;    // DFT of the padded kernel / P^3  (P^3)
+  double2* d_roots = nullptr;   // exp(-2 pi i m / P)              (P)
+
+  // ---- scratch --------------------------------------------------------------
+  Workspace ws_fft;     // W1 + W2 of the Coulomb passes
+  Workspace ws_pairs;   // pair lists
+  Workspace ws_gemm;    // split-K partials, W matrix
+  Workspace ws_rhs;     // RHS temporaries
+  Workspace ws_io;      // staging for host-pointer entry points
+  Workspace ws_red;     // planar reduced potentials of the last build
+  Workspace ws_conv;    // layout conversion scratch
+  Workspace ws_state;   // resident mean-field state of the fused orbital-RHS entry
+  int coul_chunk = 0;   // pairs per pass sequence (0 = automatic)
+  Prof prof;
+
+  ~Ctx();
+};
+
+// Brackets one kernel launch with events on the context stream when profiling.
+struct ProfScope {
+  Ctx& c;
+  int stage;
+  cudaEvent_t a = nullptr;
+  ProfScope(Ctx& cc, int st) : c(cc), stage(st) {
+    if (c.prof.on) {
+      cudaEventCreate(&a);
+      cudaEventRecord(a, c.stream);
+    }
+  }
+  ~ProfScope() {
+    if (c.prof.on) {
+      cudaEvent_t b;
+      cudaEventCreate(&b);
+      cudaEventRecord(b, c.stream);
+      c.prof.recs.push_back({stage, a, b});
+    }
+  }
+};
+
+// setup.cu
+int build_tables(Ctx& c, int toothnbig, int toothnsmall, int flags);
+int build_tables_from_arrays(Ctx& c, const double2* threed_two_host, const double* pot_host);
+int choose_plan(Ctx& c);
+int make_khat(Ctx& c);
+
+// coulomb.cu: R_p = T * (phi1_a conj(phi2_b)) for pairs p=(a_p,b_p).
+// Rpl (device) receives the planar real/imag parts: Rpl[p*G+x] = Re, Rpl[(npair+p)*G+x] = Im.
+// full (device, optional) receives twoereduced(x,a,b) interleaved; when `herm` the
+// conjugate pair (b,a) is written too.
+int coulomb_pairs(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa,
+                  const int* h_pb, int npair, double* Rpl, double2* full, bool herm);
+// op_tinv on explicit densities: dens(G, m) -> red(G, m)
+int coulomb_dens(Ctx& c, const double2* dens, int m, double2* red);
+
+// contract.cu
+int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa,
+               const int* h_pb, int npair, const double* Rpl, bool herm, double2* twoematel);
+int reduced_pot(Ctx& c, const double* Rpl, const int* h_pa, const int* h_pb, int npair,
+                bool herm, const double2* tally, double2* reducedpot);
+int reduced_pot_full(Ctx& c, const double2* twoereduced, const double2* tally, double2* reducedpot);
+
+// ke.cu: out = KE(in) [+ pot*in + zfield*z*in when `extra`]
+int mult_ke(Ctx& c, const double2* in, double2* out, int howmany, bool extra, double zfield);
+
+// rhs.cu
+int mult_reducedpot(Ctx& c, const double2* phi, const double2* redpot, double2* out);
+// orbitals [i0, i0+ni) only; redpot/out hold just that window
+int mult_reducedpot_range(Ctx& c, const double2* phi, const double2* redpot, int i0, int ni,
+                          double2* out);
+int actreduced(Ctx& c, const double2* phi, const double2* proj, const double2* denmat,
+               const double2* invdenmat, const double2* redpot, double2 timefac,
+               int dentimeflag, int projflag, double zfield, double2* out);
+
+}  // namespace sincgpu

@@ -1,0 +1,87 @@
+"""Seeded synthetic inputs and the named workloads of the benchmark.
+
+The reference measures on no public dataset; the workloads below are the
+synthetic systems of its benchmark configurations, with nuclei snapped to the
+grid / half-grid positions the sinc-DVR project requires
+(SINCDVR/sincproject.f90:196-204): an odd point count needs even
+`centershift` (units of spacing/2).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass(frozen=True)
+class Workload:
+    name: str
+    numpoints: int
+    spacing: float
+    centershift: tuple
+    nuccharges: tuple
+    nspf: int
+    numelec: int
+    note: str = ""
+
+    @property
+    def G(self):
+        return self.numpoints ** 3
+
+
+WORKLOADS = {
+    # He, Z=2 at the origin, 21^3, spacing 0.4, 5 orbitals, 2 electrons (25 configs)
+    "A": Workload("A", 21, 0.4, ((0, 0, 0),), (2.0,), 5, 2, "He"),
+    # H2-like, Z=1 at z=-+0.75 (centershift +-6 on the 41^3 grid), spacing 0.25, 10 orbitals
+    "B": Workload("B", 41, 0.25, ((0, 0, 6), (0, 0, -6)), (1.0, 1.0), 10, 2,
+                  "H2-like; nuclei snapped from +-0.7 to +-0.75 bohr (grid parity rule)"),
+    # LiH-like, Z=3,1 at z=-+1.5 (centershift +-10), 81^3, spacing 0.3, 16 orbitals, 4 electrons
+    "C": Workload("C", 81, 0.3, ((0, 0, 10), (0, 0, -10)), (3.0, 1.0), 16, 4, "LiH-like, 162^3 FFT grid"),
+}
+
+
+def grid_points(numpoints: int, spacing: float) -> np.ndarray:
+    p = np.arange(1, numpoints + 1, dtype=np.float64) * spacing
+    return p - (p[0] + p[-1]) / 2.0
+
+
+def seeded_orbitals(numpoints: int, spacing: float, nspf: int, seed: int, width: float = 1.0):
+    """phi_k = exp(-|x|^2/(2 w^2)) z_k(x), z ~ CN(0,1) seeded, then modified
+    Gram-Schmidt in index order with the hermitian dot.  Shape (G, nspf), Fortran order."""
+    rng = np.random.default_rng(seed)
+    p = grid_points(numpoints, spacing)
+    r2 = p[:, None, None] ** 2 + p[None, :, None] ** 2 + p[None, None, :] ** 2
+    G = numpoints ** 3
+    env = np.exp(-r2 / (2 * width ** 2)).reshape(G, order="F")
+    z = (rng.standard_normal((G, nspf)) + 1j * rng.standard_normal((G, nspf))) / math.sqrt(2)
+    out = np.asfortranarray(env[:, None] * z)
+    for i in range(nspf):
+        for j in range(i):
+            out[:, i] -= out[:, j] * np.vdot(out[:, j], out[:, i])
+        out[:, i] /= math.sqrt(np.vdot(out[:, i], out[:, i]).real)
+    return out
+
+
+def seeded_hermitian_psd(n: int, seed: int):
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    return np.asfortranarray(a @ np.conj(a).T / n + 0.1 * np.eye(n))
+
+
+def seeded_tally(n: int, seed: int):
+    """2-RDM-shaped tally with the symmetries Gamma(a,b,c,d) = conj Gamma(b,a,d,c)
+    = Gamma(c,d,a,b)."""
+    rng = np.random.default_rng(seed)
+    g = rng.standard_normal((n, n, n, n)) + 1j * rng.standard_normal((n, n, n, n))
+    g = g + np.conj(g.transpose(1, 0, 3, 2))
+    g = g + g.transpose(2, 3, 0, 1)
+    return np.asfortranarray(g / 4)
+
+
+def regularized_inverse(a, tol=1e-10):
+    """Host-side helper for synthetic inputs: SVD inverse with the denreg rule."""
+    u, s, vt = np.linalg.svd(a)
+    inv = np.where(s < tol, 1.0 / tol, 1.0 / np.where(s == 0, 1.0, s))
+    inv = np.where(s == 0, 0.0, inv)
+    return np.asfortranarray((np.conj(vt).T * inv[None, :]) @ np.conj(u).T)
