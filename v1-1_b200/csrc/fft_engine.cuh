@@ -10,7 +10,8 @@
 //   for j in [0, P/r):  k = j mod L
 //     y_q = sum_t x[j + t*P/r] * w^(t*k) * W_r^(t*q),   w = exp(-+2*pi*i/(L*r))
 //     out[(j/L)*L*r + k + q*L] = y_q
-// which ends in natural order with no bit reversal.
+// which ends in natural order with no bit reversal.  Each radix is a template so
+// that the r values of a butterfly live in registers.
 #pragma once
 #include "common.cuh"
 
@@ -33,46 +34,123 @@ __device__ __forceinline__ double2 root(const double2* roots, int m) {
   return w;
 }
 
-// One radix-r butterfly on r inputs already multiplied by their twiddles.
+// i*z (forward: -i*z)
 template <bool INV>
-__device__ __forceinline__ void dft_small(double2* a, int r, const double2* roots, int P) {
-  if (r == 2) {
+__device__ __forceinline__ double2 mul_mi(double2 z) {
+  return INV ? make_double2(-z.y, z.x) : make_double2(z.y, -z.x);
+}
+
+template <int R, bool INV>
+struct Butterfly;
+
+template <bool INV>
+struct Butterfly<2, INV> {
+  __device__ __forceinline__ static void run(double2* a, const double2*, int) {
     double2 t0 = a[0], t1 = a[1];
     a[0] = cadd(t0, t1);
     a[1] = csub(t0, t1);
-  } else if (r == 3) {
-    // W_3 = exp(-+2 pi i/3) = (-1/2, -+s)
-    const double s = INV ? -roots[P / 3].y : roots[P / 3].y;  // = -+ sin(2pi/3)
+  }
+};
+
+template <bool INV>
+struct Butterfly<3, INV> {
+  __device__ __forceinline__ static void run(double2* a, const double2* roots, int P) {
+    // W_3 = exp(-+2 pi i/3) = (-1/2, s),  s = -+ sin(2 pi/3)
+    const double s = INV ? -roots[P / 3].y : roots[P / 3].y;
     double2 sum = cadd(a[1], a[2]);
     double2 dif = csub(a[1], a[2]);
-    double2 m = make_double2(a[0].x - 0.5 * sum.x, a[0].y - 0.5 * sum.y);
-    // i*s*dif = (-s*dif.y, s*dif.x)
+    double2 m = make_double2(fma(-0.5, sum.x, a[0].x), fma(-0.5, sum.y, a[0].y));
     a[0] = cadd(a[0], sum);
-    a[1] = make_double2(m.x - s * dif.y, m.y + s * dif.x);
-    a[2] = make_double2(m.x + s * dif.y, m.y - s * dif.x);
-  } else if (r == 4) {
+    a[1] = make_double2(fma(-s, dif.y, m.x), fma(s, dif.x, m.y));
+    a[2] = make_double2(fma(s, dif.y, m.x), fma(-s, dif.x, m.y));
+  }
+};
+
+template <bool INV>
+struct Butterfly<4, INV> {
+  __device__ __forceinline__ static void run(double2* a, const double2*, int) {
     double2 s02 = cadd(a[0], a[2]), d02 = csub(a[0], a[2]);
     double2 s13 = cadd(a[1], a[3]), d13 = csub(a[1], a[3]);
-    // forward: W_4 = -i;  -i*d13 = (d13.y, -d13.x)
-    double2 rot = INV ? make_double2(-d13.y, d13.x) : make_double2(d13.y, -d13.x);
+    double2 rot = mul_mi<INV>(d13);
     a[0] = cadd(s02, s13);
     a[2] = csub(s02, s13);
     a[1] = cadd(d02, rot);
     a[3] = csub(d02, rot);
-  } else {
-    double2 in[8];
+  }
+};
+
+// odd prime radices: direct DFT with the symmetric pairing t <-> r-t
+template <int R, bool INV>
+struct ButterflyOdd {
+  __device__ __forceinline__ static void run(double2* a, const double2* roots, int P) {
+    const int step = P / R;
+    double2 sp[(R - 1) / 2], sm[(R - 1) / 2];
 #pragma unroll
-    for (int t = 0; t < 8; ++t)
-      if (t < r) in[t] = a[t];
-    const int step = P / r;
-    for (int q = 0; q < r; ++q) {
-      double2 acc = in[0];
-      for (int t = 1; t < r; ++t) {
-        int e = (t * q) % r;
-        acc = cadd(acc, cmul(in[t], root<INV>(roots, e * step)));
-      }
-      a[q] = acc;
+    for (int t = 1; t <= (R - 1) / 2; ++t) {
+      sp[t - 1] = cadd(a[t], a[R - t]);
+      sm[t - 1] = csub(a[t], a[R - t]);
     }
+    double2 y[R];
+    double2 y0 = a[0];
+#pragma unroll
+    for (int t = 0; t < (R - 1) / 2; ++t) y0 = cadd(y0, sp[t]);
+    y[0] = y0;
+#pragma unroll
+    for (int q = 1; q <= (R - 1) / 2; ++q) {
+      double2 re = a[0];   // sum_t cos(2 pi t q / R) sp_t
+      double2 im = make_double2(0.0, 0.0);  // sum_t sin-part of sm_t
+#pragma unroll
+      for (int t = 1; t <= (R - 1) / 2; ++t) {
+        const double2 w = root<INV>(roots, ((t * q) % R) * step);  // (cos, -+sin)
+        re.x = fma(w.x, sp[t - 1].x, re.x);
+        re.y = fma(w.x, sp[t - 1].y, re.y);
+        im.x = fma(w.y, sm[t - 1].x, im.x);
+        im.y = fma(w.y, sm[t - 1].y, im.y);
+      }
+      // y_q = re + i*im,  y_{R-q} = re - i*im
+      y[q] = make_double2(re.x - im.y, re.y + im.x);
+      y[R - q] = make_double2(re.x + im.y, re.y - im.x);
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) a[q] = y[q];
+  }
+};
+template <bool INV>
+struct Butterfly<5, INV> : ButterflyOdd<5, INV> {};
+template <bool INV>
+struct Butterfly<7, INV> : ButterflyOdd<7, INV> {};
+
+template <int R, bool INV>
+__device__ __forceinline__ void fft_stage(const double2* __restrict__ src, double2* __restrict__ dst,
+                                          int nlines, int lstride, int estride, int P, int L,
+                                          const double2* roots, bool lines_fast) {
+  const int Pr = P / R;
+  const int tw = P / (L * R);
+  const int nitems = nlines * Pr;
+  for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
+    int l, j;
+    if (lines_fast) {
+      j = it / nlines;
+      l = it - j * nlines;
+    } else {
+      l = it / Pr;
+      j = it - l * Pr;
+    }
+    const int jL = j / L;
+    const int k = j - jL * L;
+    double2 a[R];
+    const double2* sl = src + l * lstride;
+#pragma unroll
+    for (int t = 0; t < R; ++t) {
+      double2 v = sl[(j + t * Pr) * estride];
+      if (t > 0 && k > 0) v = cmul(v, root<INV>(roots, t * k * tw));
+      a[t] = v;
+    }
+    Butterfly<R, INV>::run(a, roots, P);
+    double2* dl = dst + l * lstride;
+    const int base = jL * L * R + k;
+#pragma unroll
+    for (int q = 0; q < R; ++q) dl[(base + q * L) * estride] = a[q];
   }
 }
 
@@ -81,6 +159,7 @@ __device__ __forceinline__ void dft_small(double2* a, int r, const double2* root
 // `lines_fast` selects the work-item order: consecutive threads on consecutive
 // lines (column tiles) or on consecutive indices of one line (row tiles).
 // Returns the buffer holding the result (A or B); both must be distinct.
+// The caller synchronises the block before the call; the call ends synchronised.
 template <bool INV>
 __device__ double2* fft_lines(double2* A, double2* B, int nlines, int lstride, int estride,
                               const FftPlan& plan, const double2* roots, bool lines_fast) {
@@ -90,35 +169,12 @@ __device__ double2* fft_lines(double2* A, double2* B, int nlines, int lstride, i
   double2* dst = B;
   for (int s = 0; s < plan.nrad; ++s) {
     const int r = plan.rad[s];
-    const int Pr = P / r;
-    const int tw = P / (L * r);
-    const int nitems = nlines * Pr;
-    for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
-      int l, j;
-      if (lines_fast) {
-        l = it % nlines;
-        j = it / nlines;
-      } else {
-        j = it % Pr;
-        l = it / Pr;
-      }
-      const int k = j % L;
-      double2 a[8];
-      const double2* sl = src + l * lstride;
-#pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        if (t < r) {
-          double2 v = sl[(j + t * Pr) * estride];
-          if (t > 0 && k > 0) v = cmul(v, root<INV>(roots, t * k * tw));
-          a[t] = v;
-        }
-      }
-      dft_small<INV>(a, r, roots, P);
-      double2* dl = dst + l * lstride;
-      const int base = (j / L) * L * r + k;
-#pragma unroll
-      for (int q = 0; q < 8; ++q)
-        if (q < r) dl[(base + q * L) * estride] = a[q];
+    switch (r) {
+      case 2: fft_stage<2, INV>(src, dst, nlines, lstride, estride, P, L, roots, lines_fast); break;
+      case 3: fft_stage<3, INV>(src, dst, nlines, lstride, estride, P, L, roots, lines_fast); break;
+      case 4: fft_stage<4, INV>(src, dst, nlines, lstride, estride, P, L, roots, lines_fast); break;
+      case 5: fft_stage<5, INV>(src, dst, nlines, lstride, estride, P, L, roots, lines_fast); break;
+      default: fft_stage<7, INV>(src, dst, nlines, lstride, estride, P, L, roots, lines_fast); break;
     }
     __syncthreads();
     double2* t = src;

@@ -140,13 +140,20 @@ __global__ void __launch_bounds__(256) dots_kernel(const double2* __restrict__ P
   }
 }
 
-__global__ void dots_reduce_kernel(const double2* __restrict__ partial, int nblk, int nn,
-                                   double2* __restrict__ D) {
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= nn) return;
+// one CTA per element: strided partial sums then a fixed-shape tree (deterministic)
+__global__ void __launch_bounds__(128) dots_reduce_kernel(const double2* __restrict__ partial,
+                                                          int nblk, int nn, double2* __restrict__ D) {
+  __shared__ double2 red[128];
+  const int e = blockIdx.x;
   double2 s = make_double2(0.0, 0.0);
-  for (int b = 0; b < nblk; ++b) s = cadd(s, partial[(long long)b * nn + e]);
-  D[e] = s;
+  for (int b = threadIdx.x; b < nblk; b += 128) s = cadd(s, partial[(long long)b * nn + e]);
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 64; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] = cadd(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) D[e] = red[0];
 }
 
 // out(x,i) = T(x,i) - sum_j P_j(x) D(j,i)
@@ -239,7 +246,7 @@ int actreduced(Ctx& c, const double2* phi, const double2* proj, const double2* d
     ProfScope ps(c, ST_RHS_PROJ);
     dots_kernel<<<nb, 256, 0, c.stream>>>(proj, T, n, G, xper, part);
     SG_LAUNCHED();
-    dots_reduce_kernel<<<ceil_div(n * n, 256), 256, 0, c.stream>>>(part, nb, n * n, D);
+    dots_reduce_kernel<<<n * n, 128, 0, c.stream>>>(part, nb, n * n, D);
     SG_LAUNCHED();
     SG_DISPATCH_N(n, project_kernel, <<<b256, 256, 0, c.stream>>>(T, proj, D, n, G, out));
     SG_LAUNCHED();

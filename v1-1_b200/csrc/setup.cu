@@ -26,11 +26,12 @@ static bool smooth7(int p) {
   return p == 1;
 }
 
+int fft_length_for(int min_len, int* p1, int* p2);  // coulomb.cu
+
 int choose_plan(Ctx& c) {
-  int P = 2 * c.N - 1;
-  while (!smooth7(P)) ++P;
-  SG_CHECK(P <= kMaxFftLen, SINCGPU_ERANGE, "padded FFT length %d exceeds %d (N=%d)", P,
-           kMaxFftLen, c.N);
+  int P = fft_length_for(2 * c.N - 1, nullptr, nullptr);
+  SG_CHECK(P > 0 && P <= kMaxFftLen && smooth7(P), SINCGPU_ERANGE,
+           "no supported padded FFT length >= %d (N=%d)", 2 * c.N - 1, c.N);
   FftPlan pl{};
   pl.P = P;
   int p = P, k = 0;
