@@ -2,12 +2,14 @@
 """Benchmark of the sinc-DVR orbital right-hand side on B200.
 
 Metric: orbital-RHS evaluations per second.  One evaluation (one "step") is a
-mean-field build -- pair densities, Toeplitz/FFT Coulomb solves, twoematel,
-reducedpot from the 2-RDM tally -- followed by one actreduced00 on the same
-orbitals (MCTDH.SRC/derivs.f90:629-852 with the SINCDVR project operators).
+mean-field build -- 1-RDM, its regularised inverse and the 2-RDM from the
+A-vector over the walk tables, pair densities, Toeplitz/FFT Coulomb solves,
+twoematel, reducedpot -- followed by one actreduced00 on the same orbitals
+(MCTDH.SRC/derivs.f90:629-852 with the SINCDVR project operators).
 
 Workload B (default): two Z=1 nuclei at z=+-0.75 bohr, 41^3 grid, spacing 0.25,
-10 orbitals, complex128, seeded synthetic orbitals/tally/density matrices.
+10 orbitals, 2 electrons (full M_s=0 CI, 100 configurations), complex128,
+seeded synthetic orbitals and A-vector.
 
   python bench.py [--gpus N --steps K --warmup W]      # this implementation
   python bench.py --impl reference [...]               # CPU reference restatement
@@ -119,18 +121,28 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU reference (oracle restatement), used for --impl reference and cpu_baseline
 # ---------------------------------------------------------------------------
+def seeded_avector(nc, seed):
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal(nc) + 1j * rng.standard_normal(nc)
+    return a / np.linalg.norm(a)
+
+
 def cpu_reference_eval(w, threads):
-    """One orbital-RHS evaluation with the CPU restatement of the reference.
-    Returns (seconds, description)."""
+    """Seconds for one orbital-RHS evaluation with the CPU restatement of the
+    reference: 1-RDM + regularised inverse + 2-RDM from the A-vector, pair
+    Coulomb solves and twoematel, reducedpot, actreduced00."""
     sys.path.insert(0, str(REPO))
     from oracle import sinc_oracle as orc
+    from oracle.walks_oracle import CIWalks
     from sincgpu import inputs as inp
     sysm = orc.SincSystem(w.numpoints, w.spacing, w.centershift, w.nuccharges)
+    ow = CIWalks(w.numelec, w.nspf, 0)
     phi = inp.seeded_orbitals(w.numpoints, w.spacing, w.nspf, seed=1)
-    tally = inp.seeded_tally(w.nspf, seed=2)
-    den = inp.seeded_hermitian_psd(w.nspf, seed=3)
-    inv = orc.invmatsmooth(den)
+    a = seeded_avector(ow.numconfig, seed=2)
     t0 = time.perf_counter()
+    den = ow.getdenmat00(a)
+    inv = orc.invmatsmooth(den)
+    tally = ow.get_tworeducedx(a)
     _, red = sysm.call_twoe_matel00(phi, phi, workers=threads)
     rp = orc.get_reducedpot(red, tally)
     orc.actreduced00(sysm, phi, phi, den, inv, rp)
@@ -173,8 +185,8 @@ def main():
         return run_reference(args)
     rank, world, local = dist_env()
     import torch
-    from sincgpu import SincProject
-    from sincgpu.inputs import WORKLOADS, seeded_orbitals, seeded_tally, seeded_hermitian_psd, regularized_inverse
+    from sincgpu import SincProject, WalkTables
+    from sincgpu.inputs import WORKLOADS, seeded_orbitals
 
     torch.cuda.set_device(local)
     dist = None
@@ -188,26 +200,29 @@ def main():
     stream = torch.cuda.current_stream()
     proj = SincProject(w.numpoints, w.spacing, w.centershift, w.nuccharges, n, device=local)
     proj.set_stream(stream.cuda_stream)
+    walks = WalkTables(w.numelec, n, 0)
+    proj.ci_attach(walks)
+    nc = walks.numconfig
 
     phi_h = seeded_orbitals(w.numpoints, w.spacing, n, seed=1 + rank)
-    tally_h = seeded_tally(n, seed=2)
-    den_h = seeded_hermitian_psd(n, seed=3)
-    inv_h = regularized_inverse(den_h)
+    a_h = seeded_avector(nc, seed=2 + rank)
 
-    def dev_from_fortran(a):
-        return torch.from_numpy(np.ascontiguousarray(a.T)).to(dev)
+    def dev_from_fortran(x):
+        return torch.from_numpy(np.ascontiguousarray(np.asarray(x).T)).to(dev)
 
     phi = dev_from_fortran(phi_h)
-    tally = dev_from_fortran(tally_h)
-    den = dev_from_fortran(den_h)
-    inv = dev_from_fortran(inv_h)
-    red = torch.empty((n, n, G), dtype=torch.complex128, device=dev)
-    mat = torch.empty((n, n, n, n), dtype=torch.complex128, device=dev)
-    out = torch.empty((n, G), dtype=torch.complex128, device=dev)
+    avec = dev_from_fortran(a_h)
+    cplx = dict(dtype=torch.complex128, device=dev)
+    den = torch.empty((n, n), **cplx)
+    inv = torch.empty((n, n), **cplx)
+    tally = torch.empty((n, n, n, n), **cplx)
+    mat = torch.empty((n, n, n, n), **cplx)
+    red = torch.empty((n, n, G), **cplx)
+    out = torch.empty((n, G), **cplx)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def step():
-        proj.orbital_rhs_dev(phi, tally, den, inv, red, out, twoematel=mat)
+        proj.orbital_rhs_avec_dev(phi, avec, den, inv, tally, mat, red, out)
 
     for _ in range(args.warmup):
         step()
@@ -238,6 +253,9 @@ def main():
     ms_step = total_ms / args.steps
     value = world * args.steps / (total_ms / 1e3)
 
+    # ---- secondary rates: orbital-RHS matvec alone, CI sigma alone ----
+    secondary = secondary_rates(proj, torch, stream, flush, phi, den, inv, red, out, mat, avec, n, G)
+
     # ---- per-kernel times (profiled pass, same stream) for the roofline ----
     proj.profile(True)
     nprof = min(20, args.steps)
@@ -251,15 +269,17 @@ def main():
     # ---- end to end through the host-array C entry (pinned host buffers) ----
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(proj, w, phi_h, tally_h, den_h, inv_h, args, stream, world, dist)
+        e2e = run_e2e(proj, w, phi_h, a_h, args, stream, world, dist)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "complex128", "data": "synthetic (seeded orbitals, tally, density matrix)",
+        "vs_baseline": None, "dtype": "complex128",
+        "data": "synthetic (seeded Gaussian-envelope orbitals, seeded normalised A-vector)",
         "config": workload_config(w), "clocks": clk, "gpu_launches": int(launches),
-        "launches_per_step": launches / args.steps, "fft_length": proj.fft_length,
-        "roofline": roofline, "stage_ms_per_step": {k: v[0] / nprof for k, v in prof.items()},
+        "launches_per_step": launches / args.steps, "fft_length": proj.fft_length, "numconfig": nc,
+        "roofline": roofline, "secondary": secondary,
+        "stage_ms_per_step": {k: v[0] / nprof for k, v in prof.items()},
     }
     if e2e:
         line["e2e"] = e2e
@@ -276,6 +296,30 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def secondary_rates(proj, torch, stream, flush, phi, den, inv, red, out, mat, avec, n, G):
+    """Krylov-matvec rate (actreduced00 alone on resident mean fields) and CI
+    sigma rate (sparseconfigmult on assembled matrices)."""
+    res = {}
+    mats = torch.empty((3, n, n), dtype=torch.complex128, device=phi.device)
+    proj.onebody_matel_dev(phi, mats)
+    proj.assemble_sparsemats_dev(mat, mats)
+    sig = torch.empty_like(avec)
+    for name, fn, reps in (
+            ("rhs_matvecs_per_s", lambda: proj.actreduced_dev(phi, phi, den, inv, red, out), 50),
+            ("sigma_per_s", lambda: proj.sparseconfigmult_dev(avec, sig), 200)):
+        for _ in range(3):
+            fn()
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[name] = reps / (e0.elapsed_time(e1) / 1e3)
+    return res
 
 
 def make_roofline(w, prof, nprof, dev):
@@ -332,19 +376,16 @@ def make_roofline(w, prof, nprof, dev):
             "frac": ach / hbm, "traffic": None, "launch_ms": per_launch_ms, "peak_source": hbm_src}
 
 
-def run_e2e(proj, w, phi_h, tally_h, den_h, inv_h, args, stream, world, dist):
+def run_e2e(proj, w, phi_h, a_h, args, stream, world, dist):
     import torch
-    n, G = w.nspf, w.G
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a.T)).pin_memory()  # noqa: E731
-    phi_p, tally_p, den_p, inv_p = pin(phi_h), pin(tally_h), pin(den_h), pin(inv_h)
-    out_p = torch.empty((n, G), dtype=torch.complex128).pin_memory()
-    mat_p = torch.empty((n, n, n, n), dtype=torch.complex128).pin_memory()
     from sincgpu.capi import _call, _ptr
-    import ctypes as C
+    n, G = w.nspf, w.G
+    phi_p = torch.from_numpy(np.ascontiguousarray(phi_h.T)).pin_memory()
+    a_p = torch.from_numpy(np.ascontiguousarray(a_h)).pin_memory()
+    out_p = torch.empty((n, G), dtype=torch.complex128).pin_memory()
 
     def call():
-        _call("sincgpu_orbital_rhs", proj._h, _ptr(phi_p), _ptr(tally_p), _ptr(den_p), _ptr(inv_p),
-              0.0, -1.0, 0.0, _ptr(mat_p), _ptr(out_p))
+        _call("sincgpu_orbital_rhs_avec", proj._h, _ptr(phi_p), _ptr(a_p), 0.0, -1.0, 0.0, _ptr(out_p))
 
     for _ in range(3):
         call()
@@ -363,11 +404,11 @@ def run_e2e(proj, w, phi_h, tally_h, den_h, inv_h, args, stream, world, dist):
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
-    h2d = 16 * (G * n + n ** 4 + 2 * n * n)
-    d2h = 16 * (G * n + n ** 4)
+    h2d = 16 * (G * n + len(a_h))
+    d2h = 16 * (G * n)
     return {"value": world * steps / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "steps": steps, "ms_per_step": ms / steps,
-            "path": "sincgpu_orbital_rhs (host arrays, pinned) through the C ABI"}
+            "path": "sincgpu_orbital_rhs_avec (host orbitals + A-vector in, host RHS out; pinned) through the C ABI"}
 
 
 if __name__ == "__main__":

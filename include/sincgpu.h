@@ -173,6 +173,98 @@ int sincgpu_orbital_rhs(sincgpu_ctx* ctx, const double* phi, const double* reduc
                         const double* denmat, const double* invdenmat, double timefac_re,
                         double timefac_im, double ztdpot, double* twoematel, double* outspfs);
 
+/* ---------------------------------------------------------------------------
+ * CI side: determinant list, walks, hops (host tables) and their device use
+ * ------------------------------------------------------------------------- */
+typedef struct sincgpu_walks sincgpu_walks;
+
+/* Builds the determinant list and the walk/hop tables exactly as
+ * fast_newconfiglist (MCTDH.SRC/newconfig.f90:349-1040), walks/getnumwalks
+ * (MCTDH.SRC/walks.f90:149-759) and hops (walks.f90:761-993) do for a full CI of
+ * numelec electrons in nspf orbitals at 2*M_s = restrictms (restrictflag=1,
+ * numshells=1, holeflag=0, single rank).  nthreads <= 0: all host cores. */
+int sincgpu_walks_create(sincgpu_walks** walks, int numelec, int nspf, int restrictms, int nthreads);
+int sincgpu_walks_destroy(sincgpu_walks* walks);
+/* sizes[0..5] = numconfig, numpart, total single walks, total double walks,
+ * total single hops, total double hops. */
+int sincgpu_walks_sizes(sincgpu_walks* walks, long long* sizes, int nsizes);
+
+/* Copies one table as int32, 1-based values as in the reference:
+ *   CONFIGLIST        configlist(2*numpart, numconfig)
+ *   NUMSINGLEWALKS    (numconfig)          NUMDOUBLEWALKS (numconfig)
+ *   SINGLEWALKOPSPF   (2, totsingle)       SINGLEWALKDIRPHASE, SINGLEWALK (totsingle)
+ *   DOUBLEWALKDIRSPF  (4, totdouble)       DOUBLEWALKDIRPHASE, DOUBLEWALK (totdouble)
+ *   SINGLEHOPOFF      (numconfig+1) CSR offsets into the flat hop arrays (0-based)
+ *   SINGLEHOP, SINGLEHOPWALKSTART, SINGLEHOPWALKEND (totsinglehops), likewise DOUBLE*
+ *   SINGLEDIAGHOP, DOUBLEDIAGHOP (numconfig): 1-based hop of config1 itself, -1 if none */
+#define SINCGPU_T_CONFIGLIST 0
+#define SINCGPU_T_NUMSINGLEWALKS 1
+#define SINCGPU_T_NUMDOUBLEWALKS 2
+#define SINCGPU_T_SINGLEWALKOPSPF 3
+#define SINCGPU_T_SINGLEWALKDIRPHASE 4
+#define SINCGPU_T_SINGLEWALK 5
+#define SINCGPU_T_DOUBLEWALKDIRSPF 6
+#define SINCGPU_T_DOUBLEWALKDIRPHASE 7
+#define SINCGPU_T_DOUBLEWALK 8
+#define SINCGPU_T_SINGLEHOPOFF 9
+#define SINCGPU_T_SINGLEHOP 10
+#define SINCGPU_T_SINGLEHOPWALKSTART 11
+#define SINCGPU_T_SINGLEHOPWALKEND 12
+#define SINCGPU_T_DOUBLEHOPOFF 13
+#define SINCGPU_T_DOUBLEHOP 14
+#define SINCGPU_T_DOUBLEHOPWALKSTART 15
+#define SINCGPU_T_DOUBLEHOPWALKEND 16
+#define SINCGPU_T_SINGLEDIAGHOP 17
+#define SINCGPU_T_DOUBLEDIAGHOP 18
+int sincgpu_walks_table(sincgpu_walks* walks, int which, int* out);
+
+/* Uploads the tables to the context's device (walk_init after hops in
+ * MCTDH.SRC/mctdhf.f90:837-853).  The walks handle may be destroyed afterwards. */
+int sincgpu_ci_attach(sincgpu_ctx* ctx, sincgpu_walks* walks);
+
+/* getdenmatstuff (MCTDH.SRC/denmat.f90:312-378): denmat(n,n) from the A-vector
+ * (getdenmat00, 177-274) and its regularised inverse invmatsmooth(denmat, denreg)
+ * (MCTDH.SRC/utils.f90:533-611, denreg 1e-10).  invdenmat may be NULL. */
+int sincgpu_getdenmat(sincgpu_ctx* ctx, const double* avector, double* denmat, double* invdenmat);
+/* get_tworeducedx (MCTDH.SRC/mean.f90:14-152): reducedpottally(n,n,n,n). */
+int sincgpu_get_tworeducedx(sincgpu_ctx* ctx, const double* avector1, const double* avector2,
+                            double* reducedpottally);
+/* One-body matrix elements <phi_i|op|phi_j>: potential (pot_matel, MCTDH.SRC/matel.f90:113-169),
+ * kinetic (sparseops_matel, 241-293) and z (pulse_matel zz, 173-238). */
+int sincgpu_onebody_matel(sincgpu_ctx* ctx, const double* phi, double* potmatel, double* kematel,
+                          double* zmatel);
+/* assemble_sparsemats (MCTDH.SRC/matel.f90:674-729; doubles 393-475): per
+ * (config, hop) sums of the matrix elements over the hop's walks. */
+int sincgpu_assemble_sparsemats(sincgpu_ctx* ctx, const double* twoematel, const double* potmatel,
+                                const double* kematel, const double* zmatel);
+/* sparseconfigmult with sparseopt=1 (MCTDH.SRC/walkmult.f90:735-907, boflag=1,
+ * numr=1): out = nucrepulsion*in + doubles + one-body singles, plus with a
+ * length-gauge z field ezfield: ezfield*(z singles + nuclear dipole*in). */
+int sincgpu_sparseconfigmult(sincgpu_ctx* ctx, const double* invector, double* outvector, double ezfield);
+
+/* Device forms of the above.  mats = [potmatel | kematel | zmatel] (3*n*n complex). */
+int sincgpu_getdenmat_dev(sincgpu_ctx* ctx, const double* avector, double* denmat, double* invdenmat,
+                          double denreg);
+int sincgpu_get_tworeducedx_dev(sincgpu_ctx* ctx, const double* avector1, const double* avector2,
+                                double* reducedpottally);
+int sincgpu_onebody_matel_dev(sincgpu_ctx* ctx, const double* phi, double* mats);
+int sincgpu_assemble_sparsemats_dev(sincgpu_ctx* ctx, const double* twoematel, const double* mats);
+int sincgpu_sparseconfigmult_dev(sincgpu_ctx* ctx, const double* invector, double* outvector,
+                                 double ezfield);
+
+/* One orbital-RHS evaluation from the A-vector: denmat, invdenmat and the 2-RDM
+ * (get_allden, MCTDH.SRC/mean.f90:467-477), then sincgpu_orbital_rhs_dev. */
+int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* ctx, const double* phi, const double* avector,
+                                 double timefac_re, double timefac_im, double ztdpot, double* denmat,
+                                 double* invdenmat, double* reducedpottally, double* twoematel,
+                                 double* reducedpot, double* outspfs);
+
+/* Host-array form: orbitals and A-vector in, orbital RHS out; the mean fields stay
+ * on the device.  This is the call a Fortran driver makes per RHS evaluation when
+ * it keeps the GPU state between calls. */
+int sincgpu_orbital_rhs_avec(sincgpu_ctx* ctx, const double* phi, const double* avector,
+                             double timefac_re, double timefac_im, double ztdpot, double* outspfs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,75 @@
+"""Walk tables: the library's C++ tables must equal the oracle's restatement of
+the reference bit for bit (integer indices, phases, order), and match closed-form
+counts.  Host code only: runs without a GPU."""
+from math import comb
+
+import numpy as np
+import pytest
+
+from oracle.walks_oracle import CIWalks, ci_count
+
+TABLES = ["configlist", "numsinglewalks", "numdoublewalks", "singlewalkopspf", "singlewalkdirphase",
+          "singlewalk", "doublewalkdirspf", "doublewalkdirphase", "doublewalk", "singlehop_off",
+          "singlehop", "singlehopwalkstart", "singlehopwalkend", "doublehop_off", "doublehop",
+          "doublehopwalkstart", "doublehopwalkend", "singlediaghop", "doublediaghop"]
+
+
+@pytest.mark.parametrize("numelec,nspf,ms", [(1, 4, 1), (2, 5, 0), (2, 10, 0), (3, 4, 1), (3, 6, -1),
+                                             (4, 5, 0), (4, 6, 2), (4, 7, 0), (5, 5, 1), (6, 6, 0)])
+def test_tables_bit_exact(built_lib, numelec, nspf, ms):
+    from sincgpu import WalkTables
+    o = CIWalks(numelec, nspf, ms)
+    w = WalkTables(numelec, nspf, ms, nthreads=3)
+    try:
+        for name in TABLES:
+            a = np.asarray(getattr(o, name))
+            b = w.table(name)
+            assert a.shape == b.shape, name
+            assert np.array_equal(a, b), name
+    finally:
+        w.close()
+
+
+def test_thread_count_does_not_change_tables(built_lib):
+    from sincgpu import WalkTables
+    w1 = WalkTables(4, 8, 0, nthreads=1)
+    w2 = WalkTables(4, 8, 0, nthreads=7)
+    for name in TABLES:
+        assert np.array_equal(w1.table(name), w2.table(name)), name
+
+
+def test_closed_form_counts_large(built_lib):
+    """4 electrons, 16 orbitals, M_s=0: per configuration 60 single walks,
+    2*C(16,2)... i.e. 1380 double walks and 1023 double hops."""
+    from sincgpu import WalkTables
+    w = WalkTables(4, 16, 0)
+    assert w.numconfig == ci_count(4, 16, 0) == comb(16, 2) ** 2 == 14400
+    assert w.totsinglewalks == 60 * 14400
+    assert w.totdoublewalks == 1380 * 14400
+    assert w.totdoublehops == 1023 * 14400
+    nsw = w.table("numsinglewalks")
+    assert np.all(nsw == 60)
+
+
+def test_walk_invariants(built_lib):
+    """Every walk's target exists, phases are +-1, and each config's diagonal hop
+    (if any) points back at itself."""
+    from sincgpu import WalkTables
+    w = WalkTables(4, 7, 0)
+    for name in ("singlewalk", "doublewalk"):
+        t = w.table(name)
+        assert t.min() >= 1 and t.max() <= w.numconfig
+    for name in ("singlewalkdirphase", "doublewalkdirphase"):
+        assert set(np.unique(w.table(name))) <= {-1, 1}
+    off = w.table("doublehop_off")
+    hop = w.table("doublehop")
+    diag = w.table("doubledaghop") if False else w.table("doublediaghop")
+    for c in range(w.numconfig):
+        if diag[c] > 0:
+            assert hop[off[c] + diag[c] - 1] == c + 1
+
+
+def test_bad_spin_projection_rejected(built_lib):
+    from sincgpu import WalkTables, SincGpuError
+    with pytest.raises(SincGpuError):
+        WalkTables(4, 6, 1)   # 4 electrons cannot have 2*M_s = 1

@@ -7,10 +7,6 @@
 #include "context.hpp"
 #include "../../include/sincgpu.h"
 
-struct sincgpu_ctx {
-  sincgpu::Ctx c;
-};
-
 namespace sincgpu {
 
 static thread_local char g_err[512] = "";
@@ -63,6 +59,9 @@ Ctx::~Ctx() {
   ws_red.release();
   ws_conv.release();
   ws_state.release();
+  ws_ci.release();
+  ws_ci2.release();
+  ci.release();
   if (stream && own_stream) cudaStreamDestroy(stream);
 }
 
@@ -106,15 +105,6 @@ static int twoe_core(Ctx& c, const double2* phi1, const double2* phi2, double2* 
 }  // namespace sincgpu
 
 using namespace sincgpu;
-
-#define CTX_CHECK(ctx)                                                                   \
-  do {                                                                                   \
-    if (!(ctx)) {                                                                        \
-      set_error("null context");                                                         \
-      return SINCGPU_EINVAL;                                                             \
-    }                                                                                    \
-    SG_CUDA(cudaSetDevice((ctx)->c.device));                                             \
-  } while (0)
 
 extern "C" {
 

@@ -1,0 +1,280 @@
+// C ABI of the CI side: walk tables, RDMs, one-body matrix elements, assembled
+// sparse matrices and the sigma product (declarations: include/sincgpu.h).
+#include <cstring>
+#include <vector>
+#include "context.hpp"
+#include "walks.hpp"
+#include "../../include/sincgpu.h"
+
+struct sincgpu_walks {
+  sincgpu::Walks w;
+};
+
+using namespace sincgpu;
+
+namespace {
+
+int up(Ctx& c, void* dst, const void* src, size_t bytes) {
+  SG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c.stream));
+  return SINCGPU_OK;
+}
+int down(Ctx& c, void* dst, const void* src, size_t bytes) {
+  SG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c.stream));
+  return SINCGPU_OK;
+}
+
+double nucdip_z(const Ctx& c) {  // nucdipvalue (SINCDVR/init_sinc_new.f90:652-662), z component
+  double d = 0.0;
+  for (int i = 0; i < c.numcenters; ++i) d += c.nuccharges[i] * c.centershift[3 * i + 2] / 2.0 * c.spacing;
+  return d;
+}
+
+template <class T>
+void copy_out(const std::vector<T>& v, int* out) {
+  for (size_t i = 0; i < v.size(); ++i) out[i] = (int)v[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+int sincgpu_walks_create(sincgpu_walks** out, int numelec, int nspf, int restrictms, int nthreads) {
+  SG_CHECK(out, SINCGPU_EINVAL, "null output pointer");
+  *out = nullptr;
+  sincgpu_walks* h = new sincgpu_walks();
+  int rc = build_walks(h->w, numelec, nspf, restrictms, nthreads);
+  if (rc != SINCGPU_OK) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return SINCGPU_OK;
+}
+
+int sincgpu_walks_destroy(sincgpu_walks* h) {
+  delete h;
+  return SINCGPU_OK;
+}
+
+int sincgpu_walks_sizes(sincgpu_walks* h, long long* s, int n) {
+  SG_CHECK(h && s, SINCGPU_EINVAL, "null argument");
+  const Walks& w = h->w;
+  long long v[6] = {w.numconfig, w.numpart, w.scol.back(), w.dcol.back(), (long long)w.singlehop.size(),
+                    (long long)w.doublehop.size()};
+  for (int i = 0; i < n && i < 6; ++i) s[i] = v[i];
+  return SINCGPU_OK;
+}
+
+int sincgpu_walks_table(sincgpu_walks* h, int which, int* out) {
+  SG_CHECK(h && out, SINCGPU_EINVAL, "null argument");
+  const Walks& w = h->w;
+  switch (which) {
+    case SINCGPU_T_CONFIGLIST: copy_out(w.configlist, out); break;
+    case SINCGPU_T_NUMSINGLEWALKS: copy_out(w.numsinglewalks, out); break;
+    case SINCGPU_T_NUMDOUBLEWALKS: copy_out(w.numdoublewalks, out); break;
+    case SINCGPU_T_SINGLEWALKOPSPF: copy_out(w.singlewalkopspf, out); break;
+    case SINCGPU_T_SINGLEWALKDIRPHASE: copy_out(w.singlewalkdirphase, out); break;
+    case SINCGPU_T_SINGLEWALK: copy_out(w.singlewalk, out); break;
+    case SINCGPU_T_DOUBLEWALKDIRSPF: copy_out(w.doublewalkdirspf, out); break;
+    case SINCGPU_T_DOUBLEWALKDIRPHASE: copy_out(w.doublewalkdirphase, out); break;
+    case SINCGPU_T_DOUBLEWALK: copy_out(w.doublewalk, out); break;
+    case SINCGPU_T_SINGLEHOPOFF: copy_out(w.singlehop_off, out); break;
+    case SINCGPU_T_SINGLEHOP: copy_out(w.singlehop, out); break;
+    case SINCGPU_T_SINGLEHOPWALKSTART: copy_out(w.singlehopwalkstart, out); break;
+    case SINCGPU_T_SINGLEHOPWALKEND: copy_out(w.singlehopwalkend, out); break;
+    case SINCGPU_T_DOUBLEHOPOFF: copy_out(w.doublehop_off, out); break;
+    case SINCGPU_T_DOUBLEHOP: copy_out(w.doublehop, out); break;
+    case SINCGPU_T_DOUBLEHOPWALKSTART: copy_out(w.doublehopwalkstart, out); break;
+    case SINCGPU_T_DOUBLEHOPWALKEND: copy_out(w.doublehopwalkend, out); break;
+    case SINCGPU_T_SINGLEDIAGHOP: copy_out(w.singlediaghop, out); break;
+    case SINCGPU_T_DOUBLEDIAGHOP: copy_out(w.doublediaghop, out); break;
+    default:
+      set_error("unknown walk table id %d", which);
+      return SINCGPU_EINVAL;
+  }
+  return SINCGPU_OK;
+}
+
+int sincgpu_ci_attach(sincgpu_ctx* h, sincgpu_walks* w) {
+  CTX_CHECK(h);
+  SG_CHECK(w, SINCGPU_EINVAL, "null walk tables");
+  return ci_attach(h->c, w->w);
+}
+
+// ----------------------------------------------------------------- device forms
+int sincgpu_getdenmat_dev(sincgpu_ctx* h, const double* avector, double* denmat, double* invdenmat,
+                          double denreg) {
+  CTX_CHECK(h);
+  SG_CHECK(avector && denmat, SINCGPU_EINVAL, "null argument");
+  return ci_denmat(h->c, (const double2*)avector, (double2*)denmat, (double2*)invdenmat, denreg);
+}
+
+int sincgpu_get_tworeducedx_dev(sincgpu_ctx* h, const double* a1, const double* a2, double* tally) {
+  CTX_CHECK(h);
+  SG_CHECK(a1 && tally, SINCGPU_EINVAL, "null argument");
+  return ci_tally(h->c, (const double2*)a1, (const double2*)(a2 ? a2 : a1), (double2*)tally);
+}
+
+int sincgpu_onebody_matel_dev(sincgpu_ctx* h, const double* phi, double* mats) {
+  CTX_CHECK(h);
+  SG_CHECK(phi && mats, SINCGPU_EINVAL, "null argument");
+  return ci_onebody(h->c, (const double2*)phi, (double2*)mats);
+}
+
+int sincgpu_assemble_sparsemats_dev(sincgpu_ctx* h, const double* twoematel, const double* mats) {
+  CTX_CHECK(h);
+  SG_CHECK(twoematel && mats, SINCGPU_EINVAL, "null argument");
+  return ci_assemble(h->c, (const double2*)twoematel, (const double2*)mats);
+}
+
+int sincgpu_sparseconfigmult_dev(sincgpu_ctx* h, const double* in, double* out, double ezfield) {
+  CTX_CHECK(h);
+  SG_CHECK(in && out && in != out, SINCGPU_EINVAL, "in/out must be distinct, non-null");
+  return ci_sigma(h->c, (const double2*)in, (double2*)out, h->c.nucrepulsion, ezfield, nucdip_z(h->c));
+}
+
+int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* h, const double* phi, const double* avector, double tre,
+                                 double tim, double ztdpot, double* denmat, double* invdenmat, double* tally,
+                                 double* twoematel, double* reducedpot, double* out) {
+  CTX_CHECK(h);
+  SG_CHECK(phi && avector && denmat && invdenmat && tally && reducedpot && out, SINCGPU_EINVAL,
+           "null argument");
+  SG_TRY(sincgpu_getdenmat_dev(h, avector, denmat, invdenmat, 1e-10));
+  SG_TRY(sincgpu_get_tworeducedx_dev(h, avector, avector, tally));
+  return sincgpu_orbital_rhs_dev(h, phi, tally, denmat, invdenmat, tre, tim, ztdpot, twoematel, reducedpot,
+                                 out);
+}
+
+// ----------------------------------------------------------------- host forms
+int sincgpu_orbital_rhs_avec(sincgpu_ctx* h, const double* phi, const double* avector, double tre,
+                             double tim, double ztdpot, double* outspfs) {
+  CTX_CHECK(h);
+  Ctx& c = h->c;
+  SG_CHECK(c.ci.attached, SINCGPU_ESTATE, "no walk tables attached");
+  SG_CHECK(phi && avector && outspfs, SINCGPU_EINVAL, "null argument");
+  const int n = c.nspf;
+  const size_t bphi = sizeof(double2) * (size_t)c.G * n, ba = sizeof(double2) * c.ci.nc;
+  const size_t bm = sizeof(double2) * n * n, b4 = sizeof(double2) * (size_t)n * n * n * n;
+  auto pad = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t total = 2 * pad(bphi) + pad(ba) + 2 * pad(bm) + 2 * pad(b4);
+  SG_TRY(c.ws_io.ensure(total));
+  SG_TRY(c.ws_state.ensure(sizeof(double2) * (size_t)c.G * n * n));
+  char* p = (char*)c.ws_io.ptr;
+  double* dphi = (double*)p;
+  p += pad(bphi);
+  double* dout = (double*)p;
+  p += pad(bphi);
+  double* da = (double*)p;
+  p += pad(ba);
+  double* dden = (double*)p;
+  p += pad(bm);
+  double* dinv = (double*)p;
+  p += pad(bm);
+  double* dtal = (double*)p;
+  p += pad(b4);
+  double* dmat = (double*)p;
+  SG_TRY(up(c, dphi, phi, bphi));
+  SG_TRY(up(c, da, avector, ba));
+  SG_TRY(sincgpu_orbital_rhs_avec_dev(h, dphi, da, tre, tim, ztdpot, dden, dinv, dtal, dmat,
+                                      (double*)c.ws_state.ptr, dout));
+  SG_TRY(down(c, outspfs, dout, bphi));
+  SG_CUDA(cudaStreamSynchronize(c.stream));
+  return SINCGPU_OK;
+}
+
+int sincgpu_getdenmat(sincgpu_ctx* h, const double* avector, double* denmat, double* invdenmat) {
+  CTX_CHECK(h);
+  Ctx& c = h->c;
+  SG_CHECK(c.ci.attached, SINCGPU_ESTATE, "no walk tables attached");
+  SG_CHECK(avector && denmat, SINCGPU_EINVAL, "null argument");
+  const int n = c.nspf;
+  const size_t ba = sizeof(double2) * c.ci.nc, bm = sizeof(double2) * n * n;
+  SG_TRY(c.ws_io.ensure(ba + 2 * bm + 512));
+  char* base = (char*)c.ws_io.ptr;
+  double2* da = (double2*)base;
+  double2* dd = (double2*)(base + (ba + 255) / 256 * 256);
+  double2* di = dd + n * n;
+  SG_TRY(up(c, da, avector, ba));
+  SG_TRY(ci_denmat(c, da, dd, invdenmat ? di : nullptr, 1e-10));
+  SG_TRY(down(c, denmat, dd, bm));
+  if (invdenmat) SG_TRY(down(c, invdenmat, di, bm));
+  SG_CUDA(cudaStreamSynchronize(c.stream));
+  return SINCGPU_OK;
+}
+
+int sincgpu_get_tworeducedx(sincgpu_ctx* h, const double* a1, const double* a2, double* tally) {
+  CTX_CHECK(h);
+  Ctx& c = h->c;
+  SG_CHECK(c.ci.attached, SINCGPU_ESTATE, "no walk tables attached");
+  SG_CHECK(a1 && tally, SINCGPU_EINVAL, "null argument");
+  const int n = c.nspf;
+  const size_t ba = sizeof(double2) * c.ci.nc, bt = sizeof(double2) * (size_t)n * n * n * n;
+  const size_t pa = (ba + 255) / 256 * 256;
+  SG_TRY(c.ws_io.ensure(2 * pa + bt));
+  char* base = (char*)c.ws_io.ptr;
+  double2* d1 = (double2*)base;
+  double2* d2 = (double2*)(base + pa);
+  double2* dt = (double2*)(base + 2 * pa);
+  SG_TRY(up(c, d1, a1, ba));
+  if (a2 && a2 != a1) SG_TRY(up(c, d2, a2, ba));
+  SG_TRY(ci_tally(c, d1, (a2 && a2 != a1) ? d2 : d1, dt));
+  SG_TRY(down(c, tally, dt, bt));
+  SG_CUDA(cudaStreamSynchronize(c.stream));
+  return SINCGPU_OK;
+}
+
+int sincgpu_onebody_matel(sincgpu_ctx* h, const double* phi, double* potmatel, double* kematel,
+                          double* zmatel) {
+  CTX_CHECK(h);
+  Ctx& c = h->c;
+  SG_CHECK(phi && potmatel && kematel && zmatel, SINCGPU_EINVAL, "null argument");
+  const int n = c.nspf;
+  const size_t bphi = sizeof(double2) * (size_t)c.G * n, bm = sizeof(double2) * n * n;
+  SG_TRY(c.ws_io.ensure(bphi + 3 * bm + 256));
+  double2* dp = (double2*)c.ws_io.ptr;
+  double2* dm = dp + (size_t)c.G * n;
+  SG_TRY(up(c, dp, phi, bphi));
+  SG_TRY(ci_onebody(c, dp, dm));
+  SG_TRY(down(c, potmatel, dm, bm));
+  SG_TRY(down(c, kematel, dm + n * n, bm));
+  SG_TRY(down(c, zmatel, dm + 2 * n * n, bm));
+  SG_CUDA(cudaStreamSynchronize(c.stream));
+  return SINCGPU_OK;
+}
+
+int sincgpu_assemble_sparsemats(sincgpu_ctx* h, const double* twoematel, const double* potmatel,
+                                const double* kematel, const double* zmatel) {
+  CTX_CHECK(h);
+  Ctx& c = h->c;
+  SG_CHECK(twoematel && potmatel && kematel && zmatel, SINCGPU_EINVAL, "null argument");
+  const int n = c.nspf;
+  const size_t b4 = sizeof(double2) * (size_t)n * n * n * n, bm = sizeof(double2) * n * n;
+  SG_TRY(c.ws_io.ensure(b4 + 3 * bm + 256));
+  double2* dt = (double2*)c.ws_io.ptr;
+  double2* dm = dt + (size_t)n * n * n * n;
+  SG_TRY(up(c, dt, twoematel, b4));
+  SG_TRY(up(c, dm, potmatel, bm));
+  SG_TRY(up(c, dm + n * n, kematel, bm));
+  SG_TRY(up(c, dm + 2 * n * n, zmatel, bm));
+  SG_TRY(ci_assemble(c, dt, dm));
+  SG_CUDA(cudaStreamSynchronize(c.stream));
+  return SINCGPU_OK;
+}
+
+int sincgpu_sparseconfigmult(sincgpu_ctx* h, const double* in, double* out, double ezfield) {
+  CTX_CHECK(h);
+  Ctx& c = h->c;
+  SG_CHECK(c.ci.attached, SINCGPU_ESTATE, "no walk tables attached");
+  SG_CHECK(in && out, SINCGPU_EINVAL, "null argument");
+  const size_t ba = sizeof(double2) * c.ci.nc, pa = (ba + 255) / 256 * 256;
+  SG_TRY(c.ws_io.ensure(2 * pa));
+  double2* di = (double2*)c.ws_io.ptr;
+  double2* dout = (double2*)((char*)c.ws_io.ptr + pa);
+  SG_TRY(up(c, di, in, ba));
+  SG_TRY(ci_sigma(c, di, dout, c.nucrepulsion, ezfield, nucdip_z(c)));
+  SG_TRY(down(c, out, dout, ba));
+  SG_CUDA(cudaStreamSynchronize(c.stream));
+  return SINCGPU_OK;
+}
+
+}  // extern "C"

@@ -30,6 +30,22 @@ struct Prof {
   long long launches[ST_COUNT] = {};
 };
 
+// Device copies of the walk tables (ci.cu).
+struct CIState {
+  bool attached = false, assembled = false;
+  int nc = 0;
+  long long nsh = 0, ndh = 0;              // single / double hops (all configs)
+  long long *den_off = nullptr, *tal_off = nullptr;
+  int2 *den_ent = nullptr, *tal_ent = nullptr;  // (config1, +-config2) per RDM element
+  int *sidx = nullptr, *didx = nullptr;     // packed matrix index, sign = phase
+  long long *swb = nullptr, *dwb = nullptr; // first walk of each hop
+  int *swn = nullptr, *dwn = nullptr;       // walks in each hop
+  int *shop = nullptr, *dhop = nullptr;     // hop target config (0-based)
+  long long *shop_off = nullptr, *dhop_off = nullptr;  // hops of each config
+  double2 *xpot = nullptr, *xone = nullptr, *xz = nullptr;  // assembled per-hop values
+  void release();
+};
+
 struct Ctx {
   // ---- problem parameters -------------------------------------------------
   int N = 0;             // points per axis (numpoints == gridpoints, nbox=1)
@@ -68,6 +84,8 @@ struct Ctx {
   Workspace ws_red;     // planar reduced potentials of the last build
   Workspace ws_conv;    // layout conversion scratch
   Workspace ws_state;   // resident mean-field state of the fused orbital-RHS entry
+  Workspace ws_ci, ws_ci2;  // CI scratch (KE phi + partials; summed one-body matrix)
+  CIState ci;
   int coul_chunk = 0;   // pairs per pass sequence (0 = automatic)
   Prof prof;
 
@@ -120,6 +138,15 @@ int reduced_pot_full(Ctx& c, const double2* twoereduced, const double2* tally, d
 // ke.cu: out = KE(in) [+ pot*in + zfield*z*in when `extra`]
 int mult_ke(Ctx& c, const double2* in, double2* out, int howmany, bool extra, double zfield);
 
+// ci.cu (walk tables: walks.hpp)
+struct Walks;
+int ci_attach(Ctx& c, const Walks& w);
+int ci_denmat(Ctx& c, const double2* avec, double2* denmat, double2* invdenmat, double denreg);
+int ci_tally(Ctx& c, const double2* a1, const double2* a2, double2* tally);
+int ci_onebody(Ctx& c, const double2* phi, double2* mats);
+int ci_assemble(Ctx& c, const double2* twoematel, const double2* mats);
+int ci_sigma(Ctx& c, const double2* in, double2* out, double constant, double ez, double nucdipz);
+
 // rhs.cu
 int mult_reducedpot(Ctx& c, const double2* phi, const double2* redpot, double2* out);
 // orbitals [i0, i0+ni) only; redpot/out hold just that window
@@ -130,3 +157,17 @@ int actreduced(Ctx& c, const double2* phi, const double2* proj, const double2* d
                int dentimeflag, int projflag, double zfield, double2* out);
 
 }  // namespace sincgpu
+
+// Opaque handle of the C ABI.
+struct sincgpu_ctx {
+  sincgpu::Ctx c;
+};
+
+#define CTX_CHECK(ctx)                                                                   \
+  do {                                                                                   \
+    if (!(ctx)) {                                                                        \
+      ::sincgpu::set_error("null context");                                              \
+      return SINCGPU_EINVAL;                                                             \
+    }                                                                                    \
+    SG_CUDA(cudaSetDevice((ctx)->c.device));                                             \
+  } while (0)

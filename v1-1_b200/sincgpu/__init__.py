@@ -14,3 +14,4 @@ from .capi import (  # noqa: F401
     library_path,
     exported_symbols,
 )
+from .walks import WalkTables  # noqa: F401,E402

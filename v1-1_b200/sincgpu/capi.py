@@ -55,6 +55,23 @@ _SIGS = {
     "sincgpu_actreduced_dev": ([_P, _I, _P, _P, _P, _P, _P, _D, _D, _I, _D, _P], _I),
     "sincgpu_set_stream": ([_P, _P], _I),
     "sincgpu_launch_count": ([], _LL),
+    "sincgpu_walks_create": ([C.POINTER(_P), _I, _I, _I, _I], _I),
+    "sincgpu_walks_destroy": ([_P], _I),
+    "sincgpu_walks_sizes": ([_P, _P, _I], _I),
+    "sincgpu_walks_table": ([_P, _I, _P], _I),
+    "sincgpu_ci_attach": ([_P, _P], _I),
+    "sincgpu_getdenmat": ([_P, _P, _P, _P], _I),
+    "sincgpu_get_tworeducedx": ([_P, _P, _P, _P], _I),
+    "sincgpu_onebody_matel": ([_P, _P, _P, _P, _P], _I),
+    "sincgpu_assemble_sparsemats": ([_P, _P, _P, _P, _P], _I),
+    "sincgpu_sparseconfigmult": ([_P, _P, _P, _D], _I),
+    "sincgpu_getdenmat_dev": ([_P, _P, _P, _P, _D], _I),
+    "sincgpu_get_tworeducedx_dev": ([_P, _P, _P, _P], _I),
+    "sincgpu_onebody_matel_dev": ([_P, _P, _P], _I),
+    "sincgpu_assemble_sparsemats_dev": ([_P, _P, _P], _I),
+    "sincgpu_sparseconfigmult_dev": ([_P, _P, _P, _D], _I),
+    "sincgpu_orbital_rhs_avec_dev": ([_P, _P, _P, _D, _D, _D, _P, _P, _P, _P, _P, _P], _I),
+    "sincgpu_orbital_rhs_avec": ([_P, _P, _P, _D, _D, _D, _P], _I),
     "sincgpu_profile": ([_P, _I], _I),
     "sincgpu_profile_read": ([_P, _P, _P, _I], _I),
     "sincgpu_orbital_rhs_dev": ([_P, _P, _P, _P, _P, _D, _D, _D, _P, _P, _P], _I),
@@ -264,6 +281,81 @@ class SincProject:
         _call("sincgpu_actreduced00", self._h, int(dentimeflag), _ptr(phi), _ptr(proj), _ptr(dm),
               _ptr(inv), _ptr(v), tf.real, tf.imag, int(projflag), float(ztdpot), _ptr(out))
         return out
+
+    # ------------------------------------------------------------ CI side
+    def ci_attach(self, walks):
+        """Uploads the walk tables (sincgpu.WalkTables) to this context's device."""
+        _call("sincgpu_ci_attach", self._h, walks._h)
+        self.numconfig = walks.numconfig
+
+    def getdenmat(self, avector):
+        """MCTDH.SRC/denmat.f90:312-378 -> (denmat(n,n), invdenmat(n,n))."""
+        n = self.nspf
+        a = _f(avector).reshape(-1)
+        den = np.zeros((n, n), dtype=np.complex128, order="F")
+        inv = np.zeros((n, n), dtype=np.complex128, order="F")
+        _call("sincgpu_getdenmat", self._h, _ptr(a), _ptr(den), _ptr(inv))
+        return den, inv
+
+    def get_tworeducedx(self, avector1, avector2=None):
+        """MCTDH.SRC/mean.f90:14-152 -> reducedpottally(n,n,n,n)."""
+        n = self.nspf
+        a1 = _f(avector1).reshape(-1)
+        a2 = a1 if avector2 is None else _f(avector2).reshape(-1)
+        t = np.zeros((n, n, n, n), dtype=np.complex128, order="F")
+        _call("sincgpu_get_tworeducedx", self._h, _ptr(a1), _ptr(a2), _ptr(t))
+        return t
+
+    def onebody_matel(self, phi):
+        """(potmatel, kematel, zmatel), each <phi_i|op|phi_j> (n,n)."""
+        n = self.nspf
+        p = _f(phi)
+        mats = [np.zeros((n, n), dtype=np.complex128, order="F") for _ in range(3)]
+        _call("sincgpu_onebody_matel", self._h, _ptr(p), *(_ptr(m) for m in mats))
+        return tuple(mats)
+
+    def assemble_sparsemats(self, twoematel, potmatel, kematel, zmatel):
+        # keep the converted arrays alive until the call returns
+        arrs = [_f(twoematel), _f(potmatel), _f(kematel), _f(zmatel)]
+        _call("sincgpu_assemble_sparsemats", self._h, *(_ptr(a) for a in arrs))
+
+    def sparseconfigmult(self, invector, ezfield=0.0):
+        """MCTDH.SRC/walkmult.f90:735-907 (sparseopt=1)."""
+        a = _f(invector).reshape(-1)
+        out = np.zeros_like(a)
+        _call("sincgpu_sparseconfigmult", self._h, _ptr(a), _ptr(out), float(ezfield))
+        return out
+
+    def getdenmat_dev(self, avector, denmat, invdenmat, denreg=1e-10):
+        _call("sincgpu_getdenmat_dev", self._h, _ptr(avector), _ptr(denmat), _ptr(invdenmat), float(denreg))
+
+    def get_tworeducedx_dev(self, avector1, avector2, tally):
+        _call("sincgpu_get_tworeducedx_dev", self._h, _ptr(avector1), _ptr(avector2), _ptr(tally))
+
+    def onebody_matel_dev(self, phi, mats):
+        _call("sincgpu_onebody_matel_dev", self._h, _ptr(phi), _ptr(mats))
+
+    def assemble_sparsemats_dev(self, twoematel, mats):
+        _call("sincgpu_assemble_sparsemats_dev", self._h, _ptr(twoematel), _ptr(mats))
+
+    def sparseconfigmult_dev(self, invector, outvector, ezfield=0.0):
+        _call("sincgpu_sparseconfigmult_dev", self._h, _ptr(invector), _ptr(outvector), float(ezfield))
+
+    def orbital_rhs_avec(self, phi, avector, timefac=-1j, ztdpot=0.0):
+        """Host arrays: orbitals (G,n) and A-vector in, orbital RHS (G,n) out."""
+        p = _f(phi)
+        a = _f(avector).reshape(-1)
+        out = np.zeros((self.G, self.nspf), dtype=np.complex128, order="F")
+        tf = complex(timefac)
+        _call("sincgpu_orbital_rhs_avec", self._h, _ptr(p), _ptr(a), tf.real, tf.imag, float(ztdpot), _ptr(out))
+        return out
+
+    def orbital_rhs_avec_dev(self, phi, avector, denmat, invdenmat, tally, twoematel, reducedpot, out,
+                             timefac=-1j, ztdpot=0.0):
+        tf = complex(timefac)
+        _call("sincgpu_orbital_rhs_avec_dev", self._h, _ptr(phi), _ptr(avector), tf.real, tf.imag,
+              float(ztdpot), _ptr(denmat), _ptr(invdenmat), _ptr(tally), _ptr(twoematel),
+              _ptr(reducedpot), _ptr(out))
 
     # --------------------------------------------------- device-resident
     def twoe_matel_dev(self, phi1, phi2, twoematel, twoereduced=None):
