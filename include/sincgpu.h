@@ -151,6 +151,21 @@ int sincgpu_mult_reducedpot_dev(sincgpu_ctx* ctx, const double* inspfs, double* 
  * twoematel and reducedpot (MCTDH.SRC/matel.f90:72-111 + mean.f90:484-590). */
 int sincgpu_mean_field_dev(sincgpu_ctx* ctx, const double* phi, const double* reducedpottally,
                            double* twoematel, double* reducedpot);
+
+/* Allocation-free op_tinv; no counterpart in the reference.  For callers that
+ * cannot call cudaMalloc when they need the solve (a process whose device memory
+ * is partitioned once at start-up, a latency-critical loop that cannot accept
+ * the synchronisation cudaMalloc/cudaFree may cause).  Same result as
+ * sincgpu_op_tinv, on DEVICE arrays twoeden03(totpoints,allsize) ->
+ * twoereduced(totpoints,allsize), enqueued on the context stream.  The FFT
+ * scratch is a fixed 64 MiB device array inside the library (held on every GPU
+ * that loads it until exit); one density needs 16*(N*N*P + N*P*P) bytes of it
+ * (P = sincgpu_fft_length) and larger grids are rejected with SINCGPU_ERANGE.
+ * All calls share the array: calls that overlap on the GPU race.  The first
+ * call on a device looks up the array's address; make it before any stream
+ * capture. */
+int sincgpu_op_tinv_noalloc_dev(sincgpu_ctx* ctx, const double* twoeden03, double* twoereduced,
+                                int allsize);
 int sincgpu_actreduced_dev(sincgpu_ctx* ctx, int dentimeflag, const double* inspfs,
                            const double* projspfs, const double* denmat, const double* invdenmat,
                            const double* reducedpot, double timefac_re, double timefac_im,

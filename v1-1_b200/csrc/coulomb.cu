@@ -99,4 +99,33 @@ int coulomb_dens(Ctx& c, const double2* dens, int m, double2* red) {
   return coul_run(c, dens, nullptr, nullptr, nullptr, m, nullptr, red, false, true);
 }
 
+// op_tinv on explicit densities with caller-provided scratch: no allocation.
+// The densities are processed in chunks that fit `scratch_bytes`.
+int coulomb_dens_scratch(Ctx& c, const double2* dens, int m, double2* red, double2* scratch,
+                         size_t scratch_bytes) {
+  const int N = c.N, P = c.P;
+  const size_t per_dens = 16ull * ((size_t)N * N * P + (size_t)N * P * P);
+  SG_CHECK(per_dens <= scratch_bytes, SINCGPU_ERANGE,
+           "one density on a %d^3 grid (FFT length %d) needs %zu bytes of scratch; the fixed "
+           "scratch holds %zu bytes", N, P, per_dens, scratch_bytes);
+  const int chunk = (int)std::min<size_t>(scratch_bytes / per_dens, (size_t)m);
+  CoulArgs ca{};
+  ca.N = N;
+  ca.P = P;
+  ca.nspf = c.nspf;
+  ca.G = c.G;
+  ca.roots = c.d_roots;
+  ca.khat = c.d_khat;
+  ca.W1 = scratch;
+  ca.W2 = scratch + (size_t)chunk * N * N * P;
+  ca.npair_total = m;
+  ca.pa = nullptr;
+  ca.pb = nullptr;
+  for (int p0 = 0; p0 < m; p0 += chunk) {
+    ca.pair0 = p0;
+    SG_TRY(coul_dispatch(c, ca, std::min(chunk, m - p0), true, dens, nullptr, nullptr, red, false));
+  }
+  return SINCGPU_OK;
+}
+
 }  // namespace sincgpu

@@ -52,6 +52,7 @@ _SIGS = {
     "sincgpu_mult_ke_dev": ([_P, _P, _P, _I], _I),
     "sincgpu_mult_reducedpot_dev": ([_P, _P, _P, _P], _I),
     "sincgpu_mean_field_dev": ([_P, _P, _P, _P, _P], _I),
+    "sincgpu_op_tinv_noalloc_dev": ([_P, _P, _P, _I], _I),
     "sincgpu_actreduced_dev": ([_P, _I, _P, _P, _P, _P, _P, _D, _D, _I, _D, _P], _I),
     "sincgpu_set_stream": ([_P, _P], _I),
     "sincgpu_launch_count": ([], _LL),
