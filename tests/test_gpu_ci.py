@@ -46,6 +46,23 @@ def test_denmat_and_inverse(setup):
     assert relerr(den @ inv, np.eye(5)) < 1e-10
 
 
+@pytest.mark.parametrize("eps", [0.0, 1e-7])
+def test_regularised_inverse_near_singular(setup, eps):
+    """A nearly single-determinant A-vector leaves orbitals (almost) empty: the
+    density matrix is (nearly) singular and the denreg regularisation of
+    invmatsmooth decides the inverse (MCTDH.SRC/utils.f90:578-591)."""
+    sysm, gpu, ow, phi, a = setup
+    b = np.zeros(ow.numconfig, dtype=np.complex128)
+    b[0] = 1.0
+    b = b + eps * a
+    b /= np.linalg.norm(b)
+    den_ref = ow.getdenmat00(b)
+    inv_ref = orc.invmatsmooth(den_ref)
+    den, inv = gpu.getdenmat(b)
+    assert relerr(den, den_ref) < TOL
+    assert relerr(inv, inv_ref) < 1e-8
+
+
 def test_tworeducedx(setup):
     sysm, gpu, ow, phi, a = setup
     t_ref = ow.get_tworeducedx(a)
