@@ -26,6 +26,16 @@ namespace sincgpu {
 constexpr int BM = 64, BN = 64, BK = 16;
 constexpr int kMaxOrb = 32;
 
+// 8-byte asynchronous global->shared copy (zero-fill when !valid)
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int n = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
 // ---------------------------------------------------------------------------
 // C_part[split][m][n] = sum_{x in split} A(x,m) B(x,n)
 // A(x,m): m <  npair -> Re(phi1_{pa} conj(phi2_{pb}))(x),  m >= npair -> Im
@@ -121,6 +131,119 @@ __global__ void __launch_bounds__(256) twoe_gemm_kernel(const double2* __restric
   }
 }
 
+// twoematel GEMM, 128 (m) x 64 (n) tiles, 8x4 register blocks, split-K over x.
+// The B tile (Rpl rows) and the orbital values of the next k-tile are fetched with
+// cp.async while the current tile is multiplied; the A tile (real/imaginary parts
+// of the pair products) is formed in shared memory from the orbital values.
+constexpr int TM = 128, TN = 64, TK = 16;
+__global__ void __launch_bounds__(256, 2) twoe_gemm2_kernel(const double2* __restrict__ phi1,
+                                                            const double2* __restrict__ phi2,
+                                                            const int* __restrict__ pa,
+                                                            const int* __restrict__ pb,
+                                                            const double* __restrict__ Rpl, int npair,
+                                                            int nspf, long long G, int ntn,
+                                                            long long xper, double* __restrict__ part) {
+  // m-major / n-major tiles padded to TK+1: the fastest thread index walks k in the
+  // writes and rows in the FMA reads, both without bank conflicts
+  __shared__ __align__(16) double As[TM][TK + 1];
+  __shared__ __align__(16) double Bs[2][TN][TK + 1];
+  extern __shared__ __align__(16) double2 fsm[];  // [2 stages][2 sets][nspf][TK]
+  __shared__ int sa[TM], sb[TM], sc[TM];
+  auto f1 = [&](int st, int o, int k) -> double2& { return fsm[((st * 2 + 0) * nspf + o) * TK + k]; };
+  auto f2 = [&](int st, int o, int k) -> double2& { return fsm[((st * 2 + 1) * nspf + o) * TK + k]; };
+  const int M = 2 * npair;
+  const int tm = blockIdx.x / ntn, tn = blockIdx.x % ntn;
+  const int m0 = tm * TM, n0 = tn * TN;
+  const long long xb = blockIdx.y * xper;
+  const long long xe = min(G, xb + xper);
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  for (int i = tid; i < TM; i += 256) {
+    int m = m0 + i;
+    if (m < M) {
+      int p = m % npair;
+      sa[i] = pa[p];
+      sb[i] = pb[p];
+      sc[i] = m / npair;
+    } else {
+      sa[i] = 0;
+      sb[i] = 0;
+      sc[i] = -1;
+    }
+  }
+  auto load = [&](int st, long long x0) {
+    for (int i = tid; i < nspf * TK; i += 256) {
+      int o = i / TK, k = i % TK;
+      long long x = x0 + k;
+      bool ok = x < xe;
+      const double2* g1 = ok ? phi1 + (long long)o * G + x : phi1;
+      const double2* g2 = ok ? phi2 + (long long)o * G + x : phi2;
+      cp_async8(&f1(st, o, k), g1, ok);
+      cp_async8(reinterpret_cast<double*>(&f1(st, o, k)) + 1, reinterpret_cast<const double*>(g1) + 1, ok);
+      cp_async8(&f2(st, o, k), g2, ok);
+      cp_async8(reinterpret_cast<double*>(&f2(st, o, k)) + 1, reinterpret_cast<const double*>(g2) + 1, ok);
+    }
+    for (int i = tid; i < TK * TN; i += 256) {
+      int nn = i / TK, k = i % TK;  // consecutive threads along x
+      int n = n0 + nn;
+      long long x = x0 + k;
+      bool ok = n < M && x < xe;
+      cp_async8(&Bs[st][nn][k], ok ? (const void*)(Rpl + (long long)n * G + x) : (const void*)Rpl, ok);
+    }
+    cp_async_commit();
+  };
+  double acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  const long long nk = (xe - xb + TK - 1) / TK;
+  if (nk > 0) load(0, xb);
+  for (long long t = 0; t < nk; ++t) {
+    const int st = (int)(t & 1);
+    if (t + 1 < nk) {
+      load(st ^ 1, xb + (t + 1) * TK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    for (int i = tid; i < TK * TM; i += 256) {
+      int mm = i / TK, k = i % TK;
+      double v = 0.0;
+      const int comp = sc[mm];
+      if (comp >= 0) {
+        double2 r = cmulc(f1(st, sa[mm], k), f2(st, sb[mm], k));
+        v = comp == 0 ? r.x : r.y;
+      }
+      As[mm][k] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < TK; ++k) {
+      double a[8], b[4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = As[tx + 16 * i][k];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[st][ty + 16 * j][k];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+  double* out = part + (long long)blockIdx.y * M * M;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int m = m0 + tx + 16 * i;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int n = n0 + ty + 16 * j;
+      if (m < M && n < M) out[(long long)m * M + n] = acc[i][j];
+    }
+  }
+}
+
 // C[m][n] = sum_s part[s][m][n] in split order (deterministic)
 __global__ void split_reduce_kernel(const double* __restrict__ part, int nsplit, long long MM,
                                     double* __restrict__ C) {
@@ -183,11 +306,11 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
   const int n = c.nspf;
   SG_CHECK(n <= kMaxOrb, SINCGPU_ERANGE, "at most %d orbitals (got %d)", kMaxOrb, n);
   const int M = 2 * npair;
-  const int ntm = ceil_div(M, BM), ntn = ceil_div(M, BN);
+  const int ntm = ceil_div(M, TM), ntn = ceil_div(M, TN);
   const int ntiles = ntm * ntn;
-  long long target = 4LL * 148;
-  int nsplit = (int)std::max(1LL, std::min((long long)ceil_div(c.G, BK), target / ntiles));
-  long long xper = ((c.G + nsplit - 1) / nsplit + BK - 1) / BK * BK;
+  long long target = 2LL * 148;
+  int nsplit = (int)std::max(1LL, std::min((long long)ceil_div(c.G, TK), target / ntiles));
+  long long xper = ((c.G + nsplit - 1) / nsplit + TK - 1) / TK * TK;
   nsplit = ceil_div(c.G, xper);
   const long long MM = (long long)M * M;
   size_t need = sizeof(double) * (MM * nsplit + MM) + sizeof(int) * (2 * npair + n * n);
@@ -204,8 +327,15 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
   SG_CUDA(cudaMemcpyAsync(d_lut, lut.data(), sizeof(int) * n * n, cudaMemcpyHostToDevice, c.stream));
   {
     ProfScope ps(c, ST_TWOE_GEMM);
-    twoe_gemm_kernel<<<dim3(ntiles, nsplit), 256, 0, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl, npair, n,
-                                                                 c.G, ntn, xper, part);
+    const size_t fbytes = sizeof(double2) * 4 * (size_t)n * TK;
+    static bool attr = false;
+    if (!attr) {
+      SG_CUDA(cudaFuncSetAttribute(twoe_gemm2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(double2) * 4 * kMaxOrb * TK)));
+      attr = true;
+    }
+    twoe_gemm2_kernel<<<dim3(ntiles, nsplit), 256, fbytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl, npair,
+                                                                       n, c.G, ntn, xper, part);
     SG_LAUNCHED();
   }
   ProfScope ps(c, ST_TWOE_FINISH);
@@ -246,6 +376,77 @@ __global__ void build_w_kernel(const double2* __restrict__ tally, const int* __r
   }
   double2 v = comp == 0 ? A : B;
   Wm[idx] = (col & 1) ? v.y : v.x;
+}
+
+// reducedpot GEMM, 128 (x) x 64 (columns) tiles, 8x4 register blocks, two-stage
+// cp.async pipeline over k (pair components).
+constexpr int RM = 128, RN = 64, RK = 16;
+__global__ void __launch_bounds__(256, 2) rp_gemm2_kernel(const double* __restrict__ Rpl,
+                                                       const double* __restrict__ Wm, int K, int NC,
+                                                       long long G, double2* __restrict__ out) {
+  __shared__ __align__(16) double As[2][RK][RM];
+  __shared__ __align__(16) double Bs[2][RK][RN];
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  const long long x0 = (long long)blockIdx.x * RM;
+  const int c0 = blockIdx.y * RN;
+  auto load = [&](int st, int k0) {
+    for (int i = tid; i < RK * RM; i += 256) {
+      int k = i / RM, xx = i % RM;
+      long long x = x0 + xx;
+      bool ok = (k0 + k < K) && x < G;
+      cp_async8(&As[st][k][xx], ok ? (const void*)(Rpl + (long long)(k0 + k) * G + x) : (const void*)Rpl, ok);
+    }
+    for (int i = tid; i < RK * RN; i += 256) {
+      int k = i / RN, cc = i % RN;
+      bool ok = (k0 + k < K) && (c0 + cc < NC);
+      cp_async8(&Bs[st][k][cc], ok ? (const void*)(Wm + (long long)(k0 + k) * NC + c0 + cc) : (const void*)Wm, ok);
+    }
+    cp_async_commit();
+  };
+  double acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  const int nk = (K + RK - 1) / RK;
+  load(0, 0);
+  for (int t = 0; t < nk; ++t) {
+    const int st = t & 1;
+    if (t + 1 < nk) {
+      load(st ^ 1, (t + 1) * RK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < RK; ++k) {
+      double a[8], b[4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = As[st][k][tx + 16 * i];
+      const double2 b01 = *reinterpret_cast<const double2*>(&Bs[st][k][4 * ty]);
+      const double2 b23 = *reinterpret_cast<const double2*>(&Bs[st][k][4 * ty + 2]);
+      b[0] = b01.x;
+      b[1] = b01.y;
+      b[2] = b23.x;
+      b[3] = b23.y;
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const long long x = x0 + tx + 16 * i;
+    if (x >= G) continue;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int col = c0 + 4 * ty + 2 * h;
+      if (col < NC) out[(long long)(col / 2) * G + x] = make_double2(acc[i][2 * h], acc[i][2 * h + 1]);
+    }
+  }
 }
 
 // out[(ki*G + x)] (complex) = sum_k Rpl[k*G+x] * Wm[k][2ki + {0,1}]
@@ -317,9 +518,9 @@ static int reduced_pot_impl(Ctx& c, const double* Rpl, const int* h_pa, const in
                                                                            herm ? 1 : 0, Wm);
     SG_LAUNCHED();
   }
-  dim3 grid(ceil_div(c.G, BM), ceil_div(NC, BN));
+  dim3 grid(ceil_div(c.G, RM), ceil_div(NC, RN));
   ProfScope ps(c, ST_RP_GEMM);
-  rp_gemm_kernel<<<grid, 256, 0, c.stream>>>(Rpl, Wm, K, NC, c.G, reducedpot);
+  rp_gemm2_kernel<<<grid, 256, 0, c.stream>>>(Rpl, Wm, K, NC, c.G, reducedpot);
   SG_LAUNCHED();
   return SINCGPU_OK;
 }
