@@ -267,6 +267,24 @@ int sincgpu_assemble_sparsemats_dev(sincgpu_ctx* ctx, const double* twoematel, c
 int sincgpu_sparseconfigmult_dev(sincgpu_ctx* ctx, const double* invector, double* outvector,
                                  double ezfield);
 
+/* A-vector Krylov propagation, the expoavecprop -> DGEXPVxxx2 path
+ * (MCTDH.SRC/expo_driver.f90:827-1055, MCTDH.SRC/expokit.f90:2222-2688):
+ * avec_out = exp(t * timefac * H) avec_in with H the assembled CI Hamiltonian
+ * (sparseconfigmult, including nucrepulsion and, for ezfield != 0, the z field),
+ * Arnoldi of dimension krylovdim on the real-ified vector, (6,6) Pade of the
+ * Hessenberg, local error control at tolerance tol (aerror).  *stepguess is the
+ * first trial step on entry and the next call's guess on exit (the reference's
+ * saved tempstepsize); *nstep receives the number of internal steps.  Config-basis
+ * form: the spin-adapted basis transformation is not applied.  The reference scales
+ * the operator by the step (cmf_prop_avector0, MCTDH.SRC/prop.f90:688-693) and calls
+ * with t = 1, anorm = dt: pass timefac*dt and t = 1 to take the same decisions. */
+int sincgpu_expoavecprop_dev(sincgpu_ctx* ctx, const double* avec_in, double* avec_out, double t,
+                             double timefac_re, double timefac_im, int krylovdim, double tol, double anorm,
+                             double ezfield, double* stepguess, int* nstep);
+int sincgpu_expoavecprop(sincgpu_ctx* ctx, const double* avec_in, double* avec_out, double t,
+                         double timefac_re, double timefac_im, int krylovdim, double tol, double anorm,
+                         double ezfield, double* stepguess, int* nstep);
+
 /* One orbital-RHS evaluation from the A-vector: denmat, invdenmat and the 2-RDM
  * (get_allden, MCTDH.SRC/mean.f90:467-477), then sincgpu_orbital_rhs_dev. */
 int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* ctx, const double* phi, const double* avector,

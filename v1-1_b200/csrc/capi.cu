@@ -61,6 +61,7 @@ Ctx::~Ctx() {
   ws_state.release();
   ws_ci.release();
   ws_ci2.release();
+  ws_kry.release();
   ci.release();
   if (stream && own_stream) cudaStreamDestroy(stream);
 }

@@ -145,6 +145,34 @@ int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* h, const double* phi, const double
                                  out);
 }
 
+int sincgpu_expoavecprop_dev(sincgpu_ctx* h, const double* avec_in, double* avec_out, double t,
+                             double tre, double tim, int krylovdim, double tol, double anorm, double ezfield,
+                             double* stepguess, int* nstep) {
+  CTX_CHECK(h);
+  SG_CHECK(avec_in && avec_out && stepguess && avec_in != avec_out, SINCGPU_EINVAL, "bad argument");
+  SG_CHECK(*stepguess > 0.0, SINCGPU_EINVAL, "stepguess must be positive");
+  return expv_avector(h->c, (const double2*)avec_in, (double2*)avec_out, t, make_double2(tre, tim), krylovdim,
+                      tol, anorm, stepguess, nstep, ezfield, nucdip_z(h->c));
+}
+
+int sincgpu_expoavecprop(sincgpu_ctx* h, const double* avec_in, double* avec_out, double t, double tre,
+                         double tim, int krylovdim, double tol, double anorm, double ezfield, double* stepguess,
+                         int* nstep) {
+  CTX_CHECK(h);
+  Ctx& c = h->c;
+  SG_CHECK(c.ci.attached, SINCGPU_ESTATE, "no walk tables attached");
+  SG_CHECK(avec_in && avec_out, SINCGPU_EINVAL, "null argument");
+  const size_t ba = sizeof(double2) * c.ci.nc, pa = (ba + 255) / 256 * 256;
+  SG_TRY(c.ws_io.ensure(2 * pa));
+  double* di = (double*)c.ws_io.ptr;
+  double* dout = (double*)((char*)c.ws_io.ptr + pa);
+  SG_TRY(up(c, di, avec_in, ba));
+  SG_TRY(sincgpu_expoavecprop_dev(h, di, dout, t, tre, tim, krylovdim, tol, anorm, ezfield, stepguess, nstep));
+  SG_TRY(down(c, avec_out, dout, ba));
+  SG_CUDA(cudaStreamSynchronize(c.stream));
+  return SINCGPU_OK;
+}
+
 // ----------------------------------------------------------------- host forms
 int sincgpu_orbital_rhs_avec(sincgpu_ctx* h, const double* phi, const double* avector, double tre,
                              double tim, double ztdpot, double* outspfs) {

@@ -85,6 +85,7 @@ struct Ctx {
   Workspace ws_conv;    // layout conversion scratch
   Workspace ws_state;   // resident mean-field state of the fused orbital-RHS entry
   Workspace ws_ci, ws_ci2;  // CI scratch (KE phi + partials; summed one-body matrix)
+  Workspace ws_kry;         // Krylov basis, Hessenberg, Pade output
   CIState ci;
   int coul_chunk = 0;   // pairs per pass sequence (0 = automatic)
   Prof prof;
@@ -146,6 +147,10 @@ int ci_tally(Ctx& c, const double2* a1, const double2* a2, double2* tally);
 int ci_onebody(Ctx& c, const double2* phi, double2* mats);
 int ci_assemble(Ctx& c, const double2* twoematel, const double2* mats);
 int ci_sigma(Ctx& c, const double2* in, double2* out, double constant, double ez, double nucdipz);
+
+// krylov.cu: w = exp(t * timefac * H) v on the real-ified A-vector
+int expv_avector(Ctx& c, const double2* v, double2* w, double t, double2 timefac, int m, double tol,
+                 double anorm, double* stepguess, int* nstep_out, double ez, double nucdipz);
 
 // rhs.cu
 int mult_reducedpot(Ctx& c, const double2* phi, const double2* redpot, double2* out);

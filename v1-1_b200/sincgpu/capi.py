@@ -73,6 +73,8 @@ _SIGS = {
     "sincgpu_sparseconfigmult_dev": ([_P, _P, _P, _D], _I),
     "sincgpu_orbital_rhs_avec_dev": ([_P, _P, _P, _D, _D, _D, _P, _P, _P, _P, _P, _P], _I),
     "sincgpu_orbital_rhs_avec": ([_P, _P, _P, _D, _D, _D, _P], _I),
+    "sincgpu_expoavecprop_dev": ([_P, _P, _P, _D, _D, _D, _I, _D, _D, _D, _P, _P], _I),
+    "sincgpu_expoavecprop": ([_P, _P, _P, _D, _D, _D, _I, _D, _D, _D, _P, _P], _I),
     "sincgpu_profile": ([_P, _I], _I),
     "sincgpu_profile_read": ([_P, _P, _P, _I], _I),
     "sincgpu_orbital_rhs_dev": ([_P, _P, _P, _P, _P, _D, _D, _D, _P, _P, _P], _I),
@@ -326,6 +328,18 @@ class SincProject:
         out = np.zeros_like(a)
         _call("sincgpu_sparseconfigmult", self._h, _ptr(a), _ptr(out), float(ezfield))
         return out
+
+    def expoavecprop(self, avector, t, krylovdim=20, tol=1e-9, anorm=1.0, stepguess=None, timefac=-1j,
+                     ezfield=0.0):
+        """A-vector Krylov step (expo_driver.f90:827-1055): returns (avec_out, stepguess, nstep)."""
+        a = _f(avector).reshape(-1)
+        out = np.zeros_like(a)
+        g = C.c_double(t if stepguess is None else stepguess)
+        ns = C.c_int(0)
+        tf = complex(timefac)
+        _call("sincgpu_expoavecprop", self._h, _ptr(a), _ptr(out), float(t), tf.real, tf.imag, int(krylovdim),
+              float(tol), float(anorm), float(ezfield), C.byref(g), C.byref(ns))
+        return out, g.value, ns.value
 
     def getdenmat_dev(self, avector, denmat, invdenmat, denreg=1e-10):
         _call("sincgpu_getdenmat_dev", self._h, _ptr(avector), _ptr(denmat), _ptr(invdenmat), float(denreg))
