@@ -256,6 +256,9 @@ def main():
     # ---- secondary rates: orbital-RHS matvec alone, CI sigma alone ----
     secondary = secondary_rates(proj, torch, stream, flush, phi, den, inv, red, out, mat, avec, n, G)
 
+    # ---- precision form: Coulomb passes in FP32, everything else FP64 ----
+    precision = precision_form(proj, torch, stream, flush, step, out, mat, args.steps, world, dist, dev)
+
     # ---- per-kernel times (profiled pass, same stream) for the roofline ----
     proj.profile(True)
     nprof = min(20, args.steps)
@@ -278,7 +281,7 @@ def main():
         "data": "synthetic (seeded Gaussian-envelope orbitals, seeded normalised A-vector)",
         "config": workload_config(w), "clocks": clk, "gpu_launches": int(launches),
         "launches_per_step": launches / args.steps, "fft_length": proj.fft_length, "numconfig": nc,
-        "roofline": roofline, "secondary": secondary,
+        "roofline": roofline, "secondary": secondary, "precision_forms": precision,
         "stage_ms_per_step": {k: v[0] / nprof for k, v in prof.items()},
     }
     if e2e:
@@ -296,6 +299,48 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def precision_form(proj, torch, stream, flush, step, out, mat, steps, world, dist, dev):
+    """Same step with the Coulomb passes in FP32 (context option coulomb_fp32):
+    throughput and the relative errors of the orbital RHS and twoematel against
+    the FP64 form's results of the same inputs (the FP64 form is the one pinned
+    to the oracle at 1e-11)."""
+    step()
+    torch.cuda.synchronize()
+    out64, mat64 = out.clone(), mat.clone()
+    proj.set_option("coulomb_fp32", 1)
+    try:
+        for _ in range(3):
+            step()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(steps)]
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            step()
+            b.record(stream)
+        torch.cuda.synchronize()
+        total_ms = sum(a.elapsed_time(b) for a, b in evs)
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+
+        def rel(x, y):
+            return float((x - y).abs().max() / y.abs().max())
+        res = {"plain": {"coulomb": "fp64", "rhs_rel_err": 0.0},
+               "mixed_fp32_coulomb": {
+                   "value": world * steps / (total_ms / 1e3), "unit": UNIT,
+                   "ms_per_step": total_ms / steps, "coulomb": "fp32 (complex64 FFT passes, fp64 products "
+                                                               "and contractions)",
+                   "rhs_rel_err_vs_fp64": rel(out, out64), "twoematel_rel_err_vs_fp64": rel(mat, mat64)}}
+    finally:
+        proj.set_option("coulomb_fp32", 0)
+    return res
 
 
 def secondary_rates(proj, torch, stream, flush, phi, den, inv, red, out, mat, avec, n, G):

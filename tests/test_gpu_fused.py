@@ -1,0 +1,75 @@
+"""GPU parity of the fused orbital-RHS entries against the oracle.
+
+sincgpu_orbital_rhs: (phi, tally, denmat, invdenmat) -> actreduced00 output and
+twoematel in one call (the chain call_twoe_matel00 -> get_reducedpot ->
+actreduced00 of SINCDVR/coreproject.f90 and MCTDH.SRC/mean.f90).
+sincgpu_orbital_rhs_avec: (phi, A-vector) -> the same, with the 1-RDM, its
+regularised inverse and the 2-RDM tally computed from the A-vector on the GPU
+(getdenmat00 / get_tworeducedx of MCTDH.SRC).  Tolerance 1e-11 relative
+(FP64 plain form).
+"""
+import numpy as np
+import pytest
+
+from oracle import sinc_oracle as orc
+from oracle.walks_oracle import CIWalks
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-11
+
+
+def relerr(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def li(built_lib):
+    """Z=3 at the origin, 19^3 points, spacing 0.45, 6 orbitals, 3 electrons (ms=1)."""
+    from sincgpu import SincProject, WalkTables
+    n = 6
+    sysm = orc.SincSystem(19, 0.45, [[0, 0, 0]], [3.0])
+    gpu = SincProject(19, 0.45, [[0, 0, 0]], [3.0], n)
+    gpu.ci_attach(WalkTables(3, n, 1))
+    ow = CIWalks(3, n, 1)
+    phi = orc.seeded_orbitals(sysm, n, seed=41)
+    rng = np.random.default_rng(42)
+    a = rng.standard_normal(ow.numconfig) + 1j * rng.standard_normal(ow.numconfig)
+    a /= np.linalg.norm(a)
+    yield sysm, gpu, ow, phi, a
+    gpu.close()
+
+
+@pytest.mark.parametrize("timefac,ztd", [(-1j, 0.0), (-1j, 0.03), (-1.0, 0.0)])
+def test_orbital_rhs(li, timefac, ztd):
+    sysm, gpu, _, phi, _ = li
+    n = phi.shape[1]
+    tally = orc.seeded_tally(n, seed=43)
+    den = orc.seeded_hermitian_psd(n, seed=44)
+    inv = orc.invmatsmooth(den)
+    mat_ref, red_ref = sysm.call_twoe_matel00(phi, phi)
+    rp_ref = orc.get_reducedpot(red_ref, tally)
+    out_ref = orc.actreduced00(sysm, phi, phi, den, inv, rp_ref, timefac=timefac, ztdpot=ztd)
+    out, mat = gpu.orbital_rhs(phi, tally, den, inv, timefac=timefac, ztdpot=ztd)
+    assert relerr(mat, mat_ref) < TOL
+    assert relerr(out, out_ref) < TOL
+
+
+@pytest.mark.parametrize("ztd", [0.0, 0.02])
+def test_orbital_rhs_avec(li, ztd):
+    sysm, gpu, ow, phi, a = li
+    den = ow.getdenmat00(a)
+    inv = orc.invmatsmooth(den)
+    tally = ow.get_tworeducedx(a)
+    _, red = sysm.call_twoe_matel00(phi, phi)
+    rp = orc.get_reducedpot(red, tally)
+    ref = orc.actreduced00(sysm, phi, phi, den, inv, rp, ztdpot=ztd)
+    out = gpu.orbital_rhs_avec(phi, a, ztdpot=ztd)
+    assert relerr(out, ref) < TOL
+
+
+def test_orbital_rhs_avec_repeatable(li):
+    """Deterministic reductions: two evaluations are bitwise equal."""
+    _, gpu, _, phi, a = li
+    o1 = gpu.orbital_rhs_avec(phi, a)
+    o2 = gpu.orbital_rhs_avec(phi, a)
+    assert np.array_equal(o1, o2)

@@ -51,6 +51,8 @@ Ctx::~Ctx() {
   cudaFree(d_tcoul);
   cudaFree(d_khat);
   cudaFree(d_roots);
+  cudaFree(d_khat32);
+  cudaFree(d_roots32);
   ws_fft.release();
   ws_pairs.release();
   ws_gemm.release();
@@ -195,6 +197,12 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
   if (!strcmp(name, "coul_chunk")) {
     SG_CHECK(value >= 0, SINCGPU_EINVAL, "coul_chunk must be >= 0");
     h->c.coul_chunk = (int)value;
+    return SINCGPU_OK;
+  }
+  if (!strcmp(name, "coulomb_fp32")) {
+    SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "coulomb_fp32 must be 0 or 1");
+    if (value) SG_TRY(ensure_fp32_tables(h->c));
+    h->c.coul_fp32 = (int)value;
     return SINCGPU_OK;
   }
   set_error("unknown option '%s'", name);

@@ -68,6 +68,33 @@ __host__ __device__ __forceinline__ double2 cscale(double2 a, double s) {
   return make_double2(a.x * s, a.y * s);
 }
 
+// single-precision complex helpers (precision form of the Coulomb passes)
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// real type and constructor of a complex type
+template <class C>
+struct CplxTraits;
+template <>
+struct CplxTraits<double2> {
+  using Real = double;
+  __host__ __device__ static double2 make(double re, double im) { return make_double2(re, im); }
+};
+template <>
+struct CplxTraits<float2> {
+  using Real = float;
+  __host__ __device__ static float2 make(double re, double im) { return make_float2((float)re, (float)im); }
+};
+template <class C>
+__host__ __device__ __forceinline__ C cvt(double2 v) {
+  return CplxTraits<C>::make(v.x, v.y);
+}
+__host__ __device__ __forceinline__ double2 widen(double2 v) { return v; }
+__host__ __device__ __forceinline__ double2 widen(float2 v) { return make_double2(v.x, v.y); }
+
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 }  // namespace sincgpu

@@ -74,6 +74,8 @@ struct Ctx {
   double* d_tcoul = nullptr;    // threed_two on [1-N,N-1]^3 (real) ((2N-1)^3)
   double2* d_khat = nullptr;    // DFT of the padded kernel / P^3  (P^3)
   double2* d_roots = nullptr;   // exp(-2 pi i m / P)              (P)
+  float2* d_khat32 = nullptr;   // FP32 copies for the precision form, made on demand
+  float2* d_roots32 = nullptr;
 
   // ---- scratch --------------------------------------------------------------
   Workspace ws_fft;     // W1 + W2 of the Coulomb passes
@@ -88,6 +90,7 @@ struct Ctx {
   Workspace ws_kry;         // Krylov basis, Hessenberg, Pade output
   CIState ci;
   int coul_chunk = 0;   // pairs per pass sequence (0 = automatic)
+  int coul_fp32 = 0;    // 1: Coulomb passes in FP32 (precision form), 0: FP64
   Prof prof;
 
   ~Ctx();
@@ -119,6 +122,8 @@ int build_tables(Ctx& c, int toothnbig, int toothnsmall, int flags);
 int build_tables_from_arrays(Ctx& c, const double2* threed_two_host, const double* pot_host);
 int choose_plan(Ctx& c);
 int make_khat(Ctx& c);
+// FP32 roots and kernel spectrum (rounded once from the FP64 tables)
+int ensure_fp32_tables(Ctx& c);
 
 // coulomb.cu: R_p = T * (phi1_a conj(phi2_b)) for pairs p=(a_p,b_p).
 // Rpl (device) receives the planar real/imag parts: Rpl[p*G+x] = Re, Rpl[(npair+p)*G+x] = Im.

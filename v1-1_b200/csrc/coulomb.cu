@@ -16,6 +16,8 @@
 //   CXI: inverse DFT along x              (N^2 rows, only x<N kept) -> R
 // Pruned inputs/outputs never touch memory.  Pairs are processed in chunks
 // sized so that the intermediates W1 (N*N*P) and W2 (N*P*P) stay L2 resident.
+// The passes run in FP64 (double2) or, with the context option coulomb_fp32,
+// in FP32 (float2) with FP64 inputs and outputs.
 #include <algorithm>
 #include <vector>
 #include "coulomb_kernels.cuh"
@@ -38,12 +40,13 @@ int fft_length_for(int min_len, int* p1, int* p2) {
   return -1;
 }
 
-static int coul_dispatch(Ctx& c, const CoulArgs& ca, int np, bool dens, const double2* s1,
+template <class C>
+static int coul_dispatch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2* s1,
                          const double2* s2, double* Rpl, double2* full, bool herm) {
   switch (c.P) {
 #define SINCGPU_CASE(P, A, B) \
   case P:                     \
-    return coul_launch<A, B>(c, ca, np, dens, s1, s2, Rpl, full, herm);
+    return coul_launch<A, B, C>(c, ca, np, dens, s1, s2, Rpl, full, herm);
     SINCGPU_FFT_LENGTHS(SINCGPU_CASE)
 #undef SINCGPU_CASE
     default:
@@ -52,10 +55,24 @@ static int coul_dispatch(Ctx& c, const CoulArgs& ca, int np, bool dens, const do
   }
 }
 
-static int coul_run(Ctx& c, const double2* src1, const double2* src2, const int* h_pa,
-                    const int* h_pb, int npair, double* Rpl, double2* full, bool herm, bool dens) {
+template <class C>
+static const C* roots_of(const Ctx& c);
+template <>
+const double2* roots_of<double2>(const Ctx& c) { return c.d_roots; }
+template <>
+const float2* roots_of<float2>(const Ctx& c) { return c.d_roots32; }
+template <class C>
+static const C* khat_of(const Ctx& c);
+template <>
+const double2* khat_of<double2>(const Ctx& c) { return c.d_khat; }
+template <>
+const float2* khat_of<float2>(const Ctx& c) { return c.d_khat32; }
+
+template <class C>
+static int coul_run_t(Ctx& c, const double2* src1, const double2* src2, const int* h_pa,
+                      const int* h_pb, int npair, double* Rpl, double2* full, bool herm, bool dens) {
   const int N = c.N, P = c.P;
-  const long long per_pair = 16LL * ((long long)N * N * P + (long long)N * P * P);
+  const long long per_pair = (long long)sizeof(C) * ((long long)N * N * P + (long long)N * P * P);
   int chunk = c.coul_chunk;
   if (chunk <= 0) {
     const long long budget = 48LL << 20;
@@ -70,14 +87,14 @@ static int coul_run(Ctx& c, const double2* src1, const double2* src2, const int*
     SG_CUDA(cudaMemcpyAsync(d_pa, h_pa, sizeof(int) * npair, cudaMemcpyHostToDevice, c.stream));
     SG_CUDA(cudaMemcpyAsync(d_pb, h_pb, sizeof(int) * npair, cudaMemcpyHostToDevice, c.stream));
   }
-  CoulArgs ca{};
+  CoulArgs<C> ca{};
   ca.N = N;
   ca.P = P;
   ca.nspf = c.nspf;
   ca.G = c.G;
-  ca.roots = c.d_roots;
-  ca.khat = c.d_khat;
-  ca.W1 = (double2*)c.ws_fft.ptr;
+  ca.roots = roots_of<C>(c);
+  ca.khat = khat_of<C>(c);
+  ca.W1 = (C*)c.ws_fft.ptr;
   ca.W2 = ca.W1 + (long long)chunk * N * N * P;
   ca.npair_total = npair;
   for (int p0 = 0; p0 < npair; p0 += chunk) {
@@ -88,6 +105,15 @@ static int coul_run(Ctx& c, const double2* src1, const double2* src2, const int*
     SG_TRY(coul_dispatch(c, ca, np, dens, src1, src2, Rpl, full, herm));
   }
   return SINCGPU_OK;
+}
+
+static int coul_run(Ctx& c, const double2* src1, const double2* src2, const int* h_pa,
+                    const int* h_pb, int npair, double* Rpl, double2* full, bool herm, bool dens) {
+  if (c.coul_fp32) {
+    SG_TRY(ensure_fp32_tables(c));
+    return coul_run_t<float2>(c, src1, src2, h_pa, h_pb, npair, Rpl, full, herm, dens);
+  }
+  return coul_run_t<double2>(c, src1, src2, h_pa, h_pb, npair, Rpl, full, herm, dens);
 }
 
 int coulomb_pairs(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa,
@@ -101,23 +127,24 @@ int coulomb_dens(Ctx& c, const double2* dens, int m, double2* red) {
 
 // op_tinv on explicit densities with caller-provided scratch: no allocation.
 // The densities are processed in chunks that fit `scratch_bytes`.
-int coulomb_dens_scratch(Ctx& c, const double2* dens, int m, double2* red, double2* scratch,
-                         size_t scratch_bytes) {
+template <class C>
+static int coulomb_dens_scratch_t(Ctx& c, const double2* dens, int m, double2* red, void* scratch,
+                                  size_t scratch_bytes) {
   const int N = c.N, P = c.P;
-  const size_t per_dens = 16ull * ((size_t)N * N * P + (size_t)N * P * P);
+  const size_t per_dens = sizeof(C) * ((size_t)N * N * P + (size_t)N * P * P);
   SG_CHECK(per_dens <= scratch_bytes, SINCGPU_ERANGE,
            "one density on a %d^3 grid (FFT length %d) needs %zu bytes of scratch; the fixed "
            "scratch holds %zu bytes", N, P, per_dens, scratch_bytes);
   const int chunk = (int)std::min<size_t>(scratch_bytes / per_dens, (size_t)m);
-  CoulArgs ca{};
+  CoulArgs<C> ca{};
   ca.N = N;
   ca.P = P;
   ca.nspf = c.nspf;
   ca.G = c.G;
-  ca.roots = c.d_roots;
-  ca.khat = c.d_khat;
-  ca.W1 = scratch;
-  ca.W2 = scratch + (size_t)chunk * N * N * P;
+  ca.roots = roots_of<C>(c);
+  ca.khat = khat_of<C>(c);
+  ca.W1 = (C*)scratch;
+  ca.W2 = ca.W1 + (size_t)chunk * N * N * P;
   ca.npair_total = m;
   ca.pa = nullptr;
   ca.pb = nullptr;
@@ -126,6 +153,15 @@ int coulomb_dens_scratch(Ctx& c, const double2* dens, int m, double2* red, doubl
     SG_TRY(coul_dispatch(c, ca, std::min(chunk, m - p0), true, dens, nullptr, nullptr, red, false));
   }
   return SINCGPU_OK;
+}
+
+int coulomb_dens_scratch(Ctx& c, const double2* dens, int m, double2* red, double2* scratch,
+                         size_t scratch_bytes) {
+  if (c.coul_fp32) {
+    SG_CHECK(c.d_khat32 && c.d_roots32, SINCGPU_ESTATE, "FP32 Coulomb tables are missing");
+    return coulomb_dens_scratch_t<float2>(c, dens, m, red, scratch, scratch_bytes);
+  }
+  return coulomb_dens_scratch_t<double2>(c, dens, m, red, scratch, scratch_bytes);
 }
 
 }  // namespace sincgpu

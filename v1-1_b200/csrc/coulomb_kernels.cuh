@@ -1,5 +1,9 @@
 // Coulomb pass kernels on the register two-step FFT (fft_reg.cuh), templated on
-// the padded length P = P1*P2.  See coulomb.cu for the algorithm and the passes.
+// the padded length P = P1*P2 and on the complex type C of the transforms:
+// double2 (FP64 form) or float2 (FP32 precision form: pair products are formed
+// in FP64 and rounded once, the spectra W1/W2, twiddles and kernel spectrum are
+// FP32, and the potentials are widened back to FP64 on output).  See coulomb.cu
+// for the algorithm and the passes.
 #pragma once
 #include "context.hpp"
 #include "fft_reg.cuh"
@@ -10,30 +14,32 @@ namespace sincgpu {
 // static shared memory
 constexpr int lines_for(int P) { return P <= 128 ? 16 : 8; }
 
+template <class C>
 struct CoulArgs {
   int N, P, nspf;
   long long G;
-  const double2* roots;
-  const double2* khat;
-  double2* W1;  // [pair][z][y<N][kx]
-  double2* W2;  // [pair][z<N][ky][kx]
+  const C* roots;
+  const C* khat;
+  C* W1;  // [pair][z][y<N][kx]
+  C* W2;  // [pair][z<N][ky][kx]
   const int* pa;
   const int* pb;
   int pair0;        // index of the chunk's first pair in the full list
   int npair_total;  // planar output: Re at pair p, Im at npair_total + p
 };
 
-__device__ __forceinline__ void load_roots(double2* roots, const double2* g, int P) {
+template <class C>
+__device__ __forceinline__ void load_roots(C* roots, const C* g, int P) {
   for (int i = threadIdx.x; i < P; i += blockDim.x) roots[i] = g[i];
 }
 
 // CX: rows of rho -> DFT along x -> W1
-template <int P1, int P2, bool DENS>
+template <int P1, int P2, bool DENS, class C>
 __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul_fwd_x_t(
-    const double2* __restrict__ phi1, const double2* __restrict__ phi2, CoulArgs ca) {
+    const double2* __restrict__ phi1, const double2* __restrict__ phi2, CoulArgs<C> ca) {
   constexpr int P = P1 * P2, S = P1 > P2 ? P1 : P2, TL = lines_for(P);
-  __shared__ double2 roots[P];
-  __shared__ double2 ex[P * TL];
+  __shared__ C roots[P];
+  __shared__ C ex[P * TL];
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int s = threadIdx.x % S, l = threadIdx.x / S;
@@ -48,77 +54,77 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
     s1 = phi1 + (long long)ca.pa[p] * ca.G + off;
     s2 = phi2 + (long long)ca.pb[p] * ca.G + off;
   }
-  double2 a[P1], b[P2];
+  C a[P1], b[P2];
 #pragma unroll
   for (int n1 = 0; n1 < P1; ++n1) {
     const int x = s + P2 * n1;
     double2 v = make_double2(0.0, 0.0);
     if (row && s < P2 && x < N) v = DENS ? s1[x] : cmulc(s1[x], s2[x]);
-    a[n1] = v;
+    a[n1] = cvt<C>(v);
   }
   __syncthreads();
-  dft_in_to_out<P1, P2, false>(a, b, s, l, TL, ex, roots);
+  dft_in_to_out<P1, P2, false, C>(a, b, s, l, TL, ex, roots);
   if (row && s < P1) {
-    double2* dst = ca.W1 + (((long long)p * N + z) * N + y) * P;
+    C* dst = ca.W1 + (((long long)p * N + z) * N + y) * P;
 #pragma unroll
     for (int k2 = 0; k2 < P2; ++k2) dst[s + P1 * k2] = b[k2];
   }
 }
 
 // CY: W1 columns (y < N) -> DFT along y -> W2
-template <int P1, int P2>
-__global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul_fwd_y_t(CoulArgs ca) {
+template <int P1, int P2, class C>
+__global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul_fwd_y_t(CoulArgs<C> ca) {
   constexpr int P = P1 * P2, TL = lines_for(P);
-  __shared__ double2 roots[P];
-  __shared__ double2 ex[P * TL];
+  __shared__ C roots[P];
+  __shared__ C ex[P * TL];
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int l = threadIdx.x % TL, s = threadIdx.x / TL;
   const int p = blockIdx.z, z = blockIdx.y, kx = blockIdx.x * TL + l;
   const bool col = kx < P;
-  const double2* src = ca.W1 + ((long long)p * N + z) * N * P + kx;
-  double2 a[P1], b[P2];
+  const C* src = ca.W1 + ((long long)p * N + z) * N * P + kx;
+  C a[P1], b[P2];
 #pragma unroll
   for (int n1 = 0; n1 < P1; ++n1) {
     const int y = s + P2 * n1;
-    a[n1] = (col && s < P2 && y < N) ? src[(long long)y * P] : make_double2(0.0, 0.0);
+    a[n1] = (col && s < P2 && y < N) ? src[(long long)y * P] : CplxTraits<C>::make(0.0, 0.0);
   }
   __syncthreads();
-  dft_in_to_out<P1, P2, false>(a, b, s, l, TL, ex, roots);
+  dft_in_to_out<P1, P2, false, C>(a, b, s, l, TL, ex, roots);
   if (col && s < P1) {
-    double2* dst = ca.W2 + ((long long)p * N + z) * P * P + kx;
+    C* dst = ca.W2 + ((long long)p * N + z) * P * P + kx;
 #pragma unroll
     for (int k2 = 0; k2 < P2; ++k2) dst[(long long)(s + P1 * k2) * P] = b[k2];
   }
 }
 
 // CZ: W2 columns along z (z < N): forward, * khat, inverse, z < N written back
-template <int P1, int P2>
-__global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul_z_t(CoulArgs ca) {
+template <int P1, int P2, class C>
+__global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul_z_t(CoulArgs<C> ca) {
   constexpr int P = P1 * P2, TL = lines_for(P);
-  __shared__ double2 roots[P];
-  __shared__ double2 ex[P * TL];
+  __shared__ C roots[P];
+  __shared__ C ex[P * TL];
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int l = threadIdx.x % TL, s = threadIdx.x / TL;
   const int p = blockIdx.z, ky = blockIdx.y, kx = blockIdx.x * TL + l;
   const bool col = kx < P;
   const long long zs = (long long)P * P;
-  double2* base = ca.W2 + (long long)p * N * zs + (long long)ky * P + kx;
-  double2 a[P1], b[P2];
+  C* base = ca.W2 + (long long)p * N * zs + (long long)ky * P + kx;
+  C a[P1], b[P2];
 #pragma unroll
   for (int n1 = 0; n1 < P1; ++n1) {
     const int z = s + P2 * n1;
-    a[n1] = (col && s < P2 && z < N) ? base[z * zs] : make_double2(0.0, 0.0);
+    a[n1] = (col && s < P2 && z < N) ? base[z * zs] : CplxTraits<C>::make(0.0, 0.0);
   }
   __syncthreads();
-  dft_in_to_out<P1, P2, false>(a, b, s, l, TL, ex, roots);
+  dft_in_to_out<P1, P2, false, C>(a, b, s, l, TL, ex, roots);
   if (col && s < P1) {
-    const double2* kh = ca.khat + (long long)ky * P + kx;
+    const C* kh = ca.khat + (long long)ky * P + kx;
 #pragma unroll
     for (int k2 = 0; k2 < P2; ++k2) b[k2] = cmul(b[k2], kh[(long long)(s + P1 * k2) * zs]);
   }
-  dft_out_to_in<P1, P2, true>(b, a, s, l, TL, ex, roots);
+  dft_out_to_in<P1, P2, true, C>(b, a, s, l, TL, ex, roots);
   if (col && s < P2) {
 #pragma unroll
     for (int m1 = 0; m1 < P1; ++m1) {
@@ -129,25 +135,25 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
 }
 
 // CYI: W2 columns along ky (all P) -> inverse DFT -> W1 (y < N)
-template <int P1, int P2>
-__global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul_inv_y_t(CoulArgs ca) {
+template <int P1, int P2, class C>
+__global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul_inv_y_t(CoulArgs<C> ca) {
   constexpr int P = P1 * P2, TL = lines_for(P);
-  __shared__ double2 roots[P];
-  __shared__ double2 ex[P * TL];
+  __shared__ C roots[P];
+  __shared__ C ex[P * TL];
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int l = threadIdx.x % TL, s = threadIdx.x / TL;
   const int p = blockIdx.z, z = blockIdx.y, kx = blockIdx.x * TL + l;
   const bool col = kx < P;
-  const double2* src = ca.W2 + ((long long)p * N + z) * P * P + kx;
-  double2 a[P1], b[P2];
+  const C* src = ca.W2 + ((long long)p * N + z) * P * P + kx;
+  C a[P1], b[P2];
 #pragma unroll
   for (int n1 = 0; n1 < P1; ++n1)
-    a[n1] = (col && s < P2) ? src[(long long)(s + P2 * n1) * P] : make_double2(0.0, 0.0);
+    a[n1] = (col && s < P2) ? src[(long long)(s + P2 * n1) * P] : CplxTraits<C>::make(0.0, 0.0);
   __syncthreads();
-  dft_in_to_out<P1, P2, true>(a, b, s, l, TL, ex, roots);
+  dft_in_to_out<P1, P2, true, C>(a, b, s, l, TL, ex, roots);
   if (col && s < P1) {
-    double2* dst = ca.W1 + ((long long)p * N + z) * N * P + kx;
+    C* dst = ca.W1 + ((long long)p * N + z) * N * P + kx;
 #pragma unroll
     for (int k2 = 0; k2 < P2; ++k2) {
       const int y = s + P1 * k2;
@@ -157,24 +163,24 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
 }
 
 // CXI: W1 rows along kx -> inverse DFT -> R (x < N)
-template <int P1, int P2, bool DENS>
+template <int P1, int P2, bool DENS, class C>
 __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul_inv_x_t(
-    CoulArgs ca, double* __restrict__ Rpl, double2* __restrict__ full, int herm) {
+    CoulArgs<C> ca, double* __restrict__ Rpl, double2* __restrict__ full, int herm) {
   constexpr int P = P1 * P2, S = P1 > P2 ? P1 : P2, TL = lines_for(P);
-  __shared__ double2 roots[P];
-  __shared__ double2 ex[P * TL];
+  __shared__ C roots[P];
+  __shared__ C ex[P * TL];
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int s = threadIdx.x % S, l = threadIdx.x / S;
   const int p = blockIdx.z, z = blockIdx.y, y = blockIdx.x * TL + l;
   const bool row = y < N;
-  const double2* src = ca.W1 + (((long long)p * N + z) * N + y) * P;
-  double2 a[P1], b[P2];
+  const C* src = ca.W1 + (((long long)p * N + z) * N + y) * P;
+  C a[P1], b[P2];
 #pragma unroll
   for (int n1 = 0; n1 < P1; ++n1)
-    a[n1] = (row && s < P2) ? src[s + P2 * n1] : make_double2(0.0, 0.0);
+    a[n1] = (row && s < P2) ? src[s + P2 * n1] : CplxTraits<C>::make(0.0, 0.0);
   __syncthreads();
-  dft_in_to_out<P1, P2, true>(a, b, s, l, TL, ex, roots);
+  dft_in_to_out<P1, P2, true, C>(a, b, s, l, TL, ex, roots);
   if (!(row && s < P1)) return;
   const long long G = ca.G;
   const long long g0 = (long long)z * N * N + (long long)y * N;
@@ -193,7 +199,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   for (int k2 = 0; k2 < P2; ++k2) {
     const int x = s + P1 * k2;
     if (x < N) {
-      const double2 v = b[k2];
+      const double2 v = widen(b[k2]);
       const long long g = g0 + x;
       if (Rpl) {
         Rpl[(long long)gp * G + g] = v.x;
@@ -208,8 +214,8 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
 }
 
 // Launches the five passes for one chunk of np pairs.
-template <int P1, int P2>
-int coul_launch(Ctx& c, const CoulArgs& ca, int np, bool dens, const double2* src1,
+template <int P1, int P2, class C>
+int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2* src1,
                 const double2* src2, double* Rpl, double2* full, bool herm) {
   constexpr int P = P1 * P2, S = P1 > P2 ? P1 : P2, TL = lines_for(P);
   const int N = ca.N;
@@ -218,32 +224,32 @@ int coul_launch(Ctx& c, const CoulArgs& ca, int np, bool dens, const double2* sr
   {
     ProfScope ps(c, ST_COUL_FWD_X);
     if (dens)
-      coul_fwd_x_t<P1, P2, true><<<dim3(nrow, N, np), nthr, 0, c.stream>>>(src1, nullptr, ca);
+      coul_fwd_x_t<P1, P2, true, C><<<dim3(nrow, N, np), nthr, 0, c.stream>>>(src1, nullptr, ca);
     else
-      coul_fwd_x_t<P1, P2, false><<<dim3(nrow, N, np), nthr, 0, c.stream>>>(src1, src2, ca);
+      coul_fwd_x_t<P1, P2, false, C><<<dim3(nrow, N, np), nthr, 0, c.stream>>>(src1, src2, ca);
     SG_LAUNCHED();
   }
   {
     ProfScope ps(c, ST_COUL_FWD_Y);
-    coul_fwd_y_t<P1, P2><<<dim3(ncol, N, np), nthr, 0, c.stream>>>(ca);
+    coul_fwd_y_t<P1, P2, C><<<dim3(ncol, N, np), nthr, 0, c.stream>>>(ca);
     SG_LAUNCHED();
   }
   {
     ProfScope ps(c, ST_COUL_Z);
-    coul_z_t<P1, P2><<<dim3(ncol, P, np), nthr, 0, c.stream>>>(ca);
+    coul_z_t<P1, P2, C><<<dim3(ncol, P, np), nthr, 0, c.stream>>>(ca);
     SG_LAUNCHED();
   }
   {
     ProfScope ps(c, ST_COUL_INV_Y);
-    coul_inv_y_t<P1, P2><<<dim3(ncol, N, np), nthr, 0, c.stream>>>(ca);
+    coul_inv_y_t<P1, P2, C><<<dim3(ncol, N, np), nthr, 0, c.stream>>>(ca);
     SG_LAUNCHED();
   }
   {
     ProfScope ps(c, ST_COUL_INV_X);
     if (dens)
-      coul_inv_x_t<P1, P2, true><<<dim3(nrow, N, np), nthr, 0, c.stream>>>(ca, Rpl, full, 0);
+      coul_inv_x_t<P1, P2, true, C><<<dim3(nrow, N, np), nthr, 0, c.stream>>>(ca, Rpl, full, 0);
     else
-      coul_inv_x_t<P1, P2, false><<<dim3(nrow, N, np), nthr, 0, c.stream>>>(ca, Rpl, full, herm ? 1 : 0);
+      coul_inv_x_t<P1, P2, false, C><<<dim3(nrow, N, np), nthr, 0, c.stream>>>(ca, Rpl, full, herm ? 1 : 0);
     SG_LAUNCHED();
   }
   return SINCGPU_OK;
@@ -256,14 +262,20 @@ int coul_launch(Ctx& c, const CoulArgs& ca, int np, bool dens, const double2* sr
   X(108, 12, 9) X(120, 12, 10) X(126, 14, 9) X(144, 12, 12) X(162, 18, 9) X(180, 15, 12) \
   X(192, 16, 12) X(216, 18, 12) X(240, 16, 15) X(256, 16, 16)
 
-#define SINCGPU_DECLARE_LAUNCH(P, A, B)                                                   \
-  extern template int coul_launch<A, B>(Ctx&, const CoulArgs&, int, bool, const double2*, \
-                                        const double2*, double*, double2*, bool);
+#define SINCGPU_DECLARE_LAUNCH(P, A, B)                                                             \
+  extern template int coul_launch<A, B, double2>(Ctx&, const CoulArgs<double2>&, int, bool,         \
+                                                 const double2*, const double2*, double*, double2*, \
+                                                 bool);                                            \
+  extern template int coul_launch<A, B, float2>(Ctx&, const CoulArgs<float2>&, int, bool,           \
+                                                const double2*, const double2*, double*, double2*,  \
+                                                bool);
 SINCGPU_FFT_LENGTHS(SINCGPU_DECLARE_LAUNCH)
 #undef SINCGPU_DECLARE_LAUNCH
 
-#define SINCGPU_INSTANTIATE_LAUNCH(P, A, B)                                       \
-  template int coul_launch<A, B>(Ctx&, const CoulArgs&, int, bool, const double2*, \
-                                 const double2*, double*, double2*, bool);
+#define SINCGPU_INSTANTIATE_LAUNCH(P, A, B)                                                       \
+  template int coul_launch<A, B, double2>(Ctx&, const CoulArgs<double2>&, int, bool,              \
+                                          const double2*, const double2*, double*, double2*, bool); \
+  template int coul_launch<A, B, float2>(Ctx&, const CoulArgs<float2>&, int, bool,                \
+                                         const double2*, const double2*, double*, double2*, bool);
 
 }  // namespace sincgpu

@@ -1,17 +1,18 @@
-// In-shared-memory batched line FFT (Stockham auto-sort, mixed radix 2/3/4/5/7).
+// In-shared-memory batched line FFT (Stockham auto-sort, mixed radix 2/3/4/5/7)
+// and the radix butterflies shared with the register FFT (fft_reg.cuh).
 //
 // The Toeplitz Coulomb solve of the reference (SINCDVR/toeplitz_subs.f90:561-589)
 // needs forward-unnormalised 3-D DFTs on a doubled grid (COREPROJECT/ftcore.f90
-// uses DFFTPACK zfftf / FFTW_FORWARD).  Here each CTA transforms a tile of lines
-// that already sits in shared memory; the global-memory passes (coulomb.cu) decide
-// which axis the lines run along.
+// uses DFFTPACK zfftf / FFTW_FORWARD).  The Stockham engine transforms a tile of
+// lines held in shared memory (used at set-up for the kernel spectrum).
 //
 // Stage with radix r after a span L (product of the earlier radices):
 //   for j in [0, P/r):  k = j mod L
 //     y_q = sum_t x[j + t*P/r] * w^(t*k) * W_r^(t*q),   w = exp(-+2*pi*i/(L*r))
 //     out[(j/L)*L*r + k + q*L] = y_q
-// which ends in natural order with no bit reversal.  Each radix is a template so
-// that the r values of a butterfly live in registers.
+// which ends in natural order with no bit reversal.  The butterflies are
+// templates over the radix and the complex type (double2, or float2 for the
+// precision form).
 #pragma once
 #include "common.cuh"
 
@@ -27,51 +28,65 @@ struct FftPlan {
 };
 
 // roots[m] = exp(-2*pi*i*m/P), m in [0,P).  Inverse transforms use conj(roots).
-template <bool INV>
-__device__ __forceinline__ double2 root(const double2* roots, int m) {
-  double2 w = roots[m];
+template <bool INV, class C>
+__device__ __forceinline__ C root(const C* roots, int m) {
+  C w = roots[m];
   if (INV) w.y = -w.y;
   return w;
 }
 
-// i*z (forward: -i*z)
-template <bool INV>
-__device__ __forceinline__ double2 mul_mi(double2 z) {
-  return INV ? make_double2(-z.y, z.x) : make_double2(z.y, -z.x);
+// -i*z (forward) or +i*z (inverse)
+template <bool INV, class C>
+__device__ __forceinline__ C mul_mi(C z) {
+  C r;
+  if (INV) {
+    r.x = -z.y;
+    r.y = z.x;
+  } else {
+    r.x = z.y;
+    r.y = -z.x;
+  }
+  return r;
 }
 
-template <int R, bool INV>
+template <int R, bool INV, class C>
 struct Butterfly;
 
-template <bool INV>
-struct Butterfly<2, INV> {
-  __device__ __forceinline__ static void run(double2* a, const double2*, int) {
-    double2 t0 = a[0], t1 = a[1];
+template <bool INV, class C>
+struct Butterfly<2, INV, C> {
+  __device__ __forceinline__ static void run(C* a, const C*, int) {
+    C t0 = a[0], t1 = a[1];
     a[0] = cadd(t0, t1);
     a[1] = csub(t0, t1);
   }
 };
 
-template <bool INV>
-struct Butterfly<3, INV> {
-  __device__ __forceinline__ static void run(double2* a, const double2* roots, int P) {
+template <bool INV, class C>
+struct Butterfly<3, INV, C> {
+  __device__ __forceinline__ static void run(C* a, const C* roots, int P) {
+    using Re = typename CplxTraits<C>::Real;
     // W_3 = exp(-+2 pi i/3) = (-1/2, s),  s = -+ sin(2 pi/3)
-    const double s = INV ? -roots[P / 3].y : roots[P / 3].y;
-    double2 sum = cadd(a[1], a[2]);
-    double2 dif = csub(a[1], a[2]);
-    double2 m = make_double2(fma(-0.5, sum.x, a[0].x), fma(-0.5, sum.y, a[0].y));
+    const Re s = INV ? -roots[P / 3].y : roots[P / 3].y;
+    const Re h = (Re)-0.5;
+    C sum = cadd(a[1], a[2]);
+    C dif = csub(a[1], a[2]);
+    C m;
+    m.x = fma(h, sum.x, a[0].x);
+    m.y = fma(h, sum.y, a[0].y);
     a[0] = cadd(a[0], sum);
-    a[1] = make_double2(fma(-s, dif.y, m.x), fma(s, dif.x, m.y));
-    a[2] = make_double2(fma(s, dif.y, m.x), fma(-s, dif.x, m.y));
+    a[1].x = fma(-s, dif.y, m.x);
+    a[1].y = fma(s, dif.x, m.y);
+    a[2].x = fma(s, dif.y, m.x);
+    a[2].y = fma(-s, dif.x, m.y);
   }
 };
 
-template <bool INV>
-struct Butterfly<4, INV> {
-  __device__ __forceinline__ static void run(double2* a, const double2*, int) {
-    double2 s02 = cadd(a[0], a[2]), d02 = csub(a[0], a[2]);
-    double2 s13 = cadd(a[1], a[3]), d13 = csub(a[1], a[3]);
-    double2 rot = mul_mi<INV>(d13);
+template <bool INV, class C>
+struct Butterfly<4, INV, C> {
+  __device__ __forceinline__ static void run(C* a, const C*, int) {
+    C s02 = cadd(a[0], a[2]), d02 = csub(a[0], a[2]);
+    C s13 = cadd(a[1], a[3]), d13 = csub(a[1], a[3]);
+    C rot = mul_mi<INV>(d13);
     a[0] = cadd(s02, s13);
     a[2] = csub(s02, s13);
     a[1] = cadd(d02, rot);
@@ -80,45 +95,49 @@ struct Butterfly<4, INV> {
 };
 
 // odd prime radices: direct DFT with the symmetric pairing t <-> r-t
-template <int R, bool INV>
+template <int R, bool INV, class C>
 struct ButterflyOdd {
-  __device__ __forceinline__ static void run(double2* a, const double2* roots, int P) {
+  __device__ __forceinline__ static void run(C* a, const C* roots, int P) {
     const int step = P / R;
-    double2 sp[(R - 1) / 2], sm[(R - 1) / 2];
+    C sp[(R - 1) / 2], sm[(R - 1) / 2];
 #pragma unroll
     for (int t = 1; t <= (R - 1) / 2; ++t) {
       sp[t - 1] = cadd(a[t], a[R - t]);
       sm[t - 1] = csub(a[t], a[R - t]);
     }
-    double2 y[R];
-    double2 y0 = a[0];
+    C y[R];
+    C y0 = a[0];
 #pragma unroll
     for (int t = 0; t < (R - 1) / 2; ++t) y0 = cadd(y0, sp[t]);
     y[0] = y0;
 #pragma unroll
     for (int q = 1; q <= (R - 1) / 2; ++q) {
-      double2 re = a[0];   // sum_t cos(2 pi t q / R) sp_t
-      double2 im = make_double2(0.0, 0.0);  // sum_t sin-part of sm_t
+      C re = a[0];  // sum_t cos(2 pi t q / R) sp_t
+      C im;         // sum_t sin-part of sm_t
+      im.x = 0;
+      im.y = 0;
 #pragma unroll
       for (int t = 1; t <= (R - 1) / 2; ++t) {
-        const double2 w = root<INV>(roots, ((t * q) % R) * step);  // (cos, -+sin)
+        const C w = root<INV>(roots, ((t * q) % R) * step);  // (cos, -+sin)
         re.x = fma(w.x, sp[t - 1].x, re.x);
         re.y = fma(w.x, sp[t - 1].y, re.y);
         im.x = fma(w.y, sm[t - 1].x, im.x);
         im.y = fma(w.y, sm[t - 1].y, im.y);
       }
       // y_q = re + i*im,  y_{R-q} = re - i*im
-      y[q] = make_double2(re.x - im.y, re.y + im.x);
-      y[R - q] = make_double2(re.x + im.y, re.y - im.x);
+      y[q].x = re.x - im.y;
+      y[q].y = re.y + im.x;
+      y[R - q].x = re.x + im.y;
+      y[R - q].y = re.y - im.x;
     }
 #pragma unroll
     for (int q = 0; q < R; ++q) a[q] = y[q];
   }
 };
-template <bool INV>
-struct Butterfly<5, INV> : ButterflyOdd<5, INV> {};
-template <bool INV>
-struct Butterfly<7, INV> : ButterflyOdd<7, INV> {};
+template <bool INV, class C>
+struct Butterfly<5, INV, C> : ButterflyOdd<5, INV, C> {};
+template <bool INV, class C>
+struct Butterfly<7, INV, C> : ButterflyOdd<7, INV, C> {};
 
 template <int R, bool INV>
 __device__ __forceinline__ void fft_stage(const double2* __restrict__ src, double2* __restrict__ dst,
@@ -146,7 +165,7 @@ __device__ __forceinline__ void fft_stage(const double2* __restrict__ src, doubl
       if (t > 0 && k > 0) v = cmul(v, root<INV>(roots, t * k * tw));
       a[t] = v;
     }
-    Butterfly<R, INV>::run(a, roots, P);
+    Butterfly<R, INV, double2>::run(a, roots, P);
     double2* dl = dst + l * lstride;
     const int base = jL * L * R + k;
 #pragma unroll

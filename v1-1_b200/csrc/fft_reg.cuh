@@ -9,7 +9,8 @@
 //   dft_out_to_in : D_out -> D_in    (inverse of the above layout, forward or inverse)
 // The sub-transforms of length P1 / P2 run fully unrolled in registers
 // (compile-time mixed radix 2/3/4/5/7 Stockham), twiddles come from the table
-// roots[m] = exp(-2 pi i m / P) in shared memory.
+// roots[m] = exp(-2 pi i m / P) in shared memory.  The complex type C is double2
+// (the FP64 form) or float2 (the FP32 precision form).
 #pragma once
 #include "fft_engine.cuh"
 
@@ -20,48 +21,48 @@ constexpr int first_radix(int m) {
 }
 
 // In-register DFT of compile-time length M (M divides P), stages from span L on.
-template <int M, int L, bool INV>
+template <int M, int L, bool INV, class C>
 struct RegFFT {
   static constexpr int R = first_radix(M / L);
-  __device__ __forceinline__ static void run(double2 (&a)[M], const double2* roots, int P) {
-    double2 b[M];
+  __device__ __forceinline__ static void run(C (&a)[M], const C* roots, int P) {
+    C b[M];
     const int rstep = P / M;
 #pragma unroll
     for (int j = 0; j < M / R; ++j) {
       const int k = j % L;
-      double2 t[R];
+      C t[R];
 #pragma unroll
       for (int q = 0; q < R; ++q) {
-        double2 v = a[j + q * (M / R)];
+        C v = a[j + q * (M / R)];
         if (q > 0 && k > 0) v = cmul(v, root<INV>(roots, (q * k * (M / (L * R))) * rstep));
         t[q] = v;
       }
-      Butterfly<R, INV>::run(t, roots, P);
+      Butterfly<R, INV, C>::run(t, roots, P);
 #pragma unroll
       for (int q = 0; q < R; ++q) b[(j / L) * L * R + k + q * L] = t[q];
     }
 #pragma unroll
     for (int i = 0; i < M; ++i) a[i] = b[i];
-    RegFFT<M, L * R, INV>::run(a, roots, P);
+    RegFFT<M, L * R, INV, C>::run(a, roots, P);
   }
 };
-template <int M, bool INV>
-struct RegFFT<M, M, INV> {
-  __device__ __forceinline__ static void run(double2 (&)[M], const double2*, int) {}
+template <int M, bool INV, class C>
+struct RegFFT<M, M, INV, C> {
+  __device__ __forceinline__ static void run(C (&)[M], const C*, int) {}
 };
 
-// ex: exchange buffer of P*TL double2 for TL lines; element e of line l at ex[e*TL + l].
+// ex: exchange buffer of P*TL complex values for TL lines; element e of line l at ex[e*TL + l].
 // Threads with s >= P2 (step 1) or s >= P1 (step 2) idle in that step.
 // On entry a[] holds D_in (valid for s < P2); on exit b[] holds D_out (valid for s < P1).
-template <int P1, int P2, bool INV>
-__device__ __forceinline__ void dft_in_to_out(double2 (&a)[P1], double2 (&b)[P2], int s, int l,
-                                              int TL, double2* ex, const double2* roots) {
+template <int P1, int P2, bool INV, class C>
+__device__ __forceinline__ void dft_in_to_out(C (&a)[P1], C (&b)[P2], int s, int l, int TL, C* ex,
+                                              const C* roots) {
   constexpr int P = P1 * P2;
   if (s < P2) {
-    RegFFT<P1, 1, INV>::run(a, roots, P);
+    RegFFT<P1, 1, INV, C>::run(a, roots, P);
 #pragma unroll
     for (int k1 = 0; k1 < P1; ++k1) {
-      double2 v = a[k1];
+      C v = a[k1];
       if (k1 > 0 && s > 0) v = cmul(v, root<INV>(roots, s * k1));
       ex[(k1 * P2 + s) * TL + l] = v;
     }
@@ -70,21 +71,21 @@ __device__ __forceinline__ void dft_in_to_out(double2 (&a)[P1], double2 (&b)[P2]
   if (s < P1) {
 #pragma unroll
     for (int n2 = 0; n2 < P2; ++n2) b[n2] = ex[(s * P2 + n2) * TL + l];
-    RegFFT<P2, 1, INV>::run(b, roots, P);
+    RegFFT<P2, 1, INV, C>::run(b, roots, P);
   }
   __syncthreads();
 }
 
 // On entry b[] holds D_out (valid for s < P1); on exit a[] holds D_in (valid for s < P2).
-template <int P1, int P2, bool INV>
-__device__ __forceinline__ void dft_out_to_in(double2 (&b)[P2], double2 (&a)[P1], int s, int l,
-                                              int TL, double2* ex, const double2* roots) {
+template <int P1, int P2, bool INV, class C>
+__device__ __forceinline__ void dft_out_to_in(C (&b)[P2], C (&a)[P1], int s, int l, int TL, C* ex,
+                                              const C* roots) {
   constexpr int P = P1 * P2;
   if (s < P1) {
-    RegFFT<P2, 1, INV>::run(b, roots, P);
+    RegFFT<P2, 1, INV, C>::run(b, roots, P);
 #pragma unroll
     for (int m2 = 0; m2 < P2; ++m2) {
-      double2 v = b[m2];
+      C v = b[m2];
       if (m2 > 0 && s > 0) v = cmul(v, root<INV>(roots, s * m2));
       ex[(m2 * P1 + s) * TL + l] = v;
     }
@@ -93,7 +94,7 @@ __device__ __forceinline__ void dft_out_to_in(double2 (&b)[P2], double2 (&a)[P1]
   if (s < P2) {
 #pragma unroll
     for (int k1 = 0; k1 < P1; ++k1) a[k1] = ex[(s * P1 + k1) * TL + l];
-    RegFFT<P1, 1, INV>::run(a, roots, P);
+    RegFFT<P1, 1, INV, C>::run(a, roots, P);
   }
   __syncthreads();
 }

@@ -464,6 +464,10 @@ int make_khat(Ctx& c) {
   const int P = c.P;
   const long long P3 = (long long)P * P * P;
   if (c.d_khat) cudaFree(c.d_khat);
+  cudaFree(c.d_khat32);  // FP32 copies follow the FP64 tables
+  cudaFree(c.d_roots32);
+  c.d_khat32 = nullptr;
+  c.d_roots32 = nullptr;
   SG_CUDA(cudaMalloc(&c.d_khat, sizeof(double2) * P3));
   embed_kernel<<<ceil_div(P3, 256), 256>>>(c.d_khat, c.d_tcoul, c.N, P);
   SG_LAUNCHED();
@@ -480,6 +484,29 @@ int make_khat(Ctx& c) {
   fft_full_axis_kernel<<<g1, 128, sm1>>>(c.d_khat, c.plan, c.d_roots, 2, c.tx, inv);
   SG_LAUNCHED();
   SG_CUDA(cudaDeviceSynchronize());
+  return SINCGPU_OK;
+}
+
+__global__ void narrow_kernel(float2* __restrict__ out, const double2* __restrict__ in, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = make_float2((float)in[i].x, (float)in[i].y);
+}
+
+int ensure_fp32_tables(Ctx& c) {
+  const long long P3 = (long long)c.P * c.P * c.P;
+  if (!c.d_khat32) {
+    SG_CUDA(cudaMalloc(&c.d_khat32, sizeof(float2) * P3));
+    narrow_kernel<<<std::min<long long>(ceil_div(P3, 256), 148 * 16), 256, 0, c.stream>>>(c.d_khat32,
+                                                                                        c.d_khat, P3);
+    SG_LAUNCHED();
+  }
+  if (!c.d_roots32) {
+    SG_CUDA(cudaMalloc(&c.d_roots32, sizeof(float2) * c.P));
+    narrow_kernel<<<1, 256, 0, c.stream>>>(c.d_roots32, c.d_roots, c.P);
+    SG_LAUNCHED();
+  }
+  SG_CUDA(cudaStreamSynchronize(c.stream));
   return SINCGPU_OK;
 }
 
