@@ -298,6 +298,44 @@ int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* ctx, const double* phi, const doub
 int sincgpu_orbital_rhs_avec(sincgpu_ctx* ctx, const double* phi, const double* avector,
                              double timefac_re, double timefac_im, double ztdpot, double* outspfs);
 
+/* Orbital propagation, the expospfprop -> DGPHIV path of intopt=3
+ * (MCTDH.SRC/expo_driver.f90:482-771 with jacinit0 :429-467 and jacoperate00
+ * :40-259; MCTDH.SRC/expokit.f90:3904-4310; spf_linear_derivs
+ * MCTDH.SRC/derivs.f90:1037-1186; spf_orthogit MCTDH.SRC/spfs.f90:120-196).
+ * phi (device, totpoints x numspf complex) is advanced in place from tin to tout:
+ * phi <- orthonormalised(phi + dt phi_1(dt J) f(phi)), J the orbital Jacobian.
+ * The mean fields come as two slots (0: the end of the mean-field interval,
+ * 1: its start), each denmat, invdenmat (numspf^2) and reducedpot
+ * (totpoints x numspf^2); with linearflag they are blended with weights
+ * ((t-firsttime)/(lasttime-firsttime), 1 - that) at the interval midpoint (the
+ * reference's effective_cmf_linearflag), otherwise slot 0 alone is used and the
+ * slot-1 pointers may be NULL.  ezfield is the z field at the midpoint.
+ * *numiters receives the number of Jacobian products (iwsp(1)).  The Krylov
+ * dimension and step guess persist in the context between calls, as the
+ * reference's saved variables do; sincgpu_orbprop_setup resets them. */
+int sincgpu_expospfprop_dev(sincgpu_ctx* ctx, double* phi, const double* denmat0, const double* invdenmat0,
+                            const double* reducedpot0, const double* denmat1, const double* invdenmat1,
+                            const double* reducedpot1, double tin, double tout, double firsttime,
+                            double lasttime, int linearflag, double timefac_re, double timefac_im,
+                            double ezfield, double expotol, int* numiters);
+
+/* Parameters of the orbital propagator (expodim, maxexpodim, expostepfac and
+ * par_timestep/littlesteps, MCTDH.SRC/parameters.f90:271-290); resets the saved
+ * state.  maxexpodim must be at most 125. */
+int sincgpu_orbprop_setup(sincgpu_ctx* ctx, int expodim, int maxexpodim, double expostepfac,
+                          double first_stepsize);
+
+/* Saved state of the orbital propagator: current Krylov dimension, next step
+ * guess, the exposet flag and the call count. */
+int sincgpu_orbprop_state(sincgpu_ctx* ctx, int* thisexpodim, double* tempstepsize, int* exposet,
+                          int* icalled);
+
+/* spf_orthogit (MCTDH.SRC/spfs.f90:120-196): two Loewdin passes
+ * phi <- phi S^(-1/2), S = <phi|phi>, S^(-1/2) by SVD with singular values below
+ * 1e-10 dropped (symorthogmat, MCTDH.SRC/utils.f90:947-1023).  *error (optional)
+ * receives max|S - 1| of the final overlap. */
+int sincgpu_spf_orthogit_dev(sincgpu_ctx* ctx, double* phi, double* error);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,8 +7,12 @@ variants the reference calls for the A-vector propagation:
   DGEXPVxxx20  Krylov exp(t A) v with full Arnoldi, externally supplied dot,
                initial step from the caller (stepguess), next step never shorter
                than the accepted one (MCTDH.SRC/expokit.f90:2222-2660)
+  DGPHIV0      Krylov w = exp(t A) v + t phi_1(t A) u on the 3-extended
+               Hessenberg (MCTDH.SRC/expokit.f90:3904-4310), with the same step
+               guess conventions and plain gamma step-down on rejection
 as called by expoavecprop (MCTDH.SRC/expo_driver.f90:827-1055) on the real-ified
-A-vector (complex vector of length nc viewed as 2*nc reals).
+A-vector and by expospfprop (MCTDH.SRC/expo_driver.f90:482-771) on the
+real-ified orbitals (complex vectors viewed as interleaved reals).
 Only tests/ and the CPU legs of bench.py import this module.
 """
 from __future__ import annotations
@@ -155,6 +159,103 @@ def dgexpv(n, m, t, v, tol, anorm, matvec, dot, stepguess, maxdim, ideg=6, mxste
             break
     new_guess = t_step if nstep == 1 else t_last
     return w, new_guess, {"nstep": nstep, "nmult": nmult, "steps": steps}
+
+
+def dgphiv(n, m, t, u, v, tol, anorm, matvec, dot, stepguess, ideg=6, mxstep=1000):
+    """Returns (w, new_stepguess, info) for w = exp(t A) v + t phi_1(t A) u,
+    phi_1(z) = (exp(z) - 1)/z (MCTDH.SRC/expokit.f90:3904-4310)."""
+    delta, gamma = 1.2, 0.8
+    if m >= n or m <= 0:
+        raise ValueError("bad Krylov dimension")
+    mh = m + 3
+    t_out = abs(t)
+    t_now = t_step = t_last = t_new = 0.0
+    eps = abs((4.0 / 3.0 - 1.0) * 3.0 - 1.0)
+    if tol <= eps:
+        tol = math.sqrt(eps)
+    break_tol = 1.0e-7
+    sgn = math.copysign(1.0, t)
+    sqr1 = math.sqrt(0.1)
+    w = np.array(v, dtype=np.float64)
+    u = np.asarray(u, dtype=np.float64)
+    nstep = nmult = nreject = 0
+    xm = 0.0
+    avnorm = 0.0
+    steps = []
+    while t_now < t_out:
+        nmult += 1
+        p = matvec(w) + u
+        beta = math.sqrt(dot(p, p))
+        if beta == 0.0:
+            break
+        V = np.zeros((m + 2, n))
+        Hm = np.zeros((mh, mh))
+        V[0] = p / beta
+        if nstep == 0:
+            t_new = stepguess
+            xm = 1.0 / m
+        nstep += 1
+        t_last = t_step
+        t_step = min(t_out - t_now, t_new)
+        k1, mbrkdwn, hj1j = 3, m, 0.0
+        brk = False
+        for j in range(m):
+            nmult += 1
+            p = matvec(V[j])
+            for i in range(j + 1):
+                hij = dot(V[i], p)
+                p = p - hij * V[i]
+                Hm[i, j] = hij
+            hj1j = math.sqrt(dot(p, p))
+            if hj1j <= break_tol:
+                k1, mbrkdwn, brk = 0, j + 1, True
+                t_step = t_out - t_now
+                break
+            Hm[j + 1, j] = hj1j
+            V[j + 1] = p / hj1j
+        if not brk:
+            nmult += 1
+            p = matvec(V[m])
+            avnorm = math.sqrt(dot(p, p))
+        # the 3-extended scheme: e_1 column, h(m+1,m) taken out, shifted identity
+        Hm[0, mbrkdwn] = 1.0
+        Hm[m, m - 1] = 0.0
+        for i in range(1, k1):
+            Hm[m + i - 1, m + i] = 1.0
+        while True:
+            mx = mbrkdwn + max(1, k1)
+            E, _ = dgpadm(ideg, Hm[:mx, :mx], sgn * t_step)
+            phih = np.zeros(mx + 2)
+            phih[:mx] = E[:, mbrkdwn]
+            if k1 != 0:
+                phih[mbrkdwn] = hj1j * E[mbrkdwn - 1, mbrkdwn + 1]
+                phih[mbrkdwn + 1] = hj1j * E[mbrkdwn - 1, mbrkdwn + 2]
+                p1 = abs(phih[m]) * beta
+                p2 = abs(phih[m + 1]) * beta * avnorm
+                if p1 > 10.0 * p2:
+                    err_loc, xm = p2, 1.0 / (m + 1)
+                else:
+                    err_loc, xm = p1, 1.0 / m
+                if err_loc > delta * t_step * tol:   # mxreject = 0: step down and retry
+                    t_step = gamma * t_step
+                    nreject += 1
+                    continue
+            else:
+                err_loc = tol
+            break
+        mx = mbrkdwn + max(0, k1 - 2)
+        w = w + beta * (V[:mx].T @ phih[:mx])
+        t_new = gamma * t_step * (t_step * tol / err_loc) ** xm
+        p1 = 10.0 ** (round_half_away(math.log10(t_new) - sqr1) - 1)
+        t_new = math.trunc(t_new / p1 + 0.55) * p1
+        if t_new < t_step:
+            t_new = t_step
+        t_now += t_step
+        steps.append(t_step)
+        if nstep >= mxstep:
+            break
+    new_guess = t_step if nstep == 1 else t_last
+    return w, new_guess, {"nstep": nstep, "nmult": nmult, "nreject": nreject, "steps": steps}
 
 
 def round_half_away(x: float) -> int:

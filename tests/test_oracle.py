@@ -131,3 +131,43 @@ def test_ci_counts_and_hermitian_sigma(ne, n, ms):
     hab = np.vdot(a, w.sparsesparsemult(b, xp, xo, xz))
     hba = np.vdot(b, w.sparsesparsemult(a, xp, xo, xz))
     assert abs(hab - np.conj(hba)) < 1e-12 * abs(hab)
+
+
+def test_dgphiv_matches_augmented_exponential():
+    """w = exp(tA) v + t phi_1(tA) u equals the top block of
+    expm(t [[A, u], [0, 0]]) [v; 1] (Sidje's augmented-matrix identity)."""
+    import scipy.linalg as sl
+    from oracle.expokit_oracle import dgphiv
+    rng = np.random.default_rng(61)
+    n = 60
+    a = rng.standard_normal((n, n)) / math.sqrt(n)
+    a = 0.5 * (a - a.T) + 0.05 * rng.standard_normal((n, n)) / math.sqrt(n)
+    u, v = rng.standard_normal(n), rng.standard_normal(n)
+    for t, m, guess in ((0.3, 20, 1.0), (2.0, 12, 0.5), (-0.7, 15, 2.0)):
+        aug = np.zeros((n + 1, n + 1))
+        aug[:n, :n], aug[:n, n] = a, u
+        exact = (sl.expm(t * aug) @ np.append(v, 1.0))[:n]
+        w, g, info = dgphiv(n, m, t, u, v, 1e-10, 1.0, lambda x: a @ x, lambda x, y: float(x @ y), guess)
+        assert np.abs(w - exact).max() < 1e-8 * np.abs(exact).max()
+        assert g > 0 and info["nstep"] >= 1
+
+
+def test_orbital_step_is_orthonormal_and_first_order():
+    """expospfprop keeps the orbitals orthonormal and, for a short step, moves
+    them by dt * (projected RHS) to first order."""
+    from oracle import orbprop_oracle as op
+    sysm = orc.SincSystem(9, 0.6, [[0, 0, 0]], [2.0], toothnbig=30, toothnsmall=8)
+    n = 3
+    phi = orc.seeded_orbitals(sysm, n, seed=62)
+    _, red = sysm.call_twoe_matel00(phi, phi)
+    tally = orc.seeded_tally(n, seed=63)
+    den = orc.seeded_hermitian_psd(n, seed=64)
+    slot = (den, orc.invmatsmooth(den), orc.get_reducedpot(red, tally))
+    dt = 1e-4
+    st = op.OrbPropState(expodim=8, first_stepsize=dt)
+    out, info = op.expospfprop(sysm, st, phi, [slot, slot], 0.0, dt, 0.0, dt, True)
+    assert np.abs(np.conj(out).T @ out - np.eye(n)).max() < 1e-13
+    f = orc.actreduced00(sysm, phi, phi, slot[0], slot[1], slot[2])
+    assert np.abs(out - (phi + dt * f)).max() < 50 * dt * dt * np.abs(f).max() ** 2 + 1e-12
+    assert info["nstep"] == 1 and info["nmult"] == 1 + 8 + 1
+    assert st.icalled == 1 and st.thisexpodim == max(5, math.floor(8 * 0.95))

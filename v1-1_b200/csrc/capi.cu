@@ -64,6 +64,7 @@ Ctx::~Ctx() {
   ws_ci.release();
   ws_ci2.release();
   ws_kry.release();
+  ws_orb.release();
   ci.release();
   if (stream && own_stream) cudaStreamDestroy(stream);
 }

@@ -46,6 +46,18 @@ struct CIState {
   void release();
 };
 
+// saved variables of the orbital exponential propagator (expospfprop)
+struct OrbPropState {
+  int expodim = 10;          // starting Krylov dimension
+  int maxexpodim = 100;      // largest Krylov dimension
+  double expostepfac = 1.2;  // step growth once the dimension is at its maximum
+  double first_stepsize = 0.1;  // par_timestep / littlesteps
+  int icalled = 0;
+  int thisexpodim = 0;
+  int exposet = 0;
+  double tempstepsize = -1.0;
+};
+
 struct Ctx {
   // ---- problem parameters -------------------------------------------------
   int N = 0;             // points per axis (numpoints == gridpoints, nbox=1)
@@ -88,6 +100,8 @@ struct Ctx {
   Workspace ws_state;   // resident mean-field state of the fused orbital-RHS entry
   Workspace ws_ci, ws_ci2;  // CI scratch (KE phi + partials; summed one-body matrix)
   Workspace ws_kry;         // Krylov basis, Hessenberg, Pade output
+  Workspace ws_orb;         // orbital Krylov basis and Jacobian state
+  OrbPropState orb;
   CIState ci;
   int coul_chunk = 0;   // pairs per pass sequence (0 = automatic)
   int coul_fp32 = 0;    // 1: Coulomb passes in FP32 (precision form), 0: FP64
@@ -165,6 +179,33 @@ int mult_reducedpot_range(Ctx& c, const double2* phi, const double2* redpot, int
 int actreduced(Ctx& c, const double2* phi, const double2* proj, const double2* denmat,
                const double2* invdenmat, const double2* redpot, double2 timefac,
                int dentimeflag, int projflag, double zfield, double2* out);
+// D(j,i) = <P_j|T_i> over the grid (split-K, deterministic); part holds
+// orbital_dots_scratch(c) * nspf^2 partial sums
+int orbital_dots_scratch(const Ctx& c);
+int orbital_dots(Ctx& c, const double2* P, const double2* T, double2* D, double2* part);
+// out = in x mat (n x n, column-major)
+int orbital_mix(Ctx& c, const double2* in, const double2* mat, double2* out);
+// out = T - P (M1 + M2) - X D2
+int jac_combine(Ctx& c, const double2* T, const double2* P, const double2* M1, const double2* M2,
+                const double2* X, const double2* D2, double2* out);
+// acc = a acc + b in  (acc = b in when `first`)
+int axpby(Ctx& c, double2* acc, const double2* in, double a, double b, long long len, bool first);
+
+// krylov.cu: (6,6) Pade exponential of a small Hessenberg (mx <= 128)
+int pade_expm(Ctx& c, const double* Hm, int mh, int mx, double t, int col, double* exph, double* Efull,
+              double* gscratch, int* d_ns);
+
+// orbprop.cu: one orbital propagation over [tin, tout] (expospfprop) and the
+// Loewdin re-orthonormalisation (spf_orthogit)
+struct MeanFieldSlot {
+  const double2* denmat;
+  const double2* invdenmat;
+  const double2* reducedpot;
+};
+int expospfprop(Ctx& c, double2* phi, const MeanFieldSlot* slots, double tin, double tout,
+                double firsttime, double lasttime, bool linear, double2 timefac, double ez, double expotol,
+                int* numiters);
+int spf_orthogit(Ctx& c, double2* phi, double* error);
 
 }  // namespace sincgpu
 

@@ -102,18 +102,23 @@ __global__ void __launch_bounds__(kKryThreads) kry_avnorm_kernel(const double* _
 }
 
 // (6,6) Pade exp(t H) with scaling and squaring (DGPADM), H = Hm[0:mx,0:mx]
-// (column-major, leading dimension mh); writes the first column to exph.
-// One CTA; mx <= 64.
+// (column-major, leading dimension mh); writes column `col` of exp(t H) to exph
+// and, when Efull is given, the whole matrix (column-major, leading dimension mx).
+// One CTA; mx <= kMaxPade.  The five mx^2 work matrices live in dynamic shared
+// memory, or in `gscratch` (global, 5 mx^2 doubles) when it is given.
+constexpr int kMaxPade = 128;
 __global__ void __launch_bounds__(kKryThreads) kry_padm_kernel(const double* __restrict__ Hm, int mh, int mx,
                                                                double t, double* __restrict__ exph,
-                                                               int* __restrict__ ns_out) {
+                                                               int* __restrict__ ns_out, int col,
+                                                               double* __restrict__ Efull,
+                                                               double* __restrict__ gscratch) {
   constexpr int ideg = 6;
   extern __shared__ double psm[];  // H, A, B, C, T: 5 mx^2 doubles
   __shared__ double coef[ideg + 1];
-  __shared__ double rows[64];
+  __shared__ double rows[kMaxPade];
   __shared__ int piv_s;
   const int m = mx, mm = m * m, tid = threadIdx.x;
-  double* H = psm;
+  double* H = gscratch ? gscratch : psm;
   double* A = H + mm;
   double* B = A + mm;
   double* C = B + mm;
@@ -121,10 +126,10 @@ __global__ void __launch_bounds__(kKryThreads) kry_padm_kernel(const double* __r
   for (int i = tid; i < mm; i += blockDim.x) H[i] = Hm[(i / m) * mh + (i % m)];
   __syncthreads();
   // infinity norm: max row sum of |H|
-  if (tid < m) {
+  for (int r = tid; r < m; r += blockDim.x) {
     double s = 0.0;
-    for (int j = 0; j < m; ++j) s += fabs(H[tid + m * j]);
-    rows[tid] = s;
+    for (int j = 0; j < m; ++j) s += fabs(H[r + m * j]);
+    rows[r] = s;
   }
   __syncthreads();
   __shared__ double hnorm_s;
@@ -136,7 +141,9 @@ __global__ void __launch_bounds__(kKryThreads) kry_padm_kernel(const double* __r
   __syncthreads();
   const double hnorm = hnorm_s;
   if (hnorm == 0.0) {
-    for (int i = tid; i < m; i += blockDim.x) exph[i] = i == 0 ? 1.0 : 0.0;
+    for (int i = tid; i < m; i += blockDim.x) exph[i] = i == col ? 1.0 : 0.0;
+    if (Efull)
+      for (int e = tid; e < mm; e += blockDim.x) Efull[e] = (e % m) == (e / m) ? 1.0 : 0.0;
     if (tid == 0) *ns_out = 0;
     return;
   }
@@ -239,7 +246,9 @@ __global__ void __launch_bounds__(kKryThreads) kry_padm_kernel(const double* __r
   for (int e = tid; e < mm; e += blockDim.x) P[e] = 2.0 * P[e] + ((e % m) == (e / m) ? 1.0 : 0.0);
   __syncthreads();
   if (ns == 0 && iodd == 1) {
-    for (int i = tid; i < m; i += blockDim.x) exph[i] = -P[i];
+    for (int i = tid; i < m; i += blockDim.x) exph[i] = -P[i + m * col];
+    if (Efull)
+      for (int e = tid; e < mm; e += blockDim.x) Efull[e] = -P[e];
     if (tid == 0) *ns_out = ns;
     return;
   }
@@ -254,7 +263,9 @@ __global__ void __launch_bounds__(kKryThreads) kry_padm_kernel(const double* __r
     for (int e = tid; e < mm; e += blockDim.x) P[e] = T[e];
     __syncthreads();
   }
-  for (int i = tid; i < m; i += blockDim.x) exph[i] = P[i];
+  for (int i = tid; i < m; i += blockDim.x) exph[i] = P[i + m * col];
+  if (Efull)
+    for (int e = tid; e < mm; e += blockDim.x) Efull[e] = P[e];
   if (tid == 0) *ns_out = ns;
 }
 
@@ -282,6 +293,24 @@ __global__ void cscale_kernel(const double2* __restrict__ in, double2 s, int nc,
   if (st && st->mbrk) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nc) out[i] = cmul(s, in[i]);
+}
+
+int pade_expm(Ctx& c, const double* Hm, int mh, int mx, double t, int col, double* exph, double* Efull,
+              double* gscratch, int* d_ns) {
+  SG_CHECK(mx >= 1 && mx <= kMaxPade, SINCGPU_ERANGE, "Pade order %d outside [1,%d]", mx, kMaxPade);
+  static bool attr = false;
+  if (!attr) {
+    SG_CUDA(cudaFuncSetAttribute(kry_padm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(double) * 5 * 64 * 64)));
+    attr = true;
+  }
+  const bool smem = mx <= 64;
+  SG_CHECK(smem || gscratch, SINCGPU_EINVAL, "Pade order %d needs global scratch", mx);
+  const size_t psmem = smem ? sizeof(double) * 5 * (size_t)mx * mx : 0;
+  kry_padm_kernel<<<1, kKryThreads, psmem, c.stream>>>(Hm, mh, mx, t, exph, d_ns, col, Efull,
+                                                       smem ? nullptr : gscratch);
+  SG_LAUNCHED();
+  return SINCGPU_OK;
 }
 
 static double fortran_nint(double x) { return x >= 0 ? std::floor(x + 0.5) : -std::floor(-x + 0.5); }
@@ -365,7 +394,8 @@ int expv_avector(Ctx& c, const double2* v, double2* w, double t, double2 timefac
                                      (int)(sizeof(double) * 5 * 64 * 64)));
         attr = true;
       }
-      kry_padm_kernel<<<1, kKryThreads, psmem, c.stream>>>(Hm, mh, mx, sgn * t_step, exph, d_ns);
+      kry_padm_kernel<<<1, kKryThreads, psmem, c.stream>>>(Hm, mh, mx, sgn * t_step, exph, d_ns, 0, nullptr,
+                                                           nullptr);
       SG_LAUNCHED();
       if (k1 == 0) {
         err_loc = tol;

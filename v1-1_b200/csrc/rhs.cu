@@ -195,6 +195,105 @@ __global__ void __launch_bounds__(256) project_kernel(const double2* __restrict_
       KERNEL<32> __VA_ARGS__;                                             \
   } while (0)
 
+// out(x,i) = T(x,i) - sum_j P_j(x) (M1(j,i) + M2(j,i)) - sum_j X_j(x) D2(j,i)
+// (the projector and projector-derivative terms of the orbital Jacobian)
+template <int NMAX>
+__global__ void __launch_bounds__(256) jac_combine_kernel(const double2* __restrict__ Tm,
+                                                          const double2* __restrict__ Pm,
+                                                          const double2* __restrict__ M1,
+                                                          const double2* __restrict__ M2,
+                                                          const double2* __restrict__ Xm,
+                                                          const double2* __restrict__ D2, int n,
+                                                          long long G, double2* __restrict__ out) {
+  __shared__ double2 sm[NMAX * NMAX], sd[NMAX * NMAX];
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
+    sm[i] = cadd(M1[i], M2[i]);
+    sd[i] = D2[i];
+  }
+  __syncthreads();
+  long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (x >= G) return;
+  double2 p[NMAX], q[NMAX];
+#pragma unroll
+  for (int j = 0; j < NMAX; ++j)
+    if (j < n) {
+      p[j] = Pm[(long long)j * G + x];
+      q[j] = Xm[(long long)j * G + x];
+    }
+  for (int i = 0; i < n; ++i) {
+    double2 a = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int j = 0; j < NMAX; ++j)
+      if (j < n) {
+        const double2 m = sm[j + n * i], d = sd[j + n * i];
+        a.x = fma(p[j].x, m.x, fma(-p[j].y, m.y, a.x));
+        a.y = fma(p[j].x, m.y, fma(p[j].y, m.x, a.y));
+        a.x = fma(q[j].x, d.x, fma(-q[j].y, d.y, a.x));
+        a.y = fma(q[j].x, d.y, fma(q[j].y, d.x, a.y));
+      }
+    out[(long long)i * G + x] = csub(Tm[(long long)i * G + x], a);
+  }
+}
+
+// acc = a * acc + b * in  (or acc = b * in when `first`)
+__global__ void axpby_kernel(double2* __restrict__ acc, const double2* __restrict__ in, double a, double b,
+                             long long len, int first) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double2 v = in[i];
+    if (first) {
+      acc[i] = make_double2(b * v.x, b * v.y);
+    } else {
+      const double2 w = acc[i];
+      acc[i] = make_double2(fma(b, v.x, a * w.x), fma(b, v.y, a * w.y));
+    }
+  }
+}
+
+int orbital_dots_scratch(const Ctx& c) {
+  const int nblk_dots = 4 * 148;
+  const long long xper = ((c.G + nblk_dots - 1) / nblk_dots + DX - 1) / DX * DX;
+  return ceil_div(c.G, xper);
+}
+
+int orbital_dots(Ctx& c, const double2* P, const double2* T, double2* D, double2* part) {
+  const int n = c.nspf;
+  const long long G = c.G;
+  const int nblk_dots = 4 * 148;
+  const long long xper = ((G + nblk_dots - 1) / nblk_dots + DX - 1) / DX * DX;
+  const int nb = ceil_div(G, xper);
+  dots_kernel<<<nb, 256, 0, c.stream>>>(P, T, n, G, xper, part);
+  SG_LAUNCHED();
+  dots_reduce_kernel<<<n * n, 128, 0, c.stream>>>(part, nb, n * n, D);
+  SG_LAUNCHED();
+  return SINCGPU_OK;
+}
+
+int orbital_mix(Ctx& c, const double2* in, const double2* mat, double2* out) {
+  const int n = c.nspf;
+  SG_CHECK(n <= 32, SINCGPU_ERANGE, "at most 32 orbitals");
+  SG_DISPATCH_N(n, mix_kernel, <<<ceil_div(c.G, 256), 256, 0, c.stream>>>(in, mat, n, c.G, out));
+  SG_LAUNCHED();
+  return SINCGPU_OK;
+}
+
+int jac_combine(Ctx& c, const double2* T, const double2* P, const double2* M1, const double2* M2,
+                const double2* X, const double2* D2, double2* out) {
+  const int n = c.nspf;
+  SG_CHECK(n <= 32, SINCGPU_ERANGE, "at most 32 orbitals");
+  SG_DISPATCH_N(n, jac_combine_kernel, <<<ceil_div(c.G, 256), 256, 0, c.stream>>>(T, P, M1, M2, X, D2, n,
+                                                                                  c.G, out));
+  SG_LAUNCHED();
+  return SINCGPU_OK;
+}
+
+int axpby(Ctx& c, double2* acc, const double2* in, double a, double b, long long len, bool first) {
+  axpby_kernel<<<std::min<long long>(ceil_div(len, 256), 148 * 8), 256, 0, c.stream>>>(acc, in, a, b, len,
+                                                                                        first ? 1 : 0);
+  SG_LAUNCHED();
+  return SINCGPU_OK;
+}
+
 int mult_reducedpot_range(Ctx& c, const double2* phi, const double2* redpot, int i0, int ni,
                           double2* out) {
   const int n = c.nspf;

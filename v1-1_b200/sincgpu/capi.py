@@ -79,6 +79,10 @@ _SIGS = {
     "sincgpu_profile_read": ([_P, _P, _P, _I], _I),
     "sincgpu_orbital_rhs_dev": ([_P, _P, _P, _P, _P, _D, _D, _D, _P, _P, _P], _I),
     "sincgpu_orbital_rhs": ([_P, _P, _P, _P, _P, _D, _D, _D, _P, _P], _I),
+    "sincgpu_expospfprop_dev": ([_P, _P, _P, _P, _P, _P, _P, _P, _D, _D, _D, _D, _I, _D, _D, _D, _D, _P], _I),
+    "sincgpu_orbprop_setup": ([_P, _I, _I, _D, _D], _I),
+    "sincgpu_orbprop_state": ([_P, _P, _P, _P, _P], _I),
+    "sincgpu_spf_orthogit_dev": ([_P, _P, _P], _I),
 }
 
 
@@ -340,6 +344,34 @@ class SincProject:
         _call("sincgpu_expoavecprop", self._h, _ptr(a), _ptr(out), float(t), tf.real, tf.imag, int(krylovdim),
               float(tol), float(anorm), float(ezfield), C.byref(g), C.byref(ns))
         return out, g.value, ns.value
+
+    # ------------------------------------------------ orbital propagation
+    def orbprop_setup(self, expodim=10, maxexpodim=100, expostepfac=1.2, first_stepsize=0.1):
+        _call("sincgpu_orbprop_setup", self._h, int(expodim), int(maxexpodim), float(expostepfac),
+              float(first_stepsize))
+
+    def orbprop_state(self) -> dict:
+        d, s, e, i = C.c_int(0), C.c_double(0.0), C.c_int(0), C.c_int(0)
+        _call("sincgpu_orbprop_state", self._h, C.byref(d), C.byref(s), C.byref(e), C.byref(i))
+        return {"thisexpodim": d.value, "tempstepsize": s.value, "exposet": e.value, "icalled": i.value}
+
+    def expospfprop_dev(self, phi, slot0, slot1, tin, tout, firsttime, lasttime, linear=True, timefac=-1j,
+                        ezfield=0.0, expotol=1e-8) -> int:
+        """phi (device, advanced in place); slots are (denmat, invdenmat, reducedpot)
+        device tensors.  Returns the number of Jacobian products."""
+        tf = complex(timefac)
+        s1 = slot1 if slot1 is not None else (None, None, None)
+        it = C.c_int(0)
+        _call("sincgpu_expospfprop_dev", self._h, _ptr(phi), _ptr(slot0[0]), _ptr(slot0[1]), _ptr(slot0[2]),
+              _ptr(s1[0]), _ptr(s1[1]), _ptr(s1[2]), float(tin), float(tout), float(firsttime),
+              float(lasttime), 1 if linear else 0, tf.real, tf.imag, float(ezfield), float(expotol),
+              C.byref(it))
+        return it.value
+
+    def spf_orthogit_dev(self, phi) -> float:
+        e = C.c_double(0.0)
+        _call("sincgpu_spf_orthogit_dev", self._h, _ptr(phi), C.byref(e))
+        return e.value
 
     def getdenmat_dev(self, avector, denmat, invdenmat, denreg=1e-10):
         _call("sincgpu_getdenmat_dev", self._h, _ptr(avector), _ptr(denmat), _ptr(invdenmat), float(denreg))
