@@ -233,6 +233,32 @@ int sincgpu_walks_sizes(sincgpu_walks* walks, long long* sizes, int nsizes);
 #define SINCGPU_T_DOUBLEDIAGHOP 18
 int sincgpu_walks_table(sincgpu_walks* walks, int which, int* out);
 
+/* Spin walks, spin sets and S^2 projectors of the allspinproject=1 path
+ * (MCTDH.SRC/spinwalks.f90: getnumspinwalks :302-388, spinwalks :86-153,
+ * spinsets_first :156-299, configspin_matel :390-414, configspinset_projector
+ * :432-642).  spinrestrictval is 2S; a negative value selects |restrictms| (the
+ * reference's default high spin, MCTDH.SRC/getparams.f90:190-192).  Sets whose
+ * projector has rank 0 are eliminated, as the reference does.  Call before
+ * sincgpu_ci_attach so that the projectors are uploaded. */
+int sincgpu_walks_spin(sincgpu_walks* walks, int spinrestrictval);
+
+/* sizes[0..5] = number of kept spin sets, total spin rank (numspinconfig), total
+ * spin walks, projector entries (sum of set size^2), eliminated configurations,
+ * largest set size. */
+int sincgpu_walks_spin_sizes(sincgpu_walks* walks, long long* sizes, int nsizes);
+
+/* Spin tables as int32 (1-based configurations as in the reference): */
+#define SINCGPU_T_NUMSPINWALKS 19     /* numconfig */
+#define SINCGPU_T_SPINWALK 20         /* total spin walks, per config in order */
+#define SINCGPU_T_SPINWALKDIRPHASE 21 /* total spin walks */
+#define SINCGPU_T_SPINSETOFF 22       /* kept sets + 1 (CSR offsets into SPINSETS) */
+#define SINCGPU_T_SPINSETS 23         /* configurations of the kept sets */
+#define SINCGPU_T_SPINSETRANK 24      /* kept sets */
+#define SINCGPU_T_SPINELIMINATED 25   /* configurations of eliminated sets */
+
+/* Projectors of the kept sets, concatenated, each size x size row-major. */
+int sincgpu_walks_spinprojectors(sincgpu_walks* walks, double* out);
+
 /* Uploads the tables to the context's device (walk_init after hops in
  * MCTDH.SRC/mctdhf.f90:837-853).  The walks handle may be destroyed afterwards. */
 int sincgpu_ci_attach(sincgpu_ctx* ctx, sincgpu_walks* walks);
@@ -284,6 +310,13 @@ int sincgpu_expoavecprop_dev(sincgpu_ctx* ctx, const double* avec_in, double* av
 int sincgpu_expoavecprop(sincgpu_ctx* ctx, const double* avec_in, double* avec_out, double t,
                          double timefac_re, double timefac_im, int krylovdim, double tol, double anorm,
                          double ezfield, double* stepguess, int* nstep);
+
+/* basis_project with allspinproject=1 (MCTDH.SRC/spin.f90:643-660 ->
+ * configspin_project_general :339-375): each spin set's coefficients are
+ * replaced by P_set times them; configurations of eliminated sets are zeroed.
+ * Needs walk tables with spin sets attached. */
+int sincgpu_spin_project_dev(sincgpu_ctx* ctx, double* avector);
+int sincgpu_spin_project(sincgpu_ctx* ctx, const double* avector_in, double* avector_out);
 
 /* One orbital-RHS evaluation from the A-vector: denmat, invdenmat and the 2-RDM
  * (get_allden, MCTDH.SRC/mean.f90:467-477), then sincgpu_orbital_rhs_dev. */

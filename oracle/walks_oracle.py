@@ -331,6 +331,112 @@ class CIWalks:
         return out
 
 
+class SpinSets:
+    """Spin walks, spin sets and the S^2 projectors of the reference's
+    allspinproject=1 path (MCTDH.SRC/spinwalks.f90: getnumspinwalks 302-388,
+    spinwalks 86-153, spinsets_first 156-299, configspin_matel 390-414,
+    spinallowed 417-429, configspinset_projector 432-642) and its application
+    configspin_project_general (MCTDH.SRC/spin.f90:339-375).
+    spinrestrictval is 2S (default |restrictms|, getparams.f90:190-192)."""
+
+    def __init__(self, ww: CIWalks, spinrestrictval: int | None = None):
+        self.ww = ww
+        n = ww.numpart
+        srv = abs(ww.restrictms) if spinrestrictval is None else spinrestrictval
+        if srv < abs(ww.restrictms):
+            srv = abs(ww.restrictms)
+        self.spinrestrictval = srv
+        nc = ww.numconfig
+        self.msvalue = np.zeros(nc, dtype=np.int64)
+        self.unpaired = []
+        for c in range(nc):
+            cfg = [int(x) for x in ww.configlist[c]]
+            self.msvalue[c] = sum(cfg[2 * i + 1] * 2 - 3 for i in range(n))
+            up = []
+            for i in range(n):
+                if not any(j != i and cfg[2 * j] == cfg[2 * i] for j in range(n)):
+                    up.append(i + 1)
+            self.unpaired.append(up)
+        # spin walks: flip two unpaired electrons of opposite spin
+        self.spinwalk, self.spinwalkdirphase = [], []
+        for c in range(nc):
+            walks, phases = [], []
+            up = self.unpaired[c]
+            for ii in range(len(up)):
+                this = [int(x) for x in ww.configlist[c]]
+                idof = up[ii]
+                first = this[2 * idof - 1]
+                this[2 * idof - 1] = this[2 * idof - 1] % 2 + 1
+                for jj in range(ii + 1, len(up)):
+                    that = list(this)
+                    jdof = up[jj]
+                    if that[2 * jdof - 1] != first:
+                        that[2 * jdof - 1] = that[2 * jdof - 1] % 2 + 1
+                        ph = reorder(that, n)
+                        if ww.allowed(that):
+                            walks.append(ww.getconfiguration(that))
+                            phases.append(ph)
+            self.spinwalk.append(walks)
+            self.spinwalkdirphase.append(phases)
+        # spin sets: connected components grown level by level from the lowest config
+        taken = np.zeros(nc + 1, dtype=bool)
+        sets = []
+        for i in range(1, nc + 1):
+            if taken[i]:
+                continue
+            taken[i] = True
+            temp = [i]
+            prev, cur = 0, 1
+            while True:
+                add = 0
+                for j in range(prev, cur):
+                    for w in self.spinwalk[temp[j] - 1]:
+                        if w not in temp[:cur + add]:
+                            temp.append(w)
+                            add += 1
+                            taken[w] = True
+                prev, cur = cur, cur + add
+                if add == 0:
+                    break
+            sets.append(temp)
+        # S^2 in each set; keep the eigenvectors with S(S+1), projector V V^T
+        target = srv / 2.0 * (srv / 2.0 + 1.0)
+        self.sets, self.ranks, self.projectors = [], [], []
+        self.eliminated = []
+        for st in sets:
+            m = len(st)
+            s2 = np.zeros((m, m))
+            for jj in range(m):
+                cj = st[jj] - 1
+                s2[jj, jj] = self.msvalue[cj] ** 2 / 4.0 + len(self.unpaired[cj]) / 2.0
+                for ii in range(m):
+                    if ii == jj:
+                        continue
+                    for w, ph in zip(self.spinwalk[cj], self.spinwalkdirphase[cj]):
+                        if w == st[ii]:
+                            s2[ii, jj] = ph
+                            break
+            vals, vecs = np.linalg.eigh(s2)
+            keep = np.abs(vals - target) < 1e-3
+            if not keep.any():
+                self.eliminated.extend(st)
+                continue
+            v = vecs[:, keep]
+            self.sets.append(st)
+            self.ranks.append(int(keep.sum()))
+            self.projectors.append(v @ v.T)
+        self.numspinconfig = int(sum(self.ranks))
+
+    def project(self, avector):
+        """basis_project with allspinproject=1 (MCTDH.SRC/spin.f90:643-660)."""
+        a = np.asarray(avector, dtype=np.complex128)
+        out = np.zeros_like(a)
+        for st, p in zip(self.sets, self.projectors):
+            idx = np.array(st) - 1
+            out[idx] += p @ a[idx]
+        return out
+
+
 def ci_count(numelec: int, nspf: int, restrictms: int) -> int:
     """Closed form: C(n, n_alpha) * C(n, n_beta)."""
     from math import comb

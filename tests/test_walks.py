@@ -73,3 +73,40 @@ def test_bad_spin_projection_rejected(built_lib):
     from sincgpu import WalkTables, SincGpuError
     with pytest.raises(SincGpuError):
         WalkTables(4, 6, 1)   # 4 electrons cannot have 2*M_s = 1
+
+
+def weyl_dim(norb, nelec, two_s):
+    """Weyl-Paldus count of spin-adapted configurations (CSFs) with total spin S."""
+    s2 = two_s
+    return (s2 + 1) * comb(norb + 1, (nelec - s2) // 2) * comb(norb + 1, (nelec + s2) // 2 + 1) // (norb + 1)
+
+
+@pytest.mark.parametrize("numelec,nspf,ms,two_s", [(2, 4, 0, 0), (2, 4, 0, 2), (3, 4, 1, 1), (3, 4, 1, 3),
+                                                   (4, 5, 0, 0), (4, 5, 0, 2), (4, 6, 2, 2), (4, 6, 0, 4),
+                                                   (5, 6, -1, 1), (6, 6, 0, 0)])
+def test_spin_tables_bit_exact_and_weyl(built_lib, numelec, nspf, ms, two_s):
+    """Spin walks, spin sets and eliminated sets match the oracle exactly; the
+    projectors agree to rounding; the spin-adapted rank is Weyl's dimension."""
+    from oracle.walks_oracle import SpinSets
+    from sincgpu import WalkTables
+    ow = CIWalks(numelec, nspf, ms)
+    sp = SpinSets(ow, two_s)
+    wt = WalkTables(numelec, nspf, ms).build_spin(two_s)
+    assert wt.numspinconfig == sp.numspinconfig == weyl_dim(nspf, numelec, two_s)
+    assert wt.table("numspinwalks").tolist() == [len(x) for x in sp.spinwalk]
+    assert wt.table("spinwalk").tolist() == [v for x in sp.spinwalk for v in x]
+    assert wt.table("spinwalkdirphase").tolist() == [v for x in sp.spinwalkdirphase for v in x]
+    assert wt.table("spinsets").tolist() == [v for st in sp.sets for v in st]
+    assert np.diff(wt.table("spinset_off")).tolist() == [len(st) for st in sp.sets]
+    assert wt.table("spinsetrank").tolist() == sp.ranks
+    assert wt.table("spin_eliminated").tolist() == sp.eliminated
+    for p_lib, p_orc in zip(wt.spin_projectors(), sp.projectors):
+        assert np.abs(p_lib - p_orc).max() < 1e-13
+    wt.close()
+
+
+def test_spin_projector_is_idempotent_symmetric():
+    from oracle.walks_oracle import SpinSets
+    sp = SpinSets(CIWalks(4, 6, 0), 2)
+    for p in sp.projectors:
+        assert np.abs(p @ p - p).max() < 1e-13 and np.abs(p - p.T).max() == 0.0

@@ -88,10 +88,59 @@ int sincgpu_walks_table(sincgpu_walks* h, int which, int* out) {
     case SINCGPU_T_DOUBLEHOPWALKEND: copy_out(w.doublehopwalkend, out); break;
     case SINCGPU_T_SINGLEDIAGHOP: copy_out(w.singlediaghop, out); break;
     case SINCGPU_T_DOUBLEDIAGHOP: copy_out(w.doublediaghop, out); break;
+    case SINCGPU_T_NUMSPINWALKS: copy_out(w.numspinwalks, out); break;
+    case SINCGPU_T_SPINWALK: copy_out(w.spinwalk, out); break;
+    case SINCGPU_T_SPINWALKDIRPHASE: copy_out(w.spinwalkdirphase, out); break;
+    case SINCGPU_T_SPINSETOFF: copy_out(w.spinset_off, out); break;
+    case SINCGPU_T_SPINSETS: copy_out(w.spinsets, out); break;
+    case SINCGPU_T_SPINSETRANK: copy_out(w.spinsetrank, out); break;
+    case SINCGPU_T_SPINELIMINATED: copy_out(w.spin_eliminated, out); break;
     default:
       set_error("unknown walk table id %d", which);
       return SINCGPU_EINVAL;
   }
+  return SINCGPU_OK;
+}
+
+int sincgpu_walks_spin(sincgpu_walks* h, int spinrestrictval) {
+  SG_CHECK(h, SINCGPU_EINVAL, "null argument");
+  return build_spin(h->w, spinrestrictval);
+}
+
+int sincgpu_walks_spin_sizes(sincgpu_walks* h, long long* s, int n) {
+  SG_CHECK(h && s, SINCGPU_EINVAL, "null argument");
+  const Walks& w = h->w;
+  SG_CHECK(w.spinrestrictval >= 0, SINCGPU_ESTATE, "spin tables not built");
+  long long v[6] = {(long long)w.spinsetrank.size(), w.numspinconfig, (long long)w.spinwalk.size(),
+                    (long long)w.spinproj.size(), (long long)w.spin_eliminated.size(), w.maxspinsetsize};
+  for (int i = 0; i < n && i < 6; ++i) s[i] = v[i];
+  return SINCGPU_OK;
+}
+
+int sincgpu_walks_spinprojectors(sincgpu_walks* h, double* out) {
+  SG_CHECK(h && out, SINCGPU_EINVAL, "null argument");
+  SG_CHECK(h->w.spinrestrictval >= 0, SINCGPU_ESTATE, "spin tables not built");
+  std::memcpy(out, h->w.spinproj.data(), sizeof(double) * h->w.spinproj.size());
+  return SINCGPU_OK;
+}
+
+int sincgpu_spin_project_dev(sincgpu_ctx* h, double* avector) {
+  CTX_CHECK(h);
+  SG_CHECK(avector, SINCGPU_EINVAL, "null argument");
+  return ci_spin_project(h->c, (double2*)avector);
+}
+
+int sincgpu_spin_project(sincgpu_ctx* h, const double* in, double* out) {
+  CTX_CHECK(h);
+  Ctx& c = h->c;
+  SG_CHECK(c.ci.attached, SINCGPU_ESTATE, "no walk tables attached");
+  SG_CHECK(in && out, SINCGPU_EINVAL, "null argument");
+  const size_t b = sizeof(double2) * c.ci.nc;
+  SG_TRY(c.ws_io.ensure(b));
+  SG_CUDA(cudaMemcpyAsync(c.ws_io.ptr, in, b, cudaMemcpyHostToDevice, c.stream));
+  SG_TRY(ci_spin_project(c, (double2*)c.ws_io.ptr));
+  SG_CUDA(cudaMemcpyAsync(out, c.ws_io.ptr, b, cudaMemcpyDeviceToHost, c.stream));
+  SG_CUDA(cudaStreamSynchronize(c.stream));
   return SINCGPU_OK;
 }
 

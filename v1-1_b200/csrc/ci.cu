@@ -127,14 +127,83 @@ int ci_attach(Ctx& c, const Walks& w) {
     SG_CUDA(cudaMalloc(&s.xone, sizeof(double2) * std::max(1LL, s.nsh)));
     SG_CUDA(cudaMalloc(&s.xz, sizeof(double2) * std::max(1LL, s.nsh)));
   }
+  // spin sets and projectors (allspinproject=1), when built
+  s.spin = false;
+  if (w.spinrestrictval >= 0) {
+    std::vector<int> sets0(w.spinsets.size()), elim0(w.spin_eliminated.size());
+    for (size_t i = 0; i < sets0.size(); ++i) sets0[i] = w.spinsets[i] - 1;
+    for (size_t i = 0; i < elim0.size(); ++i) elim0[i] = w.spin_eliminated[i] - 1;
+    s.nspinsets = (int)w.spinsetrank.size();
+    s.nspinelim = (int)elim0.size();
+    s.maxspinset = w.maxspinsetsize;
+    SG_CHECK(s.maxspinset <= 4096, SINCGPU_ERANGE, "spin set of %d configurations exceeds 4096",
+             s.maxspinset);
+    SG_TRY(upload((void**)&s.sp_set_off, w.spinset_off.data(), sizeof(long long) * w.spinset_off.size()));
+    // empty tables stay null (upload of 0 bytes); the kernel touches only non-empty ones
+    SG_TRY(upload((void**)&s.sp_sets, sets0.data(), sizeof(int) * sets0.size()));
+    SG_TRY(upload((void**)&s.sp_proj_off, w.spinproj_off.data(), sizeof(long long) * w.spinproj_off.size()));
+    SG_TRY(upload((void**)&s.sp_proj, w.spinproj.data(), sizeof(double) * w.spinproj.size()));
+    SG_TRY(upload((void**)&s.sp_elim, elim0.data(), sizeof(int) * elim0.size()));
+    s.spin = true;
+  }
   s.attached = true;
   s.assembled = false;
   return SINCGPU_OK;
 }
 
+// basis_project with allspinproject=1 (configspin_project_general,
+// MCTDH.SRC/spin.f90:339-375): a(set) <- P_set a(set) for every kept spin set,
+// one CTA per set; configurations of eliminated (rank-0) sets become zero.
+__global__ void __launch_bounds__(256) spin_project_kernel(const long long* __restrict__ set_off,
+                                                           const int* __restrict__ sets,
+                                                           const long long* __restrict__ proj_off,
+                                                           const double* __restrict__ proj, int nsets,
+                                                           const int* __restrict__ elim, int nelim,
+                                                           double2* __restrict__ a) {
+  extern __shared__ double2 v[];
+  const int sidx = blockIdx.x;
+  if (sidx >= nsets) {  // trailing CTAs zero the eliminated configurations
+    for (int i = (sidx - nsets) * blockDim.x + threadIdx.x; i < nelim; i += (gridDim.x - nsets) * blockDim.x)
+      a[elim[i]] = make_double2(0.0, 0.0);
+    return;
+  }
+  const long long b = set_off[sidx];
+  const int m = (int)(set_off[sidx + 1] - b);
+  for (int i = threadIdx.x; i < m; i += blockDim.x) v[i] = a[sets[b + i]];
+  __syncthreads();
+  const double* P = proj + proj_off[sidx];
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int j = 0; j < m; ++j) {
+      const double p = P[(long long)i * m + j];
+      acc.x = fma(p, v[j].x, acc.x);
+      acc.y = fma(p, v[j].y, acc.y);
+    }
+    a[sets[b + i]] = acc;
+  }
+}
+
+int ci_spin_project(Ctx& c, double2* a) {
+  CIState& s = c.ci;
+  SG_CHECK(s.attached && s.spin, SINCGPU_ESTATE, "no spin projectors attached (build them with sincgpu_walks_spin)");
+  const int zb = s.nspinelim > 0 ? std::min(ceil_div(s.nspinelim, 256), 64) : 0;
+  if (s.nspinsets + zb == 0) return SINCGPU_OK;
+  static bool attr = false;
+  if (!attr) {
+    SG_CUDA(cudaFuncSetAttribute(spin_project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(double2) * 4096)));
+    attr = true;
+  }
+  spin_project_kernel<<<s.nspinsets + zb, 256, sizeof(double2) * std::max(1, s.maxspinset), c.stream>>>(
+      s.sp_set_off, s.sp_sets, s.sp_proj_off, s.sp_proj, s.nspinsets, s.sp_elim, s.nspinelim, a);
+  SG_LAUNCHED();
+  return SINCGPU_OK;
+}
+
 void CIState::release() {
   void* ptrs[] = {den_off, den_ent, tal_off, tal_ent, sidx, didx, swb, dwb, swn, dwn,
-                  shop, dhop, shop_off, dhop_off, xpot, xone, xz};
+                  shop, dhop, shop_off, dhop_off, xpot, xone, xz,
+                  sp_set_off, sp_sets, sp_proj_off, sp_proj, sp_elim};
   for (void* p : ptrs) cudaFree(p);
   *this = CIState();
 }

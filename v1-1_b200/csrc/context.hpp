@@ -43,6 +43,12 @@ struct CIState {
   int *shop = nullptr, *dhop = nullptr;     // hop target config (0-based)
   long long *shop_off = nullptr, *dhop_off = nullptr;  // hops of each config
   double2 *xpot = nullptr, *xone = nullptr, *xz = nullptr;  // assembled per-hop values
+  // spin sets (allspinproject=1): CSR of 0-based configs, row-major projectors
+  bool spin = false;
+  int nspinsets = 0, nspinelim = 0, maxspinset = 0;
+  long long *sp_set_off = nullptr, *sp_proj_off = nullptr;
+  int *sp_sets = nullptr, *sp_elim = nullptr;
+  double* sp_proj = nullptr;
   void release();
 };
 
@@ -190,6 +196,9 @@ int jac_combine(Ctx& c, const double2* T, const double2* P, const double2* M1, c
                 const double2* X, const double2* D2, double2* out);
 // acc = a acc + b in  (acc = b in when `first`)
 int axpby(Ctx& c, double2* acc, const double2* in, double a, double b, long long len, bool first);
+
+// ci.cu: spin projection of an A-vector in place (basis_project, allspinproject=1)
+int ci_spin_project(Ctx& c, double2* a);
 
 // krylov.cu: (6,6) Pade exponential of a small Hessenberg (mx <= 128)
 int pade_expm(Ctx& c, const double* Hm, int mh, int mx, double t, int col, double* exph, double* Efull,

@@ -7,10 +7,18 @@
 //   walks / getnumwalks  MCTDH.SRC/walks.f90:149-506, 510-759 (per-config sort
 //                        getlistorder 453-483: ascending target, ties last-first)
 //   hops                 MCTDH.SRC/walks.f90:761-993
+//   spin projection      MCTDH.SRC/spinwalks.f90 (getnumspinwalks 302-388,
+//                        spinwalks 86-153, spinsets_first 156-299,
+//                        configspin_matel 390-414, configspinset_projector
+//                        432-642); the S^2 eigenproblem of each set is solved
+//                        by cyclic Jacobi rotations instead of LAPACK dsyev
+//                        (the projector onto an eigenspace does not depend on
+//                        the solver beyond rounding)
 // getconfiguration (newconfig.f90:49-131) returns the unique index of an
 // allowed, ordered configuration; here that lookup is a hash of the set of
 // occupied spin-orbitals (a 64-bit mask, nspf <= 32).
 #include <algorithm>
+#include <cmath>
 #include <thread>
 #include <functional>
 #include <unordered_map>
@@ -312,6 +320,196 @@ int build_walks(Walks& w, int numelec, int nspf, int restrictms, int nthreads) {
                   w.singlehopwalkstart, w.singlehopwalkend, w.singlediaghop);
   group_hops<int>(w.doublewalk, w.dcol, w.numdoublewalks, nc, w.doublehop_off, w.doublehop,
                   w.doublehopwalkstart, w.doublehopwalkend, w.doublediaghop);
+  return SINCGPU_OK;
+}
+
+namespace {
+
+// cyclic Jacobi eigen-decomposition of a real symmetric m x m matrix (row-major);
+// on return vals holds the eigenvalues and column k of V the k-th eigenvector
+void jacobi_eigen(int m, std::vector<double>& A, std::vector<double>& V, std::vector<double>& vals) {
+  V.assign((size_t)m * m, 0.0);
+  for (int i = 0; i < m; ++i) V[(size_t)i * m + i] = 1.0;
+  double norm = 0.0;
+  for (double x : A) norm += x * x;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0;
+    for (int p = 0; p < m; ++p)
+      for (int q = p + 1; q < m; ++q) off += A[(size_t)p * m + q] * A[(size_t)p * m + q];
+    if (off <= 1e-32 * norm || off == 0.0) break;
+    for (int p = 0; p < m; ++p)
+      for (int q = p + 1; q < m; ++q) {
+        const double apq = A[(size_t)p * m + q];
+        if (apq == 0.0) continue;
+        const double theta = (A[(size_t)q * m + q] - A[(size_t)p * m + p]) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+        for (int k = 0; k < m; ++k) {  // columns p, q
+          const double akp = A[(size_t)k * m + p], akq = A[(size_t)k * m + q];
+          A[(size_t)k * m + p] = c * akp - sn * akq;
+          A[(size_t)k * m + q] = sn * akp + c * akq;
+        }
+        for (int k = 0; k < m; ++k) {  // rows p, q
+          const double apk = A[(size_t)p * m + k], aqk = A[(size_t)q * m + k];
+          A[(size_t)p * m + k] = c * apk - sn * aqk;
+          A[(size_t)q * m + k] = sn * apk + c * aqk;
+        }
+        for (int k = 0; k < m; ++k) {
+          const double vkp = V[(size_t)k * m + p], vkq = V[(size_t)k * m + q];
+          V[(size_t)k * m + p] = c * vkp - sn * vkq;
+          V[(size_t)k * m + q] = sn * vkp + c * vkq;
+        }
+      }
+  }
+  vals.resize(m);
+  for (int i = 0; i < m; ++i) vals[i] = A[(size_t)i * m + i];
+}
+
+}  // namespace
+
+int build_spin(Walks& w, int spinrestrictval) {
+  SG_CHECK(w.numconfig > 0, SINCGPU_ESTATE, "walk tables not built");
+  const int n = w.numpart, nc = w.numconfig;
+  int srv = spinrestrictval < 0 ? std::abs(w.restrictms) : spinrestrictval;
+  if (srv < std::abs(w.restrictms)) srv = std::abs(w.restrictms);  // getparams.f90:190-192
+  SG_CHECK((srv - std::abs(w.restrictms)) % 2 == 0 && srv <= n, SINCGPU_EINVAL,
+           "2S = %d not reachable with %d electrons and 2Ms = %d", srv, n, w.restrictms);
+  // index of every configuration by its spin-orbital mask
+  std::unordered_map<uint64_t, int> index;
+  index.reserve((size_t)nc * 2);
+  for (int c = 0; c < nc; ++c) {
+    uint64_t m = 0;
+    const int* cf = &w.configlist[(size_t)c * 2 * n];
+    for (int j = 0; j < n; ++j) m |= 1ull << (iind(cf[2 * j], cf[2 * j + 1]) - 1);
+    index[m] = c + 1;
+  }
+  Builder b(w);
+  std::vector<int> msvalue(nc);
+  std::vector<std::vector<int>> unpaired(nc);
+  for (int c = 0; c < nc; ++c) {
+    const int* cf = &w.configlist[(size_t)c * 2 * n];
+    int ms = 0;
+    for (int i = 0; i < n; ++i) {
+      ms += cf[2 * i + 1] * 2 - 3;
+      bool paired = false;
+      for (int j = 0; j < n; ++j)
+        if (j != i && cf[2 * j] == cf[2 * i]) {
+          paired = true;
+          break;
+        }
+      if (!paired) unpaired[c].push_back(i + 1);
+    }
+    msvalue[c] = ms;
+  }
+  // spin walks: flip one pair of unpaired electrons with opposite spins
+  w.spinrestrictval = srv;
+  w.numspinwalks.assign(nc, 0);
+  w.spinwalk_off.assign(nc + 1, 0);
+  w.spinwalk.clear();
+  w.spinwalkdirphase.clear();
+  std::vector<int> cfg(2 * n), that(2 * n);
+  for (int c = 0; c < nc; ++c) {
+    const auto& up = unpaired[c];
+    for (size_t ii = 0; ii < up.size(); ++ii) {
+      cfg.assign(&w.configlist[(size_t)c * 2 * n], &w.configlist[(size_t)c * 2 * n] + 2 * n);
+      const int idof = up[ii];
+      const int first = cfg[2 * idof - 1];
+      cfg[2 * idof - 1] = cfg[2 * idof - 1] % 2 + 1;
+      for (size_t jj = ii + 1; jj < up.size(); ++jj) {
+        that = cfg;
+        const int jdof = up[jj];
+        if (that[2 * jdof - 1] == first) continue;
+        that[2 * jdof - 1] = that[2 * jdof - 1] % 2 + 1;
+        const int ph = reorder(that.data(), n);
+        if (!b.allowed(that.data())) continue;
+        uint64_t m = 0;
+        for (int j = 0; j < n; ++j) m |= 1ull << (iind(that[2 * j], that[2 * j + 1]) - 1);
+        auto it = index.find(m);
+        SG_CHECK(it != index.end(), SINCGPU_ESTATE, "spin walk target not in the configuration list");
+        w.spinwalk.push_back(it->second);
+        w.spinwalkdirphase.push_back(ph);
+        ++w.numspinwalks[c];
+      }
+    }
+    w.spinwalk_off[c + 1] = (long long)w.spinwalk.size();
+  }
+  // spin sets: components grown level by level from the lowest untaken config
+  std::vector<char> taken(nc + 1, 0);
+  std::vector<std::vector<int>> sets;
+  for (int i = 1; i <= nc; ++i) {
+    if (taken[i]) continue;
+    taken[i] = 1;
+    std::vector<int> temp{i};
+    size_t prev = 0, cur = 1;
+    while (true) {
+      size_t add = 0;
+      for (size_t j = prev; j < cur; ++j) {
+        const int cj = temp[j] - 1;
+        for (long long k = w.spinwalk_off[cj]; k < w.spinwalk_off[cj + 1]; ++k) {
+          const int t = w.spinwalk[k];
+          if (std::find(temp.begin(), temp.begin() + (cur + add), t) == temp.begin() + (cur + add)) {
+            SG_CHECK(!taken[t], SINCGPU_ESTATE, "spin set overlap at config %d", t);
+            temp.push_back(t);
+            taken[t] = 1;
+            ++add;
+          }
+        }
+      }
+      prev = cur;
+      cur += add;
+      if (add == 0) break;
+    }
+    sets.push_back(std::move(temp));
+  }
+  // S^2 per set, eigenvectors with S(S+1), projector
+  const double target = srv / 2.0 * (srv / 2.0 + 1.0);
+  w.spinset_off.assign(1, 0);
+  w.spinsets.clear();
+  w.spinsetrank.clear();
+  w.spinproj_off.assign(1, 0);
+  w.spinproj.clear();
+  w.spin_eliminated.clear();
+  w.numspinconfig = 0;
+  w.maxspinsetsize = 0;
+  std::vector<double> A, V, vals;
+  for (const auto& st : sets) {
+    const int m = (int)st.size();
+    w.maxspinsetsize = std::max(w.maxspinsetsize, m);
+    A.assign((size_t)m * m, 0.0);
+    for (int jj = 0; jj < m; ++jj) {
+      const int cj = st[jj] - 1;
+      A[(size_t)jj * m + jj] = msvalue[cj] * (double)msvalue[cj] / 4.0 + unpaired[cj].size() / 2.0;
+      for (int ii = 0; ii < m; ++ii) {
+        if (ii == jj) continue;
+        for (long long k = w.spinwalk_off[cj]; k < w.spinwalk_off[cj + 1]; ++k)
+          if (w.spinwalk[k] == st[ii]) {
+            A[(size_t)ii * m + jj] = w.spinwalkdirphase[k];
+            break;
+          }
+      }
+    }
+    jacobi_eigen(m, A, V, vals);
+    std::vector<int> keep;
+    for (int k = 0; k < m; ++k)
+      if (std::fabs(vals[k] - target) < 1e-3) keep.push_back(k);
+    if (keep.empty()) {
+      w.spin_eliminated.insert(w.spin_eliminated.end(), st.begin(), st.end());
+      continue;
+    }
+    w.spinsets.insert(w.spinsets.end(), st.begin(), st.end());
+    w.spinset_off.push_back((long long)w.spinsets.size());
+    w.spinsetrank.push_back((int)keep.size());
+    w.numspinconfig += (long long)keep.size();
+    const size_t base = w.spinproj.size();
+    w.spinproj.resize(base + (size_t)m * m, 0.0);
+    for (int ii = 0; ii < m; ++ii)
+      for (int jj = 0; jj < m; ++jj) {
+        double s = 0.0;
+        for (int k : keep) s += V[(size_t)ii * m + k] * V[(size_t)jj * m + k];
+        w.spinproj[base + (size_t)ii * m + jj] = s;
+      }
+    w.spinproj_off.push_back((long long)w.spinproj.size());
+  }
   return SINCGPU_OK;
 }
 

@@ -83,6 +83,11 @@ _SIGS = {
     "sincgpu_orbprop_setup": ([_P, _I, _I, _D, _D], _I),
     "sincgpu_orbprop_state": ([_P, _P, _P, _P, _P], _I),
     "sincgpu_spf_orthogit_dev": ([_P, _P, _P], _I),
+    "sincgpu_walks_spin": ([_P, _I], _I),
+    "sincgpu_walks_spin_sizes": ([_P, _P, _I], _I),
+    "sincgpu_walks_spinprojectors": ([_P, _P], _I),
+    "sincgpu_spin_project_dev": ([_P, _P], _I),
+    "sincgpu_spin_project": ([_P, _P, _P], _I),
 }
 
 
@@ -372,6 +377,16 @@ class SincProject:
         e = C.c_double(0.0)
         _call("sincgpu_spf_orthogit_dev", self._h, _ptr(phi), C.byref(e))
         return e.value
+
+    def spin_project(self, avector):
+        """basis_project (allspinproject=1) of a host A-vector; returns the projection."""
+        a = _f(avector).reshape(-1)
+        out = np.zeros_like(a)
+        _call("sincgpu_spin_project", self._h, _ptr(a), _ptr(out))
+        return out
+
+    def spin_project_dev(self, avector):
+        _call("sincgpu_spin_project_dev", self._h, _ptr(avector))
 
     def getdenmat_dev(self, avector, denmat, invdenmat, denreg=1e-10):
         _call("sincgpu_getdenmat_dev", self._h, _ptr(avector), _ptr(denmat), _ptr(invdenmat), float(denreg))

@@ -17,6 +17,8 @@ TABLES = {
     "doublewalk": 8, "singlehop_off": 9, "singlehop": 10, "singlehopwalkstart": 11,
     "singlehopwalkend": 12, "doublehop_off": 13, "doublehop": 14, "doublehopwalkstart": 15,
     "doublehopwalkend": 16, "singlediaghop": 17, "doublediaghop": 18,
+    "numspinwalks": 19, "spinwalk": 20, "spinwalkdirphase": 21, "spinset_off": 22, "spinsets": 23,
+    "spinsetrank": 24, "spin_eliminated": 25,
 }
 
 
@@ -31,6 +33,26 @@ class WalkTables:
         _call("sincgpu_walks_sizes", self._h, s.ctypes.data, 6)
         (self.numconfig, self.numpart, self.totsinglewalks, self.totdoublewalks,
          self.totsinglehops, self.totdoublehops) = (int(v) for v in s)
+
+    def build_spin(self, spinrestrictval: int = -1):
+        """Spin walks, sets and S^2 projectors (allspinproject=1); 2S defaults to |restrictms|."""
+        _call("sincgpu_walks_spin", self._h, int(spinrestrictval))
+        s = np.zeros(6, dtype=np.int64)
+        _call("sincgpu_walks_spin_sizes", self._h, s.ctypes.data, 6)
+        (self.numspinsets, self.numspinconfig, self.totspinwalks, self.spinprojsize, self.numspinelim,
+         self.maxspinsetsize) = (int(v) for v in s)
+        return self
+
+    def spin_projectors(self) -> list[np.ndarray]:
+        flat = np.zeros(max(self.spinprojsize, 1))
+        _call("sincgpu_walks_spinprojectors", self._h, flat.ctypes.data)
+        off = self.table("spinset_off")
+        out, p = [], 0
+        for k in range(self.numspinsets):
+            m = int(off[k + 1] - off[k])
+            out.append(flat[p:p + m * m].reshape(m, m))
+            p += m * m
+        return out
 
     def close(self):
         if self._h:
@@ -53,6 +75,11 @@ class WalkTables:
             "singlehop_off": nc + 1, "singlehop": sh, "singlehopwalkstart": sh, "singlehopwalkend": sh,
             "doublehop_off": nc + 1, "doublehop": dh, "doublehopwalkstart": dh, "doublehopwalkend": dh,
             "singlediaghop": nc, "doublediaghop": nc,
+            "numspinwalks": nc, "spinwalk": getattr(self, "totspinwalks", 0),
+            "spinwalkdirphase": getattr(self, "totspinwalks", 0),
+            "spinset_off": getattr(self, "numspinsets", -1) + 1,
+            "spinsets": nc - getattr(self, "numspinelim", nc), "spinsetrank": getattr(self, "numspinsets", 0),
+            "spin_eliminated": getattr(self, "numspinelim", 0),
         }[name]
 
     def table(self, name: str) -> np.ndarray:
