@@ -369,6 +369,41 @@ int sincgpu_orbprop_state(sincgpu_ctx* ctx, int* thisexpodim, double* tempstepsi
  * receives max|S - 1| of the final overlap. */
 int sincgpu_spf_orthogit_dev(sincgpu_ctx* ctx, double* phi, double* error);
 
+/* Constant-mean-field propagation (cmf_prop_wfn, MCTDH.SRC/prop.f90:230-574, with
+ * prepropflag=1, step_flag=2, postpropflag=2; orbitals by expospfprop/DGPHIV,
+ * A-vector by expoavecprop/DGEXPVxxx2 followed by the spin projection, mean fields
+ * and CI matrices in two time slots blended linearly).  Parameters as the
+ * reference's namelist: par_timestep, littlesteps, expotol, aerror, aorder,
+ * maxaorder (<= 124), expodim, maxexpodim (<= 125), expostepfac, denreg
+ * (MCTDH.SRC/parameters.f90:244-295) and timefac (-i for real time). */
+int sincgpu_cmf_setup(sincgpu_ctx* ctx, double par_timestep, int littlesteps, double expotol, double aerror,
+                      int aorder, int maxaorder, int expodim, int maxexpodim, double expostepfac, double denreg,
+                      double timefac_re, double timefac_im);
+
+/* Length-gauge pulses (MCTDH.SRC/pulse.f90:8-52 tdpotlen0 and pulse types 1-5,
+ * :149-372).  params holds 8 doubles per pulse: omega, omega2, pulsestart,
+ * phaseshift, pulsestrength, longstep, pulsetheta, (unused).  Only z-polarised
+ * pulses (sin(pulsetheta) = 0) are supported. */
+int sincgpu_cmf_pulses(sincgpu_ctx* ctx, int npulses, const int* pulsetype, const double* params);
+/* z component of the field at time t. */
+int sincgpu_pulse_ez(sincgpu_ctx* ctx, double t, double* ez);
+
+/* Start of a propagation (prop_loop, MCTDH.SRC/prop.f90:811-852): the A-vector is
+ * spin projected, the mean fields and CI matrices of (phi, avector) are built
+ * (get_stuff) and *energy0 receives <A|H A>/<A|A> with the field at t = 0.
+ * phi and avector are device arrays; the context keeps its own copies.  Needs
+ * walk tables attached (with spin sets for allspinproject=1). */
+int sincgpu_cmf_init_dev(sincgpu_ctx* ctx, const double* phi, const double* avector, double* energy0);
+
+/* One CMF step from tin to tout on the resident state; *energy = <A|P H A>/<A|A>
+ * at tout without the field (timedepexpect=0), *norm = |A|, and the numbers of
+ * Jacobian products (orbitals) and sigma products (A-vector) in the step. */
+int sincgpu_cmf_step(sincgpu_ctx* ctx, double tin, double tout, double* energy, double* norm, int* orb_iters,
+                     int* avec_iters);
+
+/* Copies the current orbitals and A-vector to device arrays (either may be NULL). */
+int sincgpu_cmf_state_dev(sincgpu_ctx* ctx, double* phi, double* avector);
+
 #ifdef __cplusplus
 }
 #endif

@@ -171,3 +171,23 @@ def test_orbital_step_is_orthonormal_and_first_order():
     assert np.abs(out - (phi + dt * f)).max() < 50 * dt * dt * np.abs(f).max() ** 2 + 1e-12
     assert info["nstep"] == 1 and info["nmult"] == 1 + 8 + 1
     assert st.icalled == 1 and st.thisexpodim == max(5, math.floor(8 * 0.95))
+
+
+def test_cmf_step_is_second_order():
+    """Field-free energy drift over a fixed time falls like dt^3 per unit time
+    (the CMF predictor/corrector scheme is second order)."""
+    from oracle.cmf_oracle import CmfOracle, CmfParams
+    n = 3
+    sysm = orc.SincSystem(9, 0.6, [[0, 0, 0]], [2.0], toothnbig=30, toothnsmall=8)
+    phi = orc.seeded_orbitals(sysm, n, seed=93)
+    nc = CIWalks(2, n, 0).numconfig
+    rng = np.random.default_rng(94)
+    a = rng.standard_normal(nc) + 1j * rng.standard_normal(nc)
+    drift = []
+    for dt in (0.01, 0.005):
+        o = CmfOracle(sysm, 2, 0, phi, a / np.linalg.norm(a), CmfParams(par_timestep=dt))
+        e0 = o.energy
+        for k in range(int(round(0.02 / dt))):
+            o.step(dt * k, dt * (k + 1))
+        drift.append(abs(o.energy - e0))
+    assert drift[1] < drift[0] / 5.0

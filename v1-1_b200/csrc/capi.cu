@@ -65,6 +65,7 @@ Ctx::~Ctx() {
   ws_ci2.release();
   ws_kry.release();
   ws_orb.release();
+  cmf.ws.release();
   ci.release();
   if (stream && own_stream) cudaStreamDestroy(stream);
 }
@@ -91,8 +92,8 @@ static void all_pairs(int n, std::vector<int>& pa, std::vector<int>& pb) {
 
 // Coulomb pair solves + twoematel (+ optional full twoereduced); leaves the planar
 // reduced potentials of the pair list in ws_red.
-static int twoe_core(Ctx& c, const double2* phi1, const double2* phi2, double2* twoematel,
-                     double2* full, std::vector<int>& pa, std::vector<int>& pb, bool& herm) {
+int twoe_core(Ctx& c, const double2* phi1, const double2* phi2, double2* twoematel, double2* full,
+              std::vector<int>& pa, std::vector<int>& pb, bool& herm) {
   herm = (phi1 == phi2);
   if (herm)
     herm_pairs(c.nspf, pa, pb);

@@ -10,6 +10,14 @@ struct sincgpu_walks {
   sincgpu::Walks w;
 };
 
+namespace sincgpu {
+double nucdip_z(const Ctx& c) {  // nucdipvalue (SINCDVR/init_sinc_new.f90:652-662), z component
+  double d = 0.0;
+  for (int i = 0; i < c.numcenters; ++i) d += c.nuccharges[i] * c.centershift[3 * i + 2] / 2.0 * c.spacing;
+  return d;
+}
+}  // namespace sincgpu
+
 using namespace sincgpu;
 
 namespace {
@@ -23,11 +31,6 @@ int down(Ctx& c, void* dst, const void* src, size_t bytes) {
   return SINCGPU_OK;
 }
 
-double nucdip_z(const Ctx& c) {  // nucdipvalue (SINCDVR/init_sinc_new.f90:652-662), z component
-  double d = 0.0;
-  for (int i = 0; i < c.numcenters; ++i) d += c.nuccharges[i] * c.centershift[3 * i + 2] / 2.0 * c.spacing;
-  return d;
-}
 
 template <class T>
 void copy_out(const std::vector<T>& v, int* out) {

@@ -134,6 +134,7 @@ int ci_attach(Ctx& c, const Walks& w) {
     for (size_t i = 0; i < sets0.size(); ++i) sets0[i] = w.spinsets[i] - 1;
     for (size_t i = 0; i < elim0.size(); ++i) elim0[i] = w.spin_eliminated[i] - 1;
     s.nspinsets = (int)w.spinsetrank.size();
+    s.numspinconfig = w.numspinconfig;
     s.nspinelim = (int)elim0.size();
     s.maxspinset = w.maxspinsetsize;
     SG_CHECK(s.maxspinset <= 4096, SINCGPU_ERANGE, "spin set of %d configurations exceeds 4096",

@@ -49,6 +49,7 @@ struct CIState {
   long long *sp_set_off = nullptr, *sp_proj_off = nullptr;
   int *sp_sets = nullptr, *sp_elim = nullptr;
   double* sp_proj = nullptr;
+  long long numspinconfig = 0;              // spin-adapted dimension
   void release();
 };
 
@@ -62,6 +63,47 @@ struct OrbPropState {
   int thisexpodim = 0;
   int exposet = 0;
   double tempstepsize = -1.0;
+};
+
+// one length-gauge pulse (MCTDH.SRC/parameters.f90:105-125)
+struct PulseParams {
+  int type = 2;
+  double omega = 1.0, omega2 = 1.0, start = 0.0, phaseshift = 0.0, strength = 0.5, longstep = 1.0, theta = 0.0;
+};
+// z component of the field of all pulses at time t (tdpotlen0, which=3)
+double pulse_ez(const std::vector<PulseParams>& pulses, double t);
+
+struct CmfParams {
+  double par_timestep = 0.05;
+  int littlesteps = 1;
+  double expotol = 1e-8, aerror = 1e-9;
+  int aorder = 30, maxaorder = 100, expodim = 10, maxexpodim = 100;
+  double expostepfac = 1.2, denreg = 1e-10;
+  int step_flag = 2;
+  double2 timefac = {0.0, -1.0};
+};
+
+// saved variables of expoavecprop (expo_driver.f90:842-866)
+struct AvecPropState {
+  int icalled = 0;
+  double tempstep = -1.0;
+  int dim = -1, set = 0, maxorder = 0;
+};
+
+// two time slots of the propagated state and its mean fields (cmf.cu)
+struct CmfState {
+  bool configured = false, ready = false;
+  CmfParams p;
+  std::vector<PulseParams> pulses;
+  AvecPropState a;
+  double first = 0.0, last = 0.0, energy = 0.0, norm = 0.0, nucdipz = 0.0;
+  int orb_iters = 0, avec_iters = 0;
+  std::vector<int> pa, pb;  // pair list of the resident planar reduced potentials
+  bool herm = true;
+  Workspace ws;
+  double2 *spfs[2] = {}, *avec[2] = {}, *den[2] = {}, *inv[2] = {}, *tally[2] = {}, *rp[2] = {};
+  double2 *xpot[2] = {}, *xone[2] = {}, *xz[2] = {};
+  double2 *mat = nullptr, *mats = nullptr, *ta = nullptr, *tb = nullptr, *tc = nullptr;
 };
 
 struct Ctx {
@@ -109,6 +151,7 @@ struct Ctx {
   Workspace ws_orb;         // orbital Krylov basis and Jacobian state
   OrbPropState orb;
   CIState ci;
+  CmfState cmf;
   int coul_chunk = 0;   // pairs per pass sequence (0 = automatic)
   int coul_fp32 = 0;    // 1: Coulomb passes in FP32 (precision form), 0: FP64
   Prof prof;
@@ -174,8 +217,15 @@ int ci_assemble(Ctx& c, const double2* twoematel, const double2* mats);
 int ci_sigma(Ctx& c, const double2* in, double2* out, double constant, double ez, double nucdipz);
 
 // krylov.cu: w = exp(t * timefac * H) v on the real-ified A-vector
+// maxdim: the reference's DGEXPVxxx2 maxdim (Krylov dimension must stay below it;
+// 0 selects the vector length); nmult_out: number of sigma products
 int expv_avector(Ctx& c, const double2* v, double2* w, double t, double2 timefac, int m, double tol,
-                 double anorm, double* stepguess, int* nstep_out, double ez, double nucdipz);
+                 double anorm, double* stepguess, int* nstep_out, double ez, double nucdipz, int maxdim = 0,
+                 int* nmult_out = nullptr);
+// twoematel and the Coulomb pair solves of (phi1, phi2); leaves the planar reduced
+// potentials of the pair list (pa, pb) in ws_red (capi.cu)
+int twoe_core(Ctx& c, const double2* phi1, const double2* phi2, double2* twoematel, double2* full,
+              std::vector<int>& pa, std::vector<int>& pb, bool& herm);
 
 // rhs.cu
 int mult_reducedpot(Ctx& c, const double2* phi, const double2* redpot, double2* out);
@@ -215,6 +265,12 @@ int expospfprop(Ctx& c, double2* phi, const MeanFieldSlot* slots, double tin, do
                 double firsttime, double lasttime, bool linear, double2 timefac, double ez, double expotol,
                 int* numiters);
 int spf_orthogit(Ctx& c, double2* phi, double* error);
+
+// cmf.cu: constant-mean-field step (cmf_prop_wfn) and its initialisation
+int cmf_init(Ctx& c, const double2* phi, const double2* avec, double* e0);
+int cmf_step(Ctx& c, double tin, double tout);
+// z component of the nuclear dipole (capi_ci.cu)
+double nucdip_z(const Ctx& c);
 
 }  // namespace sincgpu
 

@@ -19,7 +19,7 @@
 namespace sincgpu {
 
 constexpr int kKryThreads = 1024;
-constexpr int kMaxKry = 62;  // Krylov dimension limit (mh <= 64)
+constexpr int kMaxKry = 124;  // Krylov dimension limit (Pade order m + 2 <= 126)
 
 // block reduction (fixed shape -> deterministic)
 __device__ double block_sum(double v, double* red) {
@@ -316,24 +316,28 @@ int pade_expm(Ctx& c, const double* Hm, int mh, int mx, double t, int col, doubl
 static double fortran_nint(double x) { return x >= 0 ? std::floor(x + 0.5) : -std::floor(-x + 0.5); }
 
 int expv_avector(Ctx& c, const double2* v, double2* w, double t, double2 timefac, int m, double tol,
-                 double anorm, double* stepguess, int* nstep_out, double ez, double nucdipz) {
+                 double anorm, double* stepguess, int* nstep_out, double ez, double nucdipz, int maxdim_in,
+                 int* nmult_out) {
   CIState& s = c.ci;
   SG_CHECK(s.attached && s.assembled, SINCGPU_ESTATE, "sparse CI matrices not assembled");
   const int nc = s.nc;
   const long long n = 2LL * nc;
-  const int maxdim = (int)std::min<long long>(n, kMaxKry + 1);
-  SG_CHECK(m > 0 && m < maxdim && m <= kMaxKry - 2, SINCGPU_ERANGE, "Krylov dimension %d outside [1,%d)", m,
-           std::min(maxdim, kMaxKry - 1));
+  // the reference checks m < maxdim (DGEXPVxxx2's maxdim argument; n by default)
+  const long long maxdim = maxdim_in > 0 ? maxdim_in : n;
+  SG_CHECK(m > 0 && m < maxdim && m <= kMaxKry, SINCGPU_ERANGE, "Krylov dimension %d outside [1,%lld)", m,
+           std::min<long long>(maxdim, kMaxKry + 1));
   const int mh = m + 2;
-  const size_t need = sizeof(double) * ((size_t)(m + 2) * n + (size_t)mh * mh + 64) + sizeof(double2) * nc +
-                      sizeof(KryState) + 64;
+  const size_t need = sizeof(double) * ((size_t)(m + 2) * n + (size_t)mh * mh + 128 + 5 * (size_t)mh * mh) +
+                      sizeof(double2) * nc + sizeof(KryState) + 64;
   SG_TRY(c.ws_kry.ensure(need));
   double* V = (double*)c.ws_kry.ptr;
   double* Hm = V + (size_t)(m + 2) * n;
   double* exph = Hm + (size_t)mh * mh;
-  double2* tmp = (double2*)(exph + 64);
+  double* pscr = exph + 128;
+  double2* tmp = (double2*)(pscr + 5 * (size_t)mh * mh);
   KryState* dst = (KryState*)(tmp + nc);
   int* d_ns = (int*)(dst + 1);
+  int nmult = 0;
   const double delta = 1.2, gamma = 0.9, break_tol = 1.0e-7;
   double eps = std::fabs((4.0 / 3.0 - 1.0) * 3.0 - 1.0);
   if (tol <= eps) tol = std::sqrt(eps);
@@ -359,12 +363,14 @@ int expv_avector(Ctx& c, const double2* v, double2* w, double t, double2 timefac
     kry_start_kernel<<<1, kKryThreads, 0, c.stream>>>((const double*)w, n, V, dst, have_beta ? 0 : 1);
     SG_LAUNCHED();
     for (int j = 0; j < m; ++j) {
+      ++nmult;
       SG_TRY(ci_sigma(c, (const double2*)(V + (size_t)j * n), tmp, c.nucrepulsion, ez, nucdipz));
       cscale_kernel<<<cb, 256, 0, c.stream>>>(tmp, timefac, nc, (double2*)(V + (size_t)(j + 1) * n), dst);
       SG_LAUNCHED();
       kry_mgs_kernel<<<1, kKryThreads, 0, c.stream>>>(V, n, j, Hm, mh, break_tol, dst);
       SG_LAUNCHED();
     }
+    ++nmult;
     SG_TRY(ci_sigma(c, (const double2*)(V + (size_t)m * n), tmp, c.nucrepulsion, ez, nucdipz));
     cscale_kernel<<<cb, 256, 0, c.stream>>>(tmp, timefac, nc, (double2*)(V + (size_t)(m + 1) * n), dst);
     SG_LAUNCHED();
@@ -387,16 +393,7 @@ int expv_avector(Ctx& c, const double2* v, double2* w, double t, double2 timefac
     double ex[2] = {0.0, 0.0};
     while (true) {
       const int mx = mbrkdwn + k1;
-      const size_t psmem = sizeof(double) * 5 * (size_t)mx * mx;
-      static bool attr = false;
-      if (!attr) {
-        SG_CUDA(cudaFuncSetAttribute(kry_padm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(sizeof(double) * 5 * 64 * 64)));
-        attr = true;
-      }
-      kry_padm_kernel<<<1, kKryThreads, psmem, c.stream>>>(Hm, mh, mx, sgn * t_step, exph, d_ns, 0, nullptr,
-                                                           nullptr);
-      SG_LAUNCHED();
+      SG_TRY(pade_expm(c, Hm, mh, mx, sgn * t_step, 0, exph, nullptr, pscr, d_ns));
       if (k1 == 0) {
         err_loc = tol;
         break;
@@ -434,6 +431,7 @@ int expv_avector(Ctx& c, const double2* v, double2* w, double t, double2 timefac
   }
   *stepguess = nstep == 1 ? t_step : t_last;
   if (nstep_out) *nstep_out = nstep;
+  if (nmult_out) *nmult_out = nmult;
   return SINCGPU_OK;
 }
 

@@ -88,6 +88,12 @@ _SIGS = {
     "sincgpu_walks_spinprojectors": ([_P, _P], _I),
     "sincgpu_spin_project_dev": ([_P, _P], _I),
     "sincgpu_spin_project": ([_P, _P, _P], _I),
+    "sincgpu_cmf_setup": ([_P, _D, _I, _D, _D, _I, _I, _I, _I, _D, _D, _D, _D], _I),
+    "sincgpu_cmf_pulses": ([_P, _I, _P, _P], _I),
+    "sincgpu_pulse_ez": ([_P, _D, _P], _I),
+    "sincgpu_cmf_init_dev": ([_P, _P, _P, _P], _I),
+    "sincgpu_cmf_step": ([_P, _D, _D, _P, _P, _P, _P], _I),
+    "sincgpu_cmf_state_dev": ([_P, _P, _P], _I),
 }
 
 
@@ -377,6 +383,41 @@ class SincProject:
         e = C.c_double(0.0)
         _call("sincgpu_spf_orthogit_dev", self._h, _ptr(phi), C.byref(e))
         return e.value
+
+    # ------------------------------------------------- CMF propagation
+    def cmf_setup(self, par_timestep=0.05, littlesteps=1, expotol=1e-8, aerror=1e-9, aorder=30, maxaorder=100,
+                  expodim=10, maxexpodim=100, expostepfac=1.2, denreg=1e-10, timefac=-1j):
+        tf = complex(timefac)
+        _call("sincgpu_cmf_setup", self._h, float(par_timestep), int(littlesteps), float(expotol), float(aerror),
+              int(aorder), int(maxaorder), int(expodim), int(maxexpodim), float(expostepfac), float(denreg),
+              tf.real, tf.imag)
+
+    def cmf_pulses(self, pulses):
+        """pulses: objects with pulsetype, omega, omega2, pulsestart, phaseshift, strength,
+        longstep, pulsetheta (oracle.cmf_oracle.Pulse has these fields)."""
+        types = np.array([p.pulsetype for p in pulses] or [0], dtype=np.int32)
+        par = np.array([[p.omega, p.omega2, p.pulsestart, p.phaseshift, p.strength, p.longstep, p.pulsetheta, 0.0]
+                        for p in pulses] or [[0.0] * 8], dtype=np.float64)
+        _call("sincgpu_cmf_pulses", self._h, len(pulses), _ptr(types), _ptr(par))
+
+    def pulse_ez(self, t) -> float:
+        e = C.c_double(0.0)
+        _call("sincgpu_pulse_ez", self._h, float(t), C.byref(e))
+        return e.value
+
+    def cmf_init_dev(self, phi, avector) -> float:
+        e = C.c_double(0.0)
+        _call("sincgpu_cmf_init_dev", self._h, _ptr(phi), _ptr(avector), C.byref(e))
+        return e.value
+
+    def cmf_step(self, tin, tout) -> dict:
+        e, nrm, oi, ai = C.c_double(0.0), C.c_double(0.0), C.c_int(0), C.c_int(0)
+        _call("sincgpu_cmf_step", self._h, float(tin), float(tout), C.byref(e), C.byref(nrm), C.byref(oi),
+              C.byref(ai))
+        return {"energy": e.value, "norm": nrm.value, "orb_iters": oi.value, "avec_iters": ai.value}
+
+    def cmf_state_dev(self, phi=None, avector=None):
+        _call("sincgpu_cmf_state_dev", self._h, _ptr(phi), _ptr(avector))
 
     def spin_project(self, avector):
         """basis_project (allspinproject=1) of a host A-vector; returns the projection."""
