@@ -318,6 +318,14 @@ int sincgpu_expoavecprop(sincgpu_ctx* ctx, const double* avec_in, double* avec_o
 int sincgpu_spin_project_dev(sincgpu_ctx* ctx, double* avector);
 int sincgpu_spin_project(sincgpu_ctx* ctx, const double* avector_in, double* avector_out);
 
+/* z-dipole expectation (dipolesub_one, MCTDH.SRC/dipolesub.f90:20-125, the z
+ * component with bra = ket): dipole = <A| Z A> + nucdipvalue_z <A|A> (complex, 2
+ * doubles) with Z the configuration singles of <phi_i|z|phi_j> assembled by
+ * sincgpu_assemble_sparsemats, and normsq = <A|A>; divide by normsq for the
+ * normalised expectation. */
+int sincgpu_dipole_z_dev(sincgpu_ctx* ctx, const double* avector, double* dipole, double* normsq);
+int sincgpu_dipole_z(sincgpu_ctx* ctx, const double* avector, double* dipole, double* normsq);
+
 /* One orbital-RHS evaluation from the A-vector: denmat, invdenmat and the 2-RDM
  * (get_allden, MCTDH.SRC/mean.f90:467-477), then sincgpu_orbital_rhs_dev. */
 int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* ctx, const double* phi, const double* avector,
@@ -369,6 +377,20 @@ int sincgpu_orbprop_state(sincgpu_ctx* ctx, int* thisexpodim, double* tempstepsi
  * receives max|S - 1| of the final overlap. */
 int sincgpu_spf_orthogit_dev(sincgpu_ctx* ctx, double* phi, double* error);
 
+/* Orbital and A-vector files in the reference's format (gfortran unformatted
+ * sequential records; save_vector / write_spf / spf_header_write,
+ * MCTDH.SRC/loadstuff.f90:9-180; avector_header_write / write_avector /
+ * easy_load_avectors, MCTDH.SRC/configload.f90:221-249, 801-863).  Host arrays;
+ * dims are spfdims(3) (numpoints per axis for the sinc project).  Loading an
+ * A-vector reorders each stored determinant, applies the reordering phase and
+ * maps it onto the walk tables' configuration list (numr = 1, complex files).
+ * sincgpu_load_spfs with spfs = NULL reads the header only. */
+int sincgpu_save_spfs(const char* path, const int* dims, int numspf, const double* spfs);
+int sincgpu_load_spfs(const char* path, int* dims, int* numspf, double* spfs, long long capacity);
+int sincgpu_save_avector(const char* path, sincgpu_walks* walks, int numvects, const double* avectors,
+                         int allspinproject, int spinrestrictval);
+int sincgpu_load_avector(const char* path, sincgpu_walks* walks, int maxvects, double* avectors, int* numvects);
+
 /* Constant-mean-field propagation (cmf_prop_wfn, MCTDH.SRC/prop.f90:230-574, with
  * prepropflag=1, step_flag=2, postpropflag=2; orbitals by expospfprop/DGPHIV,
  * A-vector by expoavecprop/DGEXPVxxx2 followed by the spin projection, mean fields
@@ -400,6 +422,10 @@ int sincgpu_cmf_init_dev(sincgpu_ctx* ctx, const double* phi, const double* avec
  * Jacobian products (orbitals) and sigma products (A-vector) in the step. */
 int sincgpu_cmf_step(sincgpu_ctx* ctx, double tin, double tout, double* energy, double* norm, int* orb_iters,
                      int* avec_iters);
+
+/* z dipole of the current CMF state (as sincgpu_dipole_z, with the CI matrices of
+ * the current orbitals). */
+int sincgpu_cmf_dipole_z(sincgpu_ctx* ctx, double* dipole, double* normsq);
 
 /* Copies the current orbitals and A-vector to device arrays (either may be NULL). */
 int sincgpu_cmf_state_dev(sincgpu_ctx* ctx, double* phi, double* avector);

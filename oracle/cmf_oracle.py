@@ -34,7 +34,7 @@ import numpy as np
 from . import orbprop_oracle as op
 from . import sinc_oracle as orc
 from .expokit_oracle import complexify, dgexpv, realify
-from .walks_oracle import CIWalks, SpinSets
+from .walks_oracle import CIWalks, SpinSets, dipole_z
 
 
 @dataclass
@@ -131,7 +131,7 @@ class CmfOracle:
         self.s0.spfs = np.array(phi, dtype=np.complex128)
         self.s0.avec = self.spin.project(avec)
         self.get_stuff()
-        self.energy = self.expect(0.0, with_pulse=True)
+        self.energy = self.expect(0.0, with_pulse=True, project=False)
         self.orb_iters = self.avec_iters = 0
 
     # ---- mean fields (slot 0) -------------------------------------------
@@ -163,11 +163,19 @@ class CmfOracle:
         return self.ow.sparsesparsemult(a, xp, xo, xk, constant=self.sysm.nucrepulsion + ez * self.nucdip,
                                         xpulse=(xz * ez if ez else None))
 
-    def expect(self, t, with_pulse=False):
+    def expect(self, t, with_pulse=False, project=True):
+        """<A|H A>/<A|A>; after a step H A is spin projected (prop.f90:944), at the
+        start it is not (prop.f90:831-838)."""
         a = self.s0.avec
         ez = pulse_ez(self.p.pulses, t) if with_pulse else 0.0
-        ha = self.spin.project(self.sigma(a, self.s0.hops, ez))
+        ha = self.sigma(a, self.s0.hops, ez)
+        if project:
+            ha = self.spin.project(ha)
         return (np.vdot(a, ha) / np.vdot(a, a)).real
+
+    def dipole(self):
+        """z dipole of the current state with the current orbitals' matrices."""
+        return dipole_z(self.ow, self.s0.hops[3], self.s0.avec, self.nucdip)
 
     # ---- A-vector propagation -------------------------------------------
     def expoavecprop(self, a, hops, dt, midtime):

@@ -331,6 +331,16 @@ class CIWalks:
         return out
 
 
+def dipole_z(ww: CIWalks, xz_singles, avector, nucdipz):
+    """dipolesub_one (MCTDH.SRC/dipolesub.f90:20-125), z component, bra = ket:
+    (<A| Z A> + nucdip <A|A>, <A|A>) with Z the assembled singles of <phi_i|z|phi_j>."""
+    a = np.asarray(avector, dtype=np.complex128)
+    contrib = xz_singles * a[ww.singlehop - 1]
+    za = np.array([contrib[ww.singlehop_off[c]:ww.singlehop_off[c + 1]].sum() for c in range(ww.numconfig)])
+    nn = float(np.vdot(a, a).real)
+    return np.vdot(a, za) + nucdipz * nn, nn
+
+
 class SpinSets:
     """Spin walks, spin sets and the S^2 projectors of the reference's
     allspinproject=1 path (MCTDH.SRC/spinwalks.f90: getnumspinwalks 302-388,

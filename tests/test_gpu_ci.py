@@ -114,3 +114,19 @@ def test_energy_from_sigma_equals_energy_from_rdms(setup):
     tally = gpu.get_tworeducedx(a)
     e_rdm = np.sum((pot + ke) * den.T) + 0.5 * np.sum(mat * tally) + sysm.nucrepulsion
     assert abs(e_sigma - e_rdm) < 1e-10 * abs(e_rdm)
+
+
+def test_dipole_z(setup):
+    from oracle.walks_oracle import dipole_z
+    sysm, gpu, ow, phi, a = setup
+    mat, _ = sysm.call_twoe_matel00(phi, phi)
+    ph = np.conj(phi).T
+    pot, ke, z = ph @ sysm.mult_pot(phi), ph @ sysm.mult_ke(phi), ph @ sysm.mult_zdipole(phi)
+    gpu.assemble_sparsemats(mat, pot, ke, z)
+    nucdip = float(np.sum(sysm.nuccharges * sysm.centershift[:, 2] / 2.0 * sysm.spacing))
+    d_ref, n_ref = dipole_z(ow, ow.assemble_singles(z), a, nucdip)
+    d, nn = gpu.dipole_z(a)
+    assert abs(d - d_ref) < TOL * max(abs(d_ref), 1.0)
+    assert nn == pytest.approx(n_ref, rel=1e-14)
+    # the expectation of a hermitian operator is real
+    assert abs(d.imag) < 1e-12 * max(abs(d), 1.0)

@@ -53,6 +53,7 @@ def run_gpu(base, params, nsteps, numelec=2, ms=0):
         av = torch.empty(len(a), dtype=torch.complex128, device="cuda")
         gpu.cmf_state_dev(p, av)
         ez = [gpu.pulse_ez(t) for t in (0.0, 0.013, 0.4, 1.0)]
+        steps[-1]["dipole"] = gpu.cmf_dipole_z()
         return e0, steps, host(p), av.cpu().numpy(), ez
 
 
@@ -64,6 +65,7 @@ def run_oracle(base, params, nsteps):
     for k in range(nsteps):
         o.step(params.par_timestep * k, params.par_timestep * (k + 1))
         steps.append({"energy": o.energy, "norm": o.norm, "orb_iters": o.orb_iters, "avec_iters": o.avec_iters})
+    steps[-1]["dipole"] = o.dipole()
     return e0, steps, o.s0.spfs, o.s0.avec
 
 
@@ -78,6 +80,8 @@ def test_cmf_steps_match_oracle(base, pulsed):
         assert (s["orb_iters"], s["avec_iters"]) == (r["orb_iters"], r["avec_iters"])
         assert s["energy"] == pytest.approx(r["energy"], rel=1e-10)
         assert s["norm"] == pytest.approx(r["norm"], rel=1e-12)
+    (d, nn), (d_r, nn_r) = steps[-1]["dipole"], steps_r[-1]["dipole"]
+    assert abs(d - d_r) < 1e-9 * max(abs(d_r), 1.0) and nn == pytest.approx(nn_r, rel=1e-12)
     assert np.abs(phi_g - phi_r).max() < 1e-9 * np.abs(phi_r).max()
     assert np.abs(a_g - a_r).max() < 1e-9 * np.abs(a_r).max()
     assert ez == pytest.approx([pulse_ez(pulses, t) for t in (0.0, 0.013, 0.4, 1.0)], abs=1e-15)

@@ -6,9 +6,6 @@
 #include "walks.hpp"
 #include "../../include/sincgpu.h"
 
-struct sincgpu_walks {
-  sincgpu::Walks w;
-};
 
 namespace sincgpu {
 double nucdip_z(const Ctx& c) {  // nucdipvalue (SINCDVR/init_sinc_new.f90:652-662), z component
@@ -125,6 +122,29 @@ int sincgpu_walks_spinprojectors(sincgpu_walks* h, double* out) {
   SG_CHECK(h->w.spinrestrictval >= 0, SINCGPU_ESTATE, "spin tables not built");
   std::memcpy(out, h->w.spinproj.data(), sizeof(double) * h->w.spinproj.size());
   return SINCGPU_OK;
+}
+
+int sincgpu_dipole_z_dev(sincgpu_ctx* h, const double* avector, double* dipole, double* normsq) {
+  CTX_CHECK(h);
+  Ctx& c = h->c;
+  SG_CHECK(avector && dipole && normsq, SINCGPU_EINVAL, "null argument");
+  SG_TRY(c.ws_ci2.ensure(sizeof(double2) * c.ci.nc));
+  double2 d;
+  SG_TRY(ci_dipole_z(c, (const double2*)avector, (double2*)c.ws_ci2.ptr, nucdip_z(c), &d, normsq));
+  dipole[0] = d.x;
+  dipole[1] = d.y;
+  return SINCGPU_OK;
+}
+
+int sincgpu_dipole_z(sincgpu_ctx* h, const double* avector, double* dipole, double* normsq) {
+  CTX_CHECK(h);
+  Ctx& c = h->c;
+  SG_CHECK(c.ci.attached, SINCGPU_ESTATE, "no walk tables attached");
+  SG_CHECK(avector, SINCGPU_EINVAL, "null argument");
+  const size_t b = sizeof(double2) * c.ci.nc;
+  SG_TRY(c.ws_io.ensure(b));
+  SG_CUDA(cudaMemcpyAsync(c.ws_io.ptr, avector, b, cudaMemcpyHostToDevice, c.stream));
+  return sincgpu_dipole_z_dev(h, (const double*)c.ws_io.ptr, dipole, normsq);
 }
 
 int sincgpu_spin_project_dev(sincgpu_ctx* h, double* avector) {

@@ -528,13 +528,14 @@ __global__ void __launch_bounds__(128) sigma_kernel(const long long* __restrict_
   const int lane = threadIdx.x & 31;
   if (c1 >= nc) return;
   double2 acc = make_double2(0.0, 0.0);
-  for (long long h = doff[c1] + lane; h < doff[c1 + 1]; h += 32) {
-    const double2 t = cmul(xpot[h], in[dhop[h]]);
-    acc = cadd(acc, t);
-  }
+  if (xpot)
+    for (long long h = doff[c1] + lane; h < doff[c1 + 1]; h += 32) {
+      const double2 t = cmul(xpot[h], in[dhop[h]]);
+      acc = cadd(acc, t);
+    }
   double2 acc1 = make_double2(0.0, 0.0);
   for (long long h = soff[c1] + lane; h < soff[c1 + 1]; h += 32) {
-    double2 m = xone[h];
+    double2 m = xone ? xone[h] : make_double2(0.0, 0.0);
     if (ez != 0.0) {
       m.x = fma(ez, xz[h].x, m.x);
       m.y = fma(ez, xz[h].y, m.y);
@@ -550,6 +551,31 @@ __global__ void __launch_bounds__(128) sigma_kernel(const long long* __restrict_
     r = cadd(r, acc1);
     out[c1] = r;
   }
+}
+
+// z-dipole expectation (dipolesub_one, MCTDH.SRC/dipolesub.f90:20-125, z part):
+// <A| Z A> with Z the singles of <phi_i|z|phi_j>, plus nucdip <A|A>; also <A|A>
+int ci_dipole_z(Ctx& c, const double2* a, double2* tmp, double nucdipz, double2* dip, double* normsq) {
+  CIState& s = c.ci;
+  SG_CHECK(s.attached && s.assembled, SINCGPU_ESTATE, "sparse CI matrices not assembled");
+  sigma_kernel<<<ceil_div(s.nc, 4), 128, 0, c.stream>>>(s.dhop_off, s.dhop, nullptr, s.shop_off, s.shop, nullptr,
+                                                        s.xz, 1.0, 0.0, a, s.nc, tmp);
+  SG_LAUNCHED();
+  std::vector<double2> ha(s.nc), za(s.nc);
+  SG_CUDA(cudaMemcpyAsync(ha.data(), a, sizeof(double2) * s.nc, cudaMemcpyDeviceToHost, c.stream));
+  SG_CUDA(cudaMemcpyAsync(za.data(), tmp, sizeof(double2) * s.nc, cudaMemcpyDeviceToHost, c.stream));
+  SG_CUDA(cudaStreamSynchronize(c.stream));
+  double2 d = make_double2(0.0, 0.0);
+  double nn = 0.0;
+  for (int i = 0; i < s.nc; ++i) {  // hermdot: sum conj(a) b
+    d.x += ha[i].x * za[i].x + ha[i].y * za[i].y;
+    d.y += ha[i].x * za[i].y - ha[i].y * za[i].x;
+    nn += ha[i].x * ha[i].x + ha[i].y * ha[i].y;
+  }
+  dip->x = d.x + nucdipz * nn;
+  dip->y = d.y;
+  *normsq = nn;
+  return SINCGPU_OK;
 }
 
 int ci_sigma(Ctx& c, const double2* in, double2* out, double constant, double ez, double nucdipz) {

@@ -423,6 +423,18 @@ int sincgpu_cmf_step(sincgpu_ctx* h, double tin, double tout, double* energy, do
   return SINCGPU_OK;
 }
 
+int sincgpu_cmf_dipole_z(sincgpu_ctx* h, double* dipole, double* normsq) {
+  CTX_CHECK(h);
+  Ctx& c = h->c;
+  SG_CHECK(c.cmf.ready && dipole && normsq, SINCGPU_EINVAL, "no CMF state or null argument");
+  SG_TRY(set_hamiltonian(c, false, 0.0, 1.0));
+  double2 d;
+  SG_TRY(ci_dipole_z(c, c.cmf.avec[0], c.cmf.tc, c.cmf.nucdipz, &d, normsq));
+  dipole[0] = d.x;
+  dipole[1] = d.y;
+  return SINCGPU_OK;
+}
+
 int sincgpu_cmf_state_dev(sincgpu_ctx* h, double* phi, double* avector) {
   CTX_CHECK(h);
   Ctx& c = h->c;

@@ -215,6 +215,7 @@ int ci_tally(Ctx& c, const double2* a1, const double2* a2, double2* tally);
 int ci_onebody(Ctx& c, const double2* phi, double2* mats);
 int ci_assemble(Ctx& c, const double2* twoematel, const double2* mats);
 int ci_sigma(Ctx& c, const double2* in, double2* out, double constant, double ez, double nucdipz);
+int ci_dipole_z(Ctx& c, const double2* a, double2* tmp, double nucdipz, double2* dip, double* normsq);
 
 // krylov.cu: w = exp(t * timefac * H) v on the real-ified A-vector
 // maxdim: the reference's DGEXPVxxx2 maxdim (Krylov dimension must stay below it;

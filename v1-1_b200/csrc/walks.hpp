@@ -46,3 +46,8 @@ int build_walks(Walks& w, int numelec, int nspf, int restrictms, int nthreads);
 int build_spin(Walks& w, int spinrestrictval);
 
 }  // namespace sincgpu
+
+// opaque handle of the C ABI (include/sincgpu.h)
+struct sincgpu_walks {
+  sincgpu::Walks w;
+};

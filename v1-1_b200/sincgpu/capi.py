@@ -94,6 +94,13 @@ _SIGS = {
     "sincgpu_cmf_init_dev": ([_P, _P, _P, _P], _I),
     "sincgpu_cmf_step": ([_P, _D, _D, _P, _P, _P, _P], _I),
     "sincgpu_cmf_state_dev": ([_P, _P, _P], _I),
+    "sincgpu_dipole_z_dev": ([_P, _P, _P, _P], _I),
+    "sincgpu_dipole_z": ([_P, _P, _P, _P], _I),
+    "sincgpu_cmf_dipole_z": ([_P, _P, _P], _I),
+    "sincgpu_save_spfs": ([C.c_char_p, _P, _I, _P], _I),
+    "sincgpu_load_spfs": ([C.c_char_p, _P, _P, _P, _LL], _I),
+    "sincgpu_save_avector": ([C.c_char_p, _P, _I, _P, _I, _I], _I),
+    "sincgpu_load_avector": ([C.c_char_p, _P, _I, _P, _P], _I),
 }
 
 
@@ -418,6 +425,20 @@ class SincProject:
 
     def cmf_state_dev(self, phi=None, avector=None):
         _call("sincgpu_cmf_state_dev", self._h, _ptr(phi), _ptr(avector))
+
+    def dipole_z(self, avector):
+        """(<A|Z A> + nucdip <A|A> as complex, <A|A>) with the assembled CI matrices."""
+        a = _f(avector).reshape(-1)
+        d = np.zeros(2)
+        nn = C.c_double(0.0)
+        _call("sincgpu_dipole_z", self._h, _ptr(a), _ptr(d), C.byref(nn))
+        return complex(d[0], d[1]), nn.value
+
+    def cmf_dipole_z(self):
+        d = np.zeros(2)
+        nn = C.c_double(0.0)
+        _call("sincgpu_cmf_dipole_z", self._h, _ptr(d), C.byref(nn))
+        return complex(d[0], d[1]), nn.value
 
     def spin_project(self, avector):
         """basis_project (allspinproject=1) of a host A-vector; returns the projection."""
