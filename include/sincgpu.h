@@ -391,6 +391,29 @@ int sincgpu_save_avector(const char* path, sincgpu_walks* walks, int numvects, c
                          int allspinproject, int spinrestrictval);
 int sincgpu_load_avector(const char* path, sincgpu_walks* walks, int maxvects, double* avectors, int* numvects);
 
+/* CUDA-graph form of sincgpu_orbital_rhs_avec_dev: one warm-up evaluation, then
+ * the same call captured into a graph kept in the context (all arguments are
+ * device pointers baked into the graph).  sincgpu_rhs_graph_launch replays it on
+ * the context stream. */
+int sincgpu_rhs_graph_capture(sincgpu_ctx* ctx, const double* phi, const double* avector, double timefac_re,
+                              double timefac_im, double ztdpot, double* denmat, double* invdenmat,
+                              double* reducedpottally, double* twoematel, double* reducedpot, double* outspfs);
+int sincgpu_rhs_graph_launch(sincgpu_ctx* ctx);
+
+/* A batch: the captured graphs of n contexts (instances of any size on one
+ * device) as independent child nodes of one parent graph, launched at once. */
+typedef struct sincgpu_batch sincgpu_batch;
+int sincgpu_batch_create(sincgpu_batch** batch, sincgpu_ctx** ctxs, int n);
+int sincgpu_batch_launch(sincgpu_batch* batch, void* stream);
+int sincgpu_batch_destroy(sincgpu_batch* batch);
+
+/* Autotuner: times the orbital-RHS evaluation for the candidate Coulomb
+ * pair-chunk sizes (automatic, all pairs, 1/2, 1/4, 16, 8) and keeps the fastest
+ * in the context; returns it and its time. */
+int sincgpu_autotune_rhs(sincgpu_ctx* ctx, const double* phi, const double* avector, double* denmat,
+                         double* invdenmat, double* reducedpottally, double* twoematel, double* reducedpot,
+                         double* outspfs, int* best_chunk, float* best_ms);
+
 /* Constant-mean-field propagation (cmf_prop_wfn, MCTDH.SRC/prop.f90:230-574, with
  * prepropflag=1, step_flag=2, postpropflag=2; orbitals by expospfprop/DGPHIV,
  * A-vector by expoavecprop/DGEXPVxxx2 followed by the spin projection, mean fields

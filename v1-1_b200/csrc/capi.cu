@@ -2,6 +2,7 @@
 #include <atomic>
 #include <cstdarg>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 #include <string>
 #include "context.hpp"
@@ -66,8 +67,30 @@ Ctx::~Ctx() {
   ws_kry.release();
   ws_orb.release();
   cmf.ws.release();
+  for (IntCache& ic : icache) cudaFree(ic.dev);
+  if (rhs_exec) cudaGraphExecDestroy(rhs_exec);
+  if (rhs_graph) cudaGraphDestroy(rhs_graph);
   ci.release();
   if (stream && own_stream) cudaStreamDestroy(stream);
+}
+
+int cached_ints(Ctx& c, int slot, const int* h, size_t n, const int** d) {
+  IntCache& ic = c.icache[slot];
+  if (ic.dev && ic.host.size() == n && std::equal(h, h + n, ic.host.begin())) {
+    *d = ic.dev;
+    return SINCGPU_OK;
+  }
+  if (n > ic.cap) {
+    cudaFree(ic.dev);
+    ic.dev = nullptr;
+    ic.cap = 0;
+    SG_CUDA(cudaMalloc(&ic.dev, sizeof(int) * std::max<size_t>(n, 1)));
+    ic.cap = n;
+  }
+  ic.host.assign(h, h + n);
+  if (n) SG_CUDA(cudaMemcpyAsync(ic.dev, ic.host.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
+  *d = ic.dev;
+  return SINCGPU_OK;
 }
 
 // hermitian pair list a <= b (0-based), b-major

@@ -53,6 +53,16 @@ struct CIState {
   void release();
 };
 
+// Host integer tables (pair lists, lookup tables) kept on the device and
+// uploaded only when their content changes, so that steady-state evaluations
+// issue no host-to-device copies (which CUDA graph capture requires).
+struct IntCache {
+  std::vector<int> host;
+  int* dev = nullptr;
+  size_t cap = 0;
+};
+enum IntSlot { IC_PA = 0, IC_PB, IC_LUT, IC_COUNT };
+
 // saved variables of the orbital exponential propagator (expospfprop)
 struct OrbPropState {
   int expodim = 10;          // starting Krylov dimension
@@ -152,6 +162,9 @@ struct Ctx {
   OrbPropState orb;
   CIState ci;
   CmfState cmf;
+  IntCache icache[IC_COUNT];
+  cudaGraph_t rhs_graph = nullptr;         // captured orbital-RHS evaluation (graph.cu)
+  cudaGraphExec_t rhs_exec = nullptr;
   int coul_chunk = 0;   // pairs per pass sequence (0 = automatic)
   int coul_fp32 = 0;    // 1: Coulomb passes in FP32 (precision form), 0: FP64
   Prof prof;
@@ -179,6 +192,9 @@ struct ProfScope {
     }
   }
 };
+
+// device copy of a host integer table (capi.cu); uploads only on a content change
+int cached_ints(Ctx& c, int slot, const int* h, size_t n, const int** d);
 
 // setup.cu
 int build_tables(Ctx& c, int toothnbig, int toothnsmall, int flags);

@@ -313,18 +313,16 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
   long long xper = ((c.G + nsplit - 1) / nsplit + TK - 1) / TK * TK;
   nsplit = ceil_div(c.G, xper);
   const long long MM = (long long)M * M;
-  size_t need = sizeof(double) * (MM * nsplit + MM) + sizeof(int) * (2 * npair + n * n);
+  size_t need = sizeof(double) * (MM * nsplit + MM);
   SG_TRY(c.ws_gemm.ensure(need));
   double* part = (double*)c.ws_gemm.ptr;
   double* C = part + MM * nsplit;
-  int* d_pa = (int*)(C + MM);
-  int* d_pb = d_pa + npair;
-  int* d_lut = d_pb + npair;
+  const int *d_pa, *d_pb, *d_lut;
   std::vector<int> lut;
   pair_lut(n, h_pa, h_pb, npair, herm, lut);
-  SG_CUDA(cudaMemcpyAsync(d_pa, h_pa, sizeof(int) * npair, cudaMemcpyHostToDevice, c.stream));
-  SG_CUDA(cudaMemcpyAsync(d_pb, h_pb, sizeof(int) * npair, cudaMemcpyHostToDevice, c.stream));
-  SG_CUDA(cudaMemcpyAsync(d_lut, lut.data(), sizeof(int) * n * n, cudaMemcpyHostToDevice, c.stream));
+  SG_TRY(cached_ints(c, IC_PA, h_pa, npair, &d_pa));
+  SG_TRY(cached_ints(c, IC_PB, h_pb, npair, &d_pb));
+  SG_TRY(cached_ints(c, IC_LUT, lut.data(), (size_t)n * n, &d_lut));
   {
     ProfScope ps(c, ST_TWOE_GEMM);
     const size_t fbytes = sizeof(double2) * 4 * (size_t)n * TK;
@@ -505,13 +503,12 @@ static int reduced_pot_impl(Ctx& c, const double* Rpl, const int* h_pa, const in
                             bool herm, const double2* tally, double2* reducedpot) {
   const int n = c.nspf;
   const int K = 2 * npair, NC = 2 * n * n;
-  size_t need = sizeof(double) * (size_t)K * NC + sizeof(int) * 2 * npair;
+  size_t need = sizeof(double) * (size_t)K * NC;
   SG_TRY(c.ws_gemm.ensure(need));
   double* Wm = (double*)c.ws_gemm.ptr;
-  int* d_pa = (int*)(Wm + (size_t)K * NC);
-  int* d_pb = d_pa + npair;
-  SG_CUDA(cudaMemcpyAsync(d_pa, h_pa, sizeof(int) * npair, cudaMemcpyHostToDevice, c.stream));
-  SG_CUDA(cudaMemcpyAsync(d_pb, h_pb, sizeof(int) * npair, cudaMemcpyHostToDevice, c.stream));
+  const int *d_pa, *d_pb;
+  SG_TRY(cached_ints(c, IC_PA, h_pa, npair, &d_pa));
+  SG_TRY(cached_ints(c, IC_PB, h_pb, npair, &d_pb));
   {
     ProfScope ps(c, ST_RP_W);
     build_w_kernel<<<ceil_div((long long)K * NC, 256), 256, 0, c.stream>>>(tally, d_pa, d_pb, npair, n,

@@ -80,12 +80,11 @@ static int coul_run_t(Ctx& c, const double2* src1, const double2* src2, const in
   }
   chunk = std::min(chunk, npair);
   SG_TRY(c.ws_fft.ensure((size_t)per_pair * chunk));
-  SG_TRY(c.ws_pairs.ensure(sizeof(int) * 2 * (size_t)npair));
-  int* d_pa = (int*)c.ws_pairs.ptr;
-  int* d_pb = d_pa + npair;
+  const int* d_pa = nullptr;
+  const int* d_pb = nullptr;
   if (!dens) {
-    SG_CUDA(cudaMemcpyAsync(d_pa, h_pa, sizeof(int) * npair, cudaMemcpyHostToDevice, c.stream));
-    SG_CUDA(cudaMemcpyAsync(d_pb, h_pb, sizeof(int) * npair, cudaMemcpyHostToDevice, c.stream));
+    SG_TRY(cached_ints(c, IC_PA, h_pa, npair, &d_pa));
+    SG_TRY(cached_ints(c, IC_PB, h_pb, npair, &d_pb));
   }
   CoulArgs<C> ca{};
   ca.N = N;
@@ -100,8 +99,8 @@ static int coul_run_t(Ctx& c, const double2* src1, const double2* src2, const in
   for (int p0 = 0; p0 < npair; p0 += chunk) {
     const int np = std::min(chunk, npair - p0);
     ca.pair0 = p0;
-    ca.pa = d_pa + p0;
-    ca.pb = d_pb + p0;
+    ca.pa = d_pa ? d_pa + p0 : nullptr;
+    ca.pb = d_pb ? d_pb + p0 : nullptr;
     SG_TRY(coul_dispatch(c, ca, np, dens, src1, src2, Rpl, full, herm));
   }
   return SINCGPU_OK;

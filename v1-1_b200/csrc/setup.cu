@@ -494,6 +494,7 @@ __global__ void narrow_kernel(float2* __restrict__ out, const double2* __restric
 }
 
 int ensure_fp32_tables(Ctx& c) {
+  if (c.d_khat32 && c.d_roots32) return SINCGPU_OK;  // no stream work once built (graph capture)
   const long long P3 = (long long)c.P * c.P * c.P;
   if (!c.d_khat32) {
     SG_CUDA(cudaMalloc(&c.d_khat32, sizeof(float2) * P3));

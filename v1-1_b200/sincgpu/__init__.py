@@ -8,6 +8,7 @@ meaning and Fortran array layouts, and call the CUDA library through its
 if libsincgpu.so is missing or no CUDA device is present, calls fail.
 """
 from .capi import (  # noqa: F401
+    Batch,
     SincGpuError,
     SincProject,
     load_library,

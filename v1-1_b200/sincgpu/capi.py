@@ -97,11 +97,41 @@ _SIGS = {
     "sincgpu_dipole_z_dev": ([_P, _P, _P, _P], _I),
     "sincgpu_dipole_z": ([_P, _P, _P, _P], _I),
     "sincgpu_cmf_dipole_z": ([_P, _P, _P], _I),
+    "sincgpu_rhs_graph_capture": ([_P, _P, _P, _D, _D, _D, _P, _P, _P, _P, _P, _P], _I),
+    "sincgpu_rhs_graph_launch": ([_P], _I),
+    "sincgpu_batch_create": ([C.POINTER(_P), _P, _I], _I),
+    "sincgpu_batch_launch": ([_P, _P], _I),
+    "sincgpu_batch_destroy": ([_P], _I),
+    "sincgpu_autotune_rhs": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
     "sincgpu_save_spfs": ([C.c_char_p, _P, _I, _P], _I),
     "sincgpu_load_spfs": ([C.c_char_p, _P, _P, _P, _LL], _I),
     "sincgpu_save_avector": ([C.c_char_p, _P, _I, _P, _I, _I], _I),
     "sincgpu_load_avector": ([C.c_char_p, _P, _I, _P, _P], _I),
 }
+
+
+class Batch:
+    """Captured orbital-RHS graphs of several SincProjects launched as one graph."""
+
+    def __init__(self, projects):
+        arr = (_P * len(projects))(*[p._h for p in projects])
+        self._h = _P()
+        self._keep = list(projects)
+        _call("sincgpu_batch_create", C.byref(self._h), arr, len(projects))
+
+    def launch(self, stream_handle: int = 0):
+        _call("sincgpu_batch_launch", self._h, _P(stream_handle))
+
+    def close(self):
+        if self._h:
+            load_library().sincgpu_batch_destroy(self._h)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def exported_symbols() -> list[str]:
@@ -439,6 +469,22 @@ class SincProject:
         nn = C.c_double(0.0)
         _call("sincgpu_cmf_dipole_z", self._h, _ptr(d), C.byref(nn))
         return complex(d[0], d[1]), nn.value
+
+    # ------------------------------------------------------- graphs
+    def rhs_graph_capture(self, phi, avector, denmat, invdenmat, tally, twoematel, reducedpot, out,
+                          timefac=-1j, ztdpot=0.0):
+        tf = complex(timefac)
+        _call("sincgpu_rhs_graph_capture", self._h, _ptr(phi), _ptr(avector), tf.real, tf.imag, float(ztdpot),
+              _ptr(denmat), _ptr(invdenmat), _ptr(tally), _ptr(twoematel), _ptr(reducedpot), _ptr(out))
+
+    def rhs_graph_launch(self):
+        _call("sincgpu_rhs_graph_launch", self._h)
+
+    def autotune_rhs(self, phi, avector, denmat, invdenmat, tally, twoematel, reducedpot, out):
+        ch, ms = C.c_int(0), C.c_float(0.0)
+        _call("sincgpu_autotune_rhs", self._h, _ptr(phi), _ptr(avector), _ptr(denmat), _ptr(invdenmat),
+              _ptr(tally), _ptr(twoematel), _ptr(reducedpot), _ptr(out), C.byref(ch), C.byref(ms))
+        return ch.value, ms.value
 
     def spin_project(self, avector):
         """basis_project (allspinproject=1) of a host A-vector; returns the projection."""
