@@ -453,6 +453,51 @@ int sincgpu_cmf_dipole_z(sincgpu_ctx* ctx, double* dipole, double* normsq);
 /* Copies the current orbitals and A-vector to device arrays (either may be NULL). */
 int sincgpu_cmf_state_dev(sincgpu_ctx* ctx, double* phi, double* avector);
 
+/* Served form: a device-resident request loop.  Requests (a sinc-DVR system,
+ * electrons and 2Ms, pulses, number of CMF steps of length dt, initial orbitals
+ * (totpoints x numspf complex) and A-vector (host arrays, copied at submit)) are
+ * admitted by max_active worker threads while the HBM budget (0: 85% of the free
+ * memory) allows; each live request keeps its orbitals, A-vector, mean fields
+ * and walk tables on the device in its own context and stream until it finishes,
+ * so requests arriving while others run join as slots and memory free up and
+ * their work overlaps on the device.  Results are deterministic: a request gives
+ * the same numbers alone or in a mix. */
+typedef struct sincgpu_request {
+  int numpoints;
+  double spacing;
+  int numcenters;
+  const int* centershift;    /* 3 x numcenters, half-grid units */
+  const double* nuccharges;  /* numcenters */
+  int numspf, numelec, restrictms, spinrestrictval;  /* spinrestrictval < 0: |restrictms| */
+  int npulses;
+  const int* pulsetype;      /* as sincgpu_cmf_pulses */
+  const double* pulseparams; /* 8 per pulse */
+  int nsteps;
+  double dt;
+  int coulomb_fp32;          /* precision form of the Coulomb passes */
+  int keep_state;            /* keep the final orbitals and A-vector for sincgpu_server_result_arrays */
+  const double* phi;
+  const double* avector;
+} sincgpu_request;
+typedef struct sincgpu_server sincgpu_server;
+int sincgpu_server_create(sincgpu_server** server, int device, long long hbm_budget, int max_active);
+int sincgpu_server_submit(sincgpu_server* server, const sincgpu_request* request, int* id);
+/* Blocks until request id finished: initial and final energy, norm, normalised z
+ * dipole, steps done; non-zero status if the request failed. */
+int sincgpu_server_wait(sincgpu_server* server, int id, double* energy0, double* energy, double* norm,
+                        double* dipole_z, int* nsteps_done);
+/* Per-step latencies (ms) and energies of a finished request; final orbitals and
+ * A-vector when it was submitted with keep_state.  Any pointer may be NULL. */
+int sincgpu_server_result_arrays(sincgpu_server* server, int id, double* step_ms, double* energies, double* phi,
+                                 double* avector);
+/* counts[0..4] = admitted, completed, steps, peak concurrent requests, pending;
+ * p50 / p99 of all finished steps' latencies (ms); steps per second between the
+ * first admission and the last completion. */
+int sincgpu_server_stats(sincgpu_server* server, long long* counts, double* p50_ms, double* p99_ms,
+                         double* steps_per_s);
+/* Finishes all submitted requests, stops the workers and frees the server. */
+int sincgpu_server_destroy(sincgpu_server* server);
+
 #ifdef __cplusplus
 }
 #endif
