@@ -46,6 +46,11 @@ def parse():
     ap.add_argument("--config", default="B")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--batched-count", type=int, default=64)
+    ap.add_argument("--served-count", type=int, default=24)
+    ap.add_argument("--served-steps", type=int, default=10)
     return ap.parse_args()
 
 
@@ -269,6 +274,9 @@ def main():
     proj.profile(False)
     roofline = make_roofline(w, prof, nprof, dev)
 
+    # ---- CMF propagation steps/s on the same workload ----
+    propagation = cmf_rate(proj, w, phi, avec, torch, local)
+
     # ---- end to end through the host-array C entry (pinned host buffers) ----
     e2e = None
     if not args.no_e2e:
@@ -282,10 +290,19 @@ def main():
         "config": workload_config(w), "clocks": clk, "gpu_launches": int(launches),
         "launches_per_step": launches / args.steps, "fft_length": proj.fft_length, "numconfig": nc,
         "roofline": roofline, "secondary": secondary, "precision_forms": precision,
+        "propagation": propagation,
         "stage_ms_per_step": {k: v[0] / nprof for k, v in prof.items()},
     }
     if e2e:
         line["e2e"] = e2e
+    proj.close()
+    if not args.no_batched:
+        line["batched"] = batched_form(torch, local, stream, args.batched_count)
+    if not args.no_served:
+        line["served"] = {f: served_form(local, f == "mixed_fp32_coulomb", args.served_count, args.served_steps)
+                          for f in ("plain_fp64", "mixed_fp32_coulomb")}
+        pl, mx = line["served"]["plain_fp64"], line["served"]["mixed_fp32_coulomb"]
+        line["served"]["mixed_vs_plain_steps_per_s"] = mx["steps_per_s"] / max(pl["steps_per_s"], 1e-30)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         t = cpu_reference_eval(w, threads)
@@ -294,7 +311,6 @@ def main():
                                           "numpy/scipy restatement of the reference"}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    proj.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -341,6 +357,160 @@ def precision_form(proj, torch, stream, flush, step, out, mat, steps, world, dis
     finally:
         proj.set_option("coulomb_fp32", 0)
     return res
+
+
+def cmf_rate(proj, w, phi, avec, torch, local, nsteps=6):
+    """Constant-mean-field steps/s (cmf_prop_wfn, dt = 0.05, field free, spin
+    projected) on the bench workload, device-resident state."""
+    from sincgpu import WalkTables
+    wt = WalkTables(w.numelec, w.nspf, 0).build_spin()
+    proj.ci_attach(wt)
+    proj.cmf_setup(par_timestep=0.05)
+    proj.cmf_pulses([])
+    e0 = proj.cmf_init_dev(phi, avec)
+    proj.cmf_step(0.0, 0.05)                     # warm-up step (sizes the Krylov workspaces)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = [proj.cmf_step(0.05 * k, 0.05 * (k + 1)) for k in range(1, nsteps + 1)]
+    dt = time.perf_counter() - t0
+    ms = [r["ms"] for r in res] if "ms" in res[0] else None
+    return {"steps_per_s": nsteps / dt, "ms_per_step": 1e3 * dt / nsteps, "steps": nsteps, "dt_au": 0.05,
+            "energy0": e0, "energy_last": res[-1]["energy"], "orb_jacobian_products_per_step":
+            float(np.mean([r["orb_iters"] for r in res])), "sigma_products_per_step":
+            float(np.mean([r["avec_iters"] for r in res])), "per_step_ms": ms,
+            "timing": "host wall clock around each step (each step ends in a device synchronisation)"}
+
+
+def batched_form(torch, local, stream, count):
+    """Batched form: `count` uneven instances (inputs.batched_instances).  Plain
+    FP64 evaluated one after another through the direct entry point, against
+    the captured graphs of all instances launched as one parent graph, in FP64
+    and with the Coulomb passes in FP32 (pair chunks from the autotuner).  Rates
+    are instance evaluations per second; errors are the mixed results against
+    the plain FP64 ones."""
+    from sincgpu import Batch, SincProject, WalkTables
+    from sincgpu.inputs import batched_instances, seeded_orbitals
+    dev = torch.device("cuda", local)
+    cx = dict(dtype=torch.complex128, device=dev)
+    inst = batched_instances(count)
+    t_setup = time.perf_counter()
+    made = []
+    for i, s in enumerate(inst):
+        n, N = s["nspf"], s["numpoints"]
+        G = N ** 3
+        p = SincProject(N, s["spacing"], s["centershift"], s["nuccharges"], n, device=local)
+        p.set_stream(stream.cuda_stream)
+        wt = WalkTables(s["numelec"], n, s["restrictms"])
+        p.ci_attach(wt)
+        phi = seeded_orbitals(N, s["spacing"], n, seed=100 + i)
+        rng = np.random.default_rng(200 + i)
+        a = rng.standard_normal(wt.numconfig) + 1j * rng.standard_normal(wt.numconfig)
+        a /= np.linalg.norm(a)
+        b = dict(phi=torch.from_numpy(np.ascontiguousarray(phi.T)).to(dev), a=torch.from_numpy(a).to(dev),
+                 den=torch.empty((n, n), **cx), inv=torch.empty((n, n), **cx), tally=torch.empty((n,) * 4, **cx),
+                 mat=torch.empty((n,) * 4, **cx), rp=torch.empty((n, n, G), **cx), out=torch.empty((n, G), **cx))
+        made.append((p, wt, b))
+    setup_s = time.perf_counter() - t_setup
+
+    def args_of(b):
+        return (b["phi"], b["a"], b["den"], b["inv"], b["tally"], b["mat"], b["rp"], b["out"])
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def sequential():
+        for p, _, b in made:
+            p.orbital_rhs_avec_dev(*args_of(b))
+
+    plain_ms = timed(sequential, 3)
+    ref_out = [b["out"].clone() for _, _, b in made]
+    ref_mat = [b["mat"].clone() for _, _, b in made]
+    for p, _, b in made:
+        p.rhs_graph_capture(*args_of(b))
+    batch = Batch([m[0] for m in made])
+    batched_plain_ms = timed(lambda: batch.launch(stream.cuda_stream), 3)
+    batch.close()
+    t_tune = time.perf_counter()
+    tuned = {}
+    for p, _, b in made:
+        p.set_option("coulomb_fp32", 1)
+        key = (p.N, p.nspf)
+        if key in tuned:
+            p.set_option("coul_chunk", tuned[key])
+        else:
+            tuned[key], _ = p.autotune_rhs(*args_of(b))
+        p.rhs_graph_capture(*args_of(b))
+    tune_s = time.perf_counter() - t_tune
+    batch = Batch([m[0] for m in made])
+    mixed_ms = timed(lambda: batch.launch(stream.cuda_stream), 3)
+    torch.cuda.synchronize()
+    rhs_err = max(float((b["out"] - r).abs().max() / r.abs().max()) for (_, _, b), r in zip(made, ref_out))
+    de = max(abs(0.5 * complex(((b["mat"] - r) * b["tally"]).sum().item())) for (_, _, b), r in zip(made, ref_mat))
+    batch.close()
+    for p, _, _ in made:
+        p.close()
+    return {
+        "instances": count, "workload": "inputs.batched_instances: odd 21^3-61^3 grids, spacing 0.25-0.4, 1-2 "
+        "nuclei Z=1-3 within +-2 bohr, 2-6 electrons, 4-12 orbitals, <= 4000 determinants, seeded",
+        "grid_points_total": int(sum(s["numpoints"] ** 3 for s in inst)),
+        "plain_fp64_sequential": {"value": count / (plain_ms / 1e3), "unit": "evals/s", "ms_per_round": plain_ms},
+        "batched_fp64_graph": {"value": count / (batched_plain_ms / 1e3), "unit": "evals/s",
+                               "ms_per_round": batched_plain_ms},
+        "batched_mixed_graph": {"value": count / (mixed_ms / 1e3), "unit": "evals/s", "ms_per_round": mixed_ms,
+                                "coulomb": "fp32 passes, fp64 products and contractions",
+                                "rhs_rel_err_max_vs_fp64": rhs_err,
+                                "two_electron_energy_dev_max_hartree": de},
+        "mixed_batched_vs_plain_sequential": plain_ms / mixed_ms,
+        "setup_s": setup_s, "autotune_s": tune_s, "autotuned_chunks": len(tuned),
+        "timing": "CUDA events on the launching stream, 3 rounds after one warm-up round; each round touches "
+                  "several GB (inputs larger than L2)",
+    }
+
+
+def served_form(local, fp32, count, nsteps):
+    """Served form: requests (inputs.served_requests) submitted at their Poisson
+    arrival offsets to the device-resident request loop; per-step latency
+    percentiles and steps/s over the run."""
+    from types import SimpleNamespace
+    from sincgpu.inputs import ci_size, seeded_orbitals, served_requests
+    from sincgpu.serve import Server
+    reqs = served_requests(count)
+    states = []
+    for i, r in enumerate(reqs):
+        phi = seeded_orbitals(r["numpoints"], r["spacing"], r["nspf"], seed=300 + i)
+        rng = np.random.default_rng(400 + i)
+        nc = ci_size(r["numelec"], r["nspf"])
+        a = rng.standard_normal(nc) + 1j * rng.standard_normal(nc)
+        states.append((phi, a / np.linalg.norm(a)))
+    pulses = [[SimpleNamespace(pulsestart=0.0, phaseshift=0.0, longstep=1.0, pulsetheta=0.0, **r["pulse"])]
+              for r in reqs]
+    with Server(device=local, max_active=8) as srv:
+        t0 = time.perf_counter()
+        ids = []
+        for r, (phi, a), pl in zip(reqs, states, pulses):
+            delay = t0 + r["arrival"] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            ids.append(srv.submit(r["numpoints"], r["spacing"], r["centershift"], r["nuccharges"], r["nspf"],
+                                  r["numelec"], r["restrictms"], phi, a, nsteps, dt=0.05, pulses=pl,
+                                  coulomb_fp32=fp32))
+        res = [srv.wait(i) for i in ids]
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+    return {"requests": count, "steps_per_request": nsteps, "dt_au": 0.05, "arrival_rate_per_s": 20.0,
+            "p50_step_ms": st["p50_ms"], "p99_step_ms": st["p99_ms"], "steps_per_s": st["steps_per_s"],
+            "peak_concurrent": st["peak_active"], "completed": st["completed"], "wall_s": wall,
+            "mean_request_s": float(np.mean([len(r["step_ms"]) and r["step_ms"].sum() / 1e3 for r in res])),
+            "workload": "inputs.served_requests: odd 21^3-41^3 grids, 2-4 electrons, 4-8 orbitals, <= 1000 "
+                        "determinants, one sin^2 pulse each (type 2), seeded; the request loop uses 8 worker slots"}
 
 
 def secondary_rates(proj, torch, stream, flush, phi, den, inv, red, out, mat, avec, n, G):

@@ -474,7 +474,11 @@ int make_khat(Ctx& c) {
   size_t sm0 = sizeof(double2) * (P + 2 * 8 * (P + 1));
   size_t sm1 = sizeof(double2) * (P + 2 * P * c.tx);
   size_t smax = std::max(sm0, sm1);
-  SG_CUDA(cudaFuncSetAttribute(fft_full_axis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
+  // the attribute is process-wide: always the same (largest) value, so contexts
+  // created concurrently on several threads never lower it under each other
+  constexpr int kSmemOptIn = 227 * 1024;
+  SG_CHECK(smax <= (size_t)kSmemOptIn, SINCGPU_ERANGE, "kernel-spectrum FFT needs %zu bytes of shared memory", smax);
+  SG_CUDA(cudaFuncSetAttribute(fft_full_axis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemOptIn));
   fft_full_axis_kernel<<<ceil_div((long long)P * P, 8), 128, sm0>>>(c.d_khat, c.plan, c.d_roots, 0, c.tx, 1.0);
   SG_LAUNCHED();
   dim3 g1(ceil_div(P, c.tx), P);

@@ -85,3 +85,69 @@ def regularized_inverse(a, tol=1e-10):
     inv = np.where(s < tol, 1.0 / tol, 1.0 / np.where(s == 0, 1.0, s))
     inv = np.where(s == 0, 0.0, inv)
     return np.asfortranarray((np.conj(vt).T * inv[None, :]) @ np.conj(u).T)
+
+
+def snap_shift(z_bohr: float, spacing: float, numpoints: int) -> int:
+    """Nuclear coordinate in half-grid units with the project's parity rule:
+    an odd point count needs an even shift, an even count an odd one."""
+    s = int(round(2.0 * z_bohr / spacing))
+    want_odd = numpoints % 2 == 0
+    if (s % 2 != 0) != want_odd:
+        s += 1 if s >= 0 else -1
+    return s
+
+
+def ci_size(numelec: int, nspf: int) -> int:
+    """Determinants of the full CI with the lowest 2Ms."""
+    na = (numelec + numelec % 2) // 2
+    nb = numelec - na
+    return math.comb(nspf, na) * math.comb(nspf, nb)
+
+
+def _system(rng, nmin, nmax, emin, emax, omin, omax, max_configs):
+    N = int(rng.integers(nmin // 2, nmax // 2 + 1)) * 2 + 1          # odd point counts
+    spacing = round(float(rng.uniform(0.25, 0.4)), 3)
+    ncent = int(rng.integers(1, 3))
+    cs, z = [], []
+    while len(cs) < ncent:
+        pos = rng.uniform(-2.0, 2.0, size=3)
+        c = tuple(snap_shift(p, spacing, N) for p in pos)
+        if c in cs:          # two nuclei on one point: draw again
+            continue
+        cs.append(c)
+        z.append(float(rng.integers(1, 4)))
+    ne = int(rng.integers(emin, emax + 1))
+    lo = max(omin, (ne + 1) // 2 + 1)
+    n = int(rng.integers(lo, omax + 1))
+    while n > lo and ci_size(ne, n) > max_configs:
+        n -= 1
+    return dict(numpoints=N, spacing=spacing, centershift=tuple(cs), nuccharges=tuple(z), nspf=n, numelec=ne,
+                restrictms=ne % 2)
+
+
+def batched_instances(count: int = 64, seed: int = 2024, max_configs: int = 4000):
+    """Instances of the batched form: 21^3-61^3 grids (odd point counts),
+    spacing 0.25-0.4, 1-2 nuclei of charge 1-3 within +-2 bohr (snapped), 2-6
+    electrons, 4-12 orbitals, lowest 2Ms; the orbital count is lowered until the
+    full CI has at most `max_configs` determinants (keeps walk-table builds short)."""
+    rng = np.random.default_rng(seed)
+    return [_system(rng, 21, 61, 2, 6, 4, 12, max_configs) for _ in range(count)]
+
+
+def served_requests(count: int = 24, seed: int = 4048, nmax: int = 41, omax: int = 8, emax: int = 4,
+                    max_configs: int = 1000, rate: float = 20.0):
+    """Requests of the served form with Poisson arrival offsets (mean `rate`
+    per second) and one linearly polarised sin^2 pulse each (peak field
+    0.005-0.17 au, carrier 0.05-1.0 au, envelope 400-1600 au; pulse type 2 with
+    omega = pi / duration and strength = peak / carrier)."""
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    for _ in range(count):
+        t += float(rng.exponential(1.0 / rate))
+        s = _system(rng, 21, nmax, 2, emax, 4, omax, max_configs)
+        peak = float(rng.uniform(0.005, 0.17))
+        w2 = float(rng.uniform(0.05, 1.0))
+        dur = float(rng.uniform(400.0, 1600.0))
+        s.update(arrival=t, pulse=dict(pulsetype=2, omega=math.pi / dur, omega2=w2, strength=peak / w2))
+        out.append(s)
+    return out
