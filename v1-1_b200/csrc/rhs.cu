@@ -8,135 +8,126 @@
 // Kernels: mix (pointwise n x n), KE (ke.cu, fused pot/pulse), reducedpot apply +
 // invdenmat mix (one pass over reducedpot, the dominant HBM stream), projector
 // dots (split-K, deterministic), projector subtraction.
+//
+// The per-point kernels work on tiles of 32 consecutive grid points (one per
+// lane) by all orbitals: each warp handles a subset of output orbitals, reads
+// every (orbital, tile) row as one coalesced 512-byte segment, and the small
+// per-point vectors (phi, the partial sums) and n x n matrices sit in shared
+// memory, so no thread keeps an n-vector in registers.
 #include <algorithm>
 #include "context.hpp"
 
 namespace sincgpu {
 
+constexpr int TXO = 32;          // grid points per tile (lanes)
+constexpr int NYO = 8;           // warps per block
+constexpr int kMaxOrbRhs = 32;   // largest orbital count of these kernels
+constexpr int kRhsSmemMax = 64 * 1024;
+
+__device__ __forceinline__ void cfma(double2& acc, double2 v, double2 m) {  // acc += v*m
+  acc.x = fma(v.x, m.x, fma(-v.y, m.y, acc.x));
+  acc.y = fma(v.x, m.y, fma(v.y, m.x, acc.y));
+}
+
 // out(x,i) = sum_j in(x,j) mat(j,i)   (column-major n x n complex mat)
-template <int NMAX>
-__global__ void __launch_bounds__(256) mix_kernel(const double2* __restrict__ in,
-                                                  const double2* __restrict__ mat, int n,
-                                                  long long G, double2* __restrict__ out) {
-  __shared__ double2 sm[NMAX * NMAX];
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x) sm[i] = mat[i];
+__global__ void __launch_bounds__(TXO * NYO) mix_kernel(const double2* __restrict__ in,
+                                                        const double2* __restrict__ mat, int n, long long G,
+                                                        double2* __restrict__ out) {
+  extern __shared__ double2 rsm[];
+  double2* sm = rsm;            // n*n
+  double2* tin = rsm + n * n;   // n x TXO
+  const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
+  for (int e = tid; e < n * n; e += TXO * NYO) sm[e] = mat[e];
+  const long long x = blockIdx.x * (long long)TXO + lx;
+  const bool ok = x < G;
+  for (int j = ty; j < n; j += NYO) tin[j * TXO + lx] = ok ? in[(long long)j * G + x] : make_double2(0.0, 0.0);
   __syncthreads();
-  long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (x >= G) return;
-  double2 v[NMAX];
-#pragma unroll
-  for (int j = 0; j < NMAX; ++j)
-    if (j < n) v[j] = in[(long long)j * G + x];
-  for (int i = 0; i < n; ++i) {
+  if (!ok) return;
+  for (int i = ty; i < n; i += NYO) {
     double2 acc = make_double2(0.0, 0.0);
-#pragma unroll
-    for (int j = 0; j < NMAX; ++j)
-      if (j < n) {
-        double2 m = sm[j + n * i];
-        acc.x = fma(v[j].x, m.x, fma(-v[j].y, m.y, acc.x));
-        acc.y = fma(v[j].x, m.y, fma(v[j].y, m.x, acc.y));
-      }
+    for (int j = 0; j < n; ++j) cfma(acc, tin[j * TXO + lx], sm[j + n * i]);
     out[(long long)i * G + x] = acc;
   }
 }
 
 // s_i = acc(x,i) + sum_k V(x,k,i) phi_k(x) over i in [i0, i0+ni); then, when
 // `dentime`, t_i = timefac * sum_j s_j inv(j,i) (all n orbitals present).
-template <int NMAX>
-__global__ void __launch_bounds__(128) redpot_kernel(const double2* __restrict__ phi,
-                                                     const double2* __restrict__ V,
-                                                     const double2* __restrict__ acc_in,
-                                                     const double2* __restrict__ inv,
-                                                     double2 timefac, int n, int i0, int ni,
-                                                     int dentime, long long G,
-                                                     double2* __restrict__ out) {
-  __shared__ double2 sinv[NMAX * NMAX];
+__global__ void __launch_bounds__(TXO * NYO) redpot_kernel(const double2* __restrict__ phi,
+                                                           const double2* __restrict__ V,
+                                                           const double2* __restrict__ acc_in,
+                                                           const double2* __restrict__ inv, double2 timefac,
+                                                           int n, int i0, int ni, int dentime, long long G,
+                                                           double2* __restrict__ out) {
+  extern __shared__ double2 rsm[];
+  double2* sinv = rsm;                 // n*n (dentime)
+  double2* sph = rsm + n * n;          // n x TXO
+  double2* ss = sph + n * TXO;         // n x TXO (dentime)
+  const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
   if (dentime)
-    for (int i = threadIdx.x; i < n * n; i += blockDim.x) sinv[i] = inv[i];
+    for (int e = tid; e < n * n; e += TXO * NYO) sinv[e] = inv[e];
+  const long long x = blockIdx.x * (long long)TXO + lx;
+  const bool ok = x < G;
+  for (int k = ty; k < n; k += NYO) sph[k * TXO + lx] = ok ? phi[(long long)k * G + x] : make_double2(0.0, 0.0);
   __syncthreads();
-  long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (x >= G) return;
-  double2 ph[NMAX];
-#pragma unroll
-  for (int k = 0; k < NMAX; ++k)
-    if (k < n) ph[k] = phi[(long long)k * G + x];
-  double2 s[NMAX];
-#pragma unroll
-  for (int ii = 0; ii < NMAX; ++ii) {
-    if (ii < ni) {
-      const int i = i0 + ii;
+  if (ok) {
+    for (int ii = ty; ii < ni; ii += NYO) {
       double2 a = acc_in ? acc_in[(long long)ii * G + x] : make_double2(0.0, 0.0);
       const double2* Vi = V + (long long)n * ii * G + x;  // V(x,k,i): column k + n*ii
-#pragma unroll
-      for (int k = 0; k < NMAX; ++k)
-        if (k < n) {
-          double2 v = Vi[(long long)k * G];
-          a.x = fma(v.x, ph[k].x, fma(-v.y, ph[k].y, a.x));
-          a.y = fma(v.x, ph[k].y, fma(v.y, ph[k].x, a.y));
-        }
-      s[ii] = a;
-      (void)i;
+#pragma unroll 4
+      for (int k = 0; k < n; ++k) cfma(a, Vi[(long long)k * G], sph[k * TXO + lx]);
+      if (dentime) ss[ii * TXO + lx] = a;
+      else out[(long long)ii * G + x] = a;
     }
+    (void)i0;
   }
-  if (!dentime) {
-    for (int ii = 0; ii < ni; ++ii) out[(long long)ii * G + x] = s[ii];
-    return;
-  }
-  for (int i = 0; i < n; ++i) {
+  if (!dentime) return;
+  __syncthreads();
+  if (!ok) return;
+  for (int i = ty; i < n; i += NYO) {
     double2 a = make_double2(0.0, 0.0);
-#pragma unroll
-    for (int j = 0; j < NMAX; ++j)
-      if (j < n) {
-        double2 m = sinv[j + n * i];
-        a.x = fma(s[j].x, m.x, fma(-s[j].y, m.y, a.x));
-        a.y = fma(s[j].x, m.y, fma(s[j].y, m.x, a.y));
-      }
+    for (int j = 0; j < n; ++j) cfma(a, ss[j * TXO + lx], sinv[j + n * i]);
     out[(long long)i * G + x] = cmul(timefac, a);
   }
 }
 
-// partial[blk][j + n*i] = sum_{x in blk} conj(P_j(x)) T_i(x)
-constexpr int DX = 32;
-__global__ void __launch_bounds__(256) dots_kernel(const double2* __restrict__ Pm,
-                                                   const double2* __restrict__ Tm, int n,
-                                                   long long G, long long xper,
-                                                   double2* __restrict__ partial) {
-  __shared__ double2 sp[32][DX];
-  __shared__ double2 st[32][DX];
-  const long long xb = blockIdx.x * xper, xe = min(G, xb + xper);
-  const int nn = n * n;
-  double2 acc[4];
-#pragma unroll
-  for (int r = 0; r < 4; ++r) acc[r] = make_double2(0.0, 0.0);
-  for (long long x0 = xb; x0 < xe; x0 += DX) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < n * DX; i += blockDim.x) {
-      int o = i / DX, k = i % DX;
-      long long x = x0 + k;
-      bool ok = x < xe;
-      sp[o][k] = ok ? Pm[(long long)o * G + x] : make_double2(0.0, 0.0);
-      st[o][k] = ok ? Tm[(long long)o * G + x] : make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      int e = threadIdx.x + 256 * r;
-      if (e < nn) {
-        int j = e % n, i = e / n;
-        double2 a = acc[r];
-        for (int k = 0; k < DX; ++k) {
-          double2 p = sp[j][k], t = st[i][k];
-          a.x = fma(p.x, t.x, fma(p.y, t.y, a.x));
-          a.y = fma(p.x, t.y, fma(-p.y, t.x, a.y));
-        }
-        acc[r] = a;
-      }
-    }
+// partial[blk][j + n*i] = sum_{x in blk} conj(P_j(x)) T_i(x); block blk covers
+// DCH consecutive points, warp w the rows j = w, w + NYO, ...
+constexpr int DCH = 128;
+__global__ void __launch_bounds__(TXO * NYO) dots_kernel(const double2* __restrict__ Pm,
+                                                         const double2* __restrict__ Tm, int n, long long G,
+                                                         double2* __restrict__ partial) {
+  extern __shared__ double2 rsm[];
+  double2* tt = rsm;  // n x DCH
+  const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
+  const long long x0 = blockIdx.x * (long long)DCH;
+  for (int e = tid; e < n * DCH; e += TXO * NYO) {
+    const int i = e / DCH, k = e % DCH;
+    const long long x = x0 + k;
+    tt[e] = x < G ? Tm[(long long)i * G + x] : make_double2(0.0, 0.0);
   }
+  __syncthreads();
+  const int nn = n * n;
+  for (int j = ty; j < n; j += NYO) {
+    double2 pv[DCH / TXO];
 #pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    int e = threadIdx.x + 256 * r;
-    if (e < nn) partial[(long long)blockIdx.x * nn + e] = acc[r];
+    for (int r = 0; r < DCH / TXO; ++r) {
+      const long long x = x0 + r * TXO + lx;
+      pv[r] = x < G ? Pm[(long long)j * G + x] : make_double2(0.0, 0.0);
+    }
+    for (int i = 0; i < n; ++i) {
+      double2 a = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int r = 0; r < DCH / TXO; ++r) {  // conj(p) t
+        const double2 p = pv[r], t = tt[i * DCH + r * TXO + lx];
+        a.x = fma(p.x, t.x, fma(p.y, t.y, a.x));
+        a.y = fma(p.x, t.y, fma(-p.y, t.x, a.y));
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        a.x += __shfl_down_sync(0xffffffffu, a.x, o);
+        a.y += __shfl_down_sync(0xffffffffu, a.y, o);
+      }
+      if (lx == 0) partial[(long long)blockIdx.x * nn + j + n * i] = a;
+    }
   }
 }
 
@@ -157,80 +148,60 @@ __global__ void __launch_bounds__(128) dots_reduce_kernel(const double2* __restr
 }
 
 // out(x,i) = T(x,i) - sum_j P_j(x) D(j,i)
-template <int NMAX>
-__global__ void __launch_bounds__(256) project_kernel(const double2* __restrict__ Tm,
-                                                      const double2* __restrict__ Pm,
-                                                      const double2* __restrict__ D, int n,
-                                                      long long G, double2* __restrict__ out) {
-  __shared__ double2 sd[NMAX * NMAX];
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x) sd[i] = D[i];
+__global__ void __launch_bounds__(TXO * NYO) project_kernel(const double2* __restrict__ Tm,
+                                                            const double2* __restrict__ Pm,
+                                                            const double2* __restrict__ D, int n, long long G,
+                                                            double2* __restrict__ out) {
+  extern __shared__ double2 rsm[];
+  double2* sd = rsm;            // n*n
+  double2* sp = rsm + n * n;    // n x TXO
+  const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
+  for (int e = tid; e < n * n; e += TXO * NYO) sd[e] = D[e];
+  const long long x = blockIdx.x * (long long)TXO + lx;
+  const bool ok = x < G;
+  for (int j = ty; j < n; j += NYO) sp[j * TXO + lx] = ok ? Pm[(long long)j * G + x] : make_double2(0.0, 0.0);
   __syncthreads();
-  long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (x >= G) return;
-  double2 p[NMAX];
-#pragma unroll
-  for (int j = 0; j < NMAX; ++j)
-    if (j < n) p[j] = Pm[(long long)j * G + x];
-  for (int i = 0; i < n; ++i) {
+  if (!ok) return;
+  for (int i = ty; i < n; i += NYO) {
     double2 a = make_double2(0.0, 0.0);
-#pragma unroll
-    for (int j = 0; j < NMAX; ++j)
-      if (j < n) {
-        double2 d = sd[j + n * i];
-        a.x = fma(p[j].x, d.x, fma(-p[j].y, d.y, a.x));
-        a.y = fma(p[j].x, d.y, fma(p[j].y, d.x, a.y));
-      }
-    double2 t = Tm[(long long)i * G + x];
-    out[(long long)i * G + x] = csub(t, a);
+    for (int j = 0; j < n; ++j) cfma(a, sp[j * TXO + lx], sd[j + n * i]);
+    out[(long long)i * G + x] = csub(Tm[(long long)i * G + x], a);
   }
 }
 
-#define SG_DISPATCH_N(n, KERNEL, ...)                                     \
-  do {                                                                    \
-    if ((n) <= 8)                                                         \
-      KERNEL<8> __VA_ARGS__;                                              \
-    else if ((n) <= 16)                                                   \
-      KERNEL<16> __VA_ARGS__;                                             \
-    else                                                                  \
-      KERNEL<32> __VA_ARGS__;                                             \
-  } while (0)
-
 // out(x,i) = T(x,i) - sum_j P_j(x) (M1(j,i) + M2(j,i)) - sum_j X_j(x) D2(j,i)
 // (the projector and projector-derivative terms of the orbital Jacobian)
-template <int NMAX>
-__global__ void __launch_bounds__(256) jac_combine_kernel(const double2* __restrict__ Tm,
-                                                          const double2* __restrict__ Pm,
-                                                          const double2* __restrict__ M1,
-                                                          const double2* __restrict__ M2,
-                                                          const double2* __restrict__ Xm,
-                                                          const double2* __restrict__ D2, int n,
-                                                          long long G, double2* __restrict__ out) {
-  __shared__ double2 sm[NMAX * NMAX], sd[NMAX * NMAX];
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
-    sm[i] = cadd(M1[i], M2[i]);
-    sd[i] = D2[i];
+__global__ void __launch_bounds__(TXO * NYO) jac_combine_kernel(const double2* __restrict__ Tm,
+                                                                const double2* __restrict__ Pm,
+                                                                const double2* __restrict__ M1,
+                                                                const double2* __restrict__ M2,
+                                                                const double2* __restrict__ Xm,
+                                                                const double2* __restrict__ D2, int n,
+                                                                long long G, double2* __restrict__ out) {
+  extern __shared__ double2 rsm[];
+  double2* sm = rsm;               // n*n: M1 + M2
+  double2* sd = sm + n * n;        // n*n: D2
+  double2* sp = sd + n * n;        // n x TXO
+  double2* sx = sp + n * TXO;      // n x TXO
+  const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
+  for (int e = tid; e < n * n; e += TXO * NYO) {
+    sm[e] = cadd(M1[e], M2[e]);
+    sd[e] = D2[e];
+  }
+  const long long x = blockIdx.x * (long long)TXO + lx;
+  const bool ok = x < G;
+  for (int j = ty; j < n; j += NYO) {
+    sp[j * TXO + lx] = ok ? Pm[(long long)j * G + x] : make_double2(0.0, 0.0);
+    sx[j * TXO + lx] = ok ? Xm[(long long)j * G + x] : make_double2(0.0, 0.0);
   }
   __syncthreads();
-  long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (x >= G) return;
-  double2 p[NMAX], q[NMAX];
-#pragma unroll
-  for (int j = 0; j < NMAX; ++j)
-    if (j < n) {
-      p[j] = Pm[(long long)j * G + x];
-      q[j] = Xm[(long long)j * G + x];
-    }
-  for (int i = 0; i < n; ++i) {
+  if (!ok) return;
+  for (int i = ty; i < n; i += NYO) {
     double2 a = make_double2(0.0, 0.0);
-#pragma unroll
-    for (int j = 0; j < NMAX; ++j)
-      if (j < n) {
-        const double2 m = sm[j + n * i], d = sd[j + n * i];
-        a.x = fma(p[j].x, m.x, fma(-p[j].y, m.y, a.x));
-        a.y = fma(p[j].x, m.y, fma(p[j].y, m.x, a.y));
-        a.x = fma(q[j].x, d.x, fma(-q[j].y, d.y, a.x));
-        a.y = fma(q[j].x, d.y, fma(q[j].y, d.x, a.y));
-      }
+    for (int j = 0; j < n; ++j) {
+      cfma(a, sp[j * TXO + lx], sm[j + n * i]);
+      cfma(a, sx[j * TXO + lx], sd[j + n * i]);
+    }
     out[(long long)i * G + x] = csub(Tm[(long long)i * G + x], a);
   }
 }
@@ -250,29 +221,52 @@ __global__ void axpby_kernel(double2* __restrict__ acc, const double2* __restric
   }
 }
 
-int orbital_dots_scratch(const Ctx& c) {
-  const int nblk_dots = 4 * 148;
-  const long long xper = ((c.G + nblk_dots - 1) / nblk_dots + DX - 1) / DX * DX;
-  return ceil_div(c.G, xper);
+namespace {
+
+// the kernels' shared-memory limit: one fixed value (race-free across threads)
+int rhs_attrs() {
+  static bool done = false;
+  if (done) return SINCGPU_OK;
+  SG_CUDA(cudaFuncSetAttribute(mix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax));
+  SG_CUDA(cudaFuncSetAttribute(redpot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax));
+  SG_CUDA(cudaFuncSetAttribute(dots_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax));
+  SG_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax));
+  SG_CUDA(cudaFuncSetAttribute(jac_combine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax));
+  done = true;
+  return SINCGPU_OK;
 }
 
-int orbital_dots(Ctx& c, const double2* P, const double2* T, double2* D, double2* part) {
-  const int n = c.nspf;
-  const long long G = c.G;
-  const int nblk_dots = 4 * 148;
-  const long long xper = ((G + nblk_dots - 1) / nblk_dots + DX - 1) / DX * DX;
-  const int nb = ceil_div(G, xper);
-  dots_kernel<<<nb, 256, 0, c.stream>>>(P, T, n, G, xper, part);
+const dim3 kTile(TXO, NYO);
+
+size_t smem_mix(int n) { return sizeof(double2) * ((size_t)n * n + (size_t)n * TXO); }
+size_t smem_redpot(int n) { return sizeof(double2) * ((size_t)n * n + 2 * (size_t)n * TXO); }
+size_t smem_dots(int n) { return sizeof(double2) * (size_t)n * DCH; }
+size_t smem_jac(int n) { return sizeof(double2) * (2 * (size_t)n * n + 2 * (size_t)n * TXO); }
+
+int launch_dots(Ctx& c, const double2* P, const double2* T, double2* D, double2* part) {
+  const int n = c.nspf, nb = ceil_div(c.G, DCH);
+  dots_kernel<<<nb, kTile, smem_dots(n), c.stream>>>(P, T, n, c.G, part);
   SG_LAUNCHED();
   dots_reduce_kernel<<<n * n, 128, 0, c.stream>>>(part, nb, n * n, D);
   SG_LAUNCHED();
   return SINCGPU_OK;
 }
 
+}  // namespace
+
+int orbital_dots_scratch(const Ctx& c) { return ceil_div(c.G, DCH); }
+
+int orbital_dots(Ctx& c, const double2* P, const double2* T, double2* D, double2* part) {
+  SG_CHECK(c.nspf <= kMaxOrbRhs, SINCGPU_ERANGE, "at most %d orbitals", kMaxOrbRhs);
+  SG_TRY(rhs_attrs());
+  return launch_dots(c, P, T, D, part);
+}
+
 int orbital_mix(Ctx& c, const double2* in, const double2* mat, double2* out) {
   const int n = c.nspf;
-  SG_CHECK(n <= 32, SINCGPU_ERANGE, "at most 32 orbitals");
-  SG_DISPATCH_N(n, mix_kernel, <<<ceil_div(c.G, 256), 256, 0, c.stream>>>(in, mat, n, c.G, out));
+  SG_CHECK(n <= kMaxOrbRhs, SINCGPU_ERANGE, "at most %d orbitals", kMaxOrbRhs);
+  SG_TRY(rhs_attrs());
+  mix_kernel<<<ceil_div(c.G, TXO), kTile, smem_mix(n), c.stream>>>(in, mat, n, c.G, out);
   SG_LAUNCHED();
   return SINCGPU_OK;
 }
@@ -280,9 +274,9 @@ int orbital_mix(Ctx& c, const double2* in, const double2* mat, double2* out) {
 int jac_combine(Ctx& c, const double2* T, const double2* P, const double2* M1, const double2* M2,
                 const double2* X, const double2* D2, double2* out) {
   const int n = c.nspf;
-  SG_CHECK(n <= 32, SINCGPU_ERANGE, "at most 32 orbitals");
-  SG_DISPATCH_N(n, jac_combine_kernel, <<<ceil_div(c.G, 256), 256, 0, c.stream>>>(T, P, M1, M2, X, D2, n,
-                                                                                  c.G, out));
+  SG_CHECK(n <= kMaxOrbRhs, SINCGPU_ERANGE, "at most %d orbitals", kMaxOrbRhs);
+  SG_TRY(rhs_attrs());
+  jac_combine_kernel<<<ceil_div(c.G, TXO), kTile, smem_jac(n), c.stream>>>(T, P, M1, M2, X, D2, n, c.G, out);
   SG_LAUNCHED();
   return SINCGPU_OK;
 }
@@ -297,12 +291,11 @@ int axpby(Ctx& c, double2* acc, const double2* in, double a, double b, long long
 int mult_reducedpot_range(Ctx& c, const double2* phi, const double2* redpot, int i0, int ni,
                           double2* out) {
   const int n = c.nspf;
-  SG_CHECK(n <= 32, SINCGPU_ERANGE, "at most 32 orbitals");
-  const int blocks = ceil_div(c.G, 128);
+  SG_CHECK(n <= kMaxOrbRhs, SINCGPU_ERANGE, "at most %d orbitals", kMaxOrbRhs);
+  SG_TRY(rhs_attrs());
   ProfScope ps(c, ST_RHS_REDPOT);
-  SG_DISPATCH_N(n, redpot_kernel, <<<blocks, 128, 0, c.stream>>>(phi, redpot, nullptr, nullptr,
-                                                               make_double2(1, 0), n, i0, ni, 0, c.G,
-                                                               out));
+  redpot_kernel<<<ceil_div(c.G, TXO), kTile, smem_redpot(n), c.stream>>>(
+      phi, redpot, nullptr, nullptr, make_double2(1, 0), n, i0, ni, 0, c.G, out);
   SG_LAUNCHED();
   return SINCGPU_OK;
 }
@@ -315,11 +308,10 @@ int actreduced(Ctx& c, const double2* phi, const double2* proj, const double2* d
                const double2* invdenmat, const double2* redpot, double2 timefac, int dentimeflag,
                int projflag, double zfield, double2* out) {
   const int n = c.nspf;
-  SG_CHECK(n <= 32, SINCGPU_ERANGE, "at most 32 orbitals");
+  SG_CHECK(n <= kMaxOrbRhs, SINCGPU_ERANGE, "at most %d orbitals", kMaxOrbRhs);
+  SG_TRY(rhs_attrs());
   const long long G = c.G;
-  const int nblk_dots = 4 * 148;
-  const long long xper = ((G + nblk_dots - 1) / nblk_dots + DX - 1) / DX * DX;
-  const int nb = ceil_div(G, xper);
+  const int nb = ceil_div(G, DCH);
   const size_t need = sizeof(double2) * (3 * (size_t)n * G + (size_t)nb * n * n + (size_t)n * n);
   SG_TRY(c.ws_rhs.ensure(need));
   double2* Y = (double2*)c.ws_rhs.ptr;
@@ -327,27 +319,24 @@ int actreduced(Ctx& c, const double2* phi, const double2* proj, const double2* d
   double2* T = S + (size_t)n * G;
   double2* part = T + (size_t)n * G;
   double2* D = part + (size_t)nb * n * n;
-  const int b256 = ceil_div(G, 256), b128 = ceil_div(G, 128);
+  const int bt = ceil_div(G, TXO);
   {
     ProfScope ps(c, ST_RHS_MIX);
-    SG_DISPATCH_N(n, mix_kernel, <<<b256, 256, 0, c.stream>>>(phi, denmat, n, G, Y));
+    mix_kernel<<<bt, kTile, smem_mix(n), c.stream>>>(phi, denmat, n, G, Y);
     SG_LAUNCHED();
   }
   SG_TRY(mult_ke(c, Y, S, n, true, zfield));
   double2* dst = projflag == 1 ? T : out;
   {
     ProfScope ps(c, ST_RHS_REDPOT);
-    SG_DISPATCH_N(n, redpot_kernel, <<<b128, 128, 0, c.stream>>>(phi, redpot, S, invdenmat, timefac, n, 0,
-                                                               n, dentimeflag ? 1 : 0, G, dst));
+    redpot_kernel<<<bt, kTile, smem_redpot(n), c.stream>>>(phi, redpot, S, invdenmat, timefac, n, 0, n,
+                                                           dentimeflag ? 1 : 0, G, dst);
     SG_LAUNCHED();
   }
   if (projflag == 1) {
     ProfScope ps(c, ST_RHS_PROJ);
-    dots_kernel<<<nb, 256, 0, c.stream>>>(proj, T, n, G, xper, part);
-    SG_LAUNCHED();
-    dots_reduce_kernel<<<n * n, 128, 0, c.stream>>>(part, nb, n * n, D);
-    SG_LAUNCHED();
-    SG_DISPATCH_N(n, project_kernel, <<<b256, 256, 0, c.stream>>>(T, proj, D, n, G, out));
+    SG_TRY(launch_dots(c, proj, T, D, part));
+    project_kernel<<<bt, kTile, smem_mix(n), c.stream>>>(T, proj, D, n, G, out);
     SG_LAUNCHED();
   }
   return SINCGPU_OK;
