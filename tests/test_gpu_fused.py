@@ -73,3 +73,23 @@ def test_orbital_rhs_avec_repeatable(li):
     o1 = gpu.orbital_rhs_avec(phi, a)
     o2 = gpu.orbital_rhs_avec(phi, a)
     assert np.array_equal(o1, o2)
+
+
+def test_avec_reducedpot_mirror_equals_full(li):
+    """The A-vector entry computes only the k <= i half of reducedpot and mirrors
+    it (its 2-RDM comes from one A-vector); it equals the full product of the
+    general mean-field entry on the same 2-RDM to rounding."""
+    import torch
+    sysm, gpu, ow, phi, a = li
+    n, G = phi.shape[1], sysm.G
+    cx = dict(dtype=torch.complex128, device="cuda")
+    dphi = torch.from_numpy(np.ascontiguousarray(phi.T)).cuda()
+    da = torch.from_numpy(a).cuda()
+    den, inv = torch.empty((n, n), **cx), torch.empty((n, n), **cx)
+    tally, mat = torch.empty((n,) * 4, **cx), torch.empty((n,) * 4, **cx)
+    rp_half, rp_full, out = torch.empty((n, n, G), **cx), torch.empty((n, n, G), **cx), torch.empty((n, G), **cx)
+    gpu.orbital_rhs_avec_dev(dphi, da, den, inv, tally, mat, rp_half, out)
+    gpu.mean_field_dev(dphi, tally, mat, rp_full)
+    torch.cuda.synchronize()
+    err = float((rp_half - rp_full).abs().max() / rp_full.abs().max())
+    assert err < 1e-13

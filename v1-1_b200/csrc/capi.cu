@@ -130,6 +130,24 @@ int twoe_core(Ctx& c, const double2* phi1, const double2* phi2, double2* twoemat
   return SINCGPU_OK;
 }
 
+// twoematel and reducedpot of one orbital set; tally_herm when the 2-RDM is the one
+// of a single A-vector (the library built it), which lets reducedpot be mirrored
+int mean_field(Ctx& c, const double2* phi, const double2* tally, double2* twoematel, double2* reducedpot,
+               bool tally_herm) {
+  std::vector<int> pa, pb;
+  bool herm;
+  SG_TRY(twoe_core(c, phi, phi, twoematel, nullptr, pa, pb, herm));
+  return reduced_pot(c, (const double*)c.ws_red.ptr, pa.data(), pb.data(), (int)pa.size(), herm, tally,
+                     reducedpot, tally_herm);
+}
+
+int orbital_rhs(Ctx& c, const double2* phi, const double2* tally, const double2* denmat, const double2* invdenmat,
+                double2 timefac, double ztdpot, double2* twoematel, double2* reducedpot, double2* out,
+                bool tally_herm) {
+  SG_TRY(mean_field(c, phi, tally, twoematel, reducedpot, tally_herm));
+  return actreduced(c, phi, phi, denmat, invdenmat, reducedpot, timefac, 1, 1, ztdpot, out);
+}
+
 }  // namespace sincgpu
 
 using namespace sincgpu;
@@ -320,16 +338,13 @@ int sincgpu_mult_reducedpot_dev(sincgpu_ctx* h, const double* inspfs, double* ou
   return mult_reducedpot(h->c, (const double2*)inspfs, (const double2*)reducedpot, (double2*)outspfs);
 }
 
+
 int sincgpu_mean_field_dev(sincgpu_ctx* h, const double* phi, const double* tally, double* twoematel,
                            double* reducedpot) {
   CTX_CHECK(h);
   SG_CHECK(phi && tally && reducedpot, SINCGPU_EINVAL, "null argument");
-  Ctx& c = h->c;
-  std::vector<int> pa, pb;
-  bool herm;
-  SG_TRY(twoe_core(c, (const double2*)phi, (const double2*)phi, (double2*)twoematel, nullptr, pa, pb, herm));
-  return reduced_pot(c, (const double*)c.ws_red.ptr, pa.data(), pb.data(), (int)pa.size(), herm,
-                     (const double2*)tally, (double2*)reducedpot);
+  return mean_field(h->c, (const double2*)phi, (const double2*)tally, (double2*)twoematel, (double2*)reducedpot,
+                    false);
 }
 
 int sincgpu_actreduced_dev(sincgpu_ctx* h, int dentimeflag, const double* inspfs, const double* projspfs,
@@ -351,10 +366,9 @@ int sincgpu_orbital_rhs_dev(sincgpu_ctx* h, const double* phi, const double* tal
   CTX_CHECK(h);
   SG_CHECK(phi && tally && denmat && invdenmat && reducedpot && out, SINCGPU_EINVAL, "null argument");
   SG_CHECK(out != phi, SINCGPU_EINVAL, "out must not alias phi");
-  SG_TRY(sincgpu_mean_field_dev(h, phi, tally, twoematel, reducedpot));
-  return actreduced(h->c, (const double2*)phi, (const double2*)phi, (const double2*)denmat,
-                    (const double2*)invdenmat, (const double2*)reducedpot, make_double2(tre, tim), 1, 1,
-                    ztdpot, (double2*)out);
+  return orbital_rhs(h->c, (const double2*)phi, (const double2*)tally, (const double2*)denmat,
+                     (const double2*)invdenmat, make_double2(tre, tim), ztdpot, (double2*)twoematel,
+                     (double2*)reducedpot, (double2*)out, false);
 }
 
 // ---------------------------------------------------------------------------

@@ -211,10 +211,13 @@ int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* h, const double* phi, const double
   CTX_CHECK(h);
   SG_CHECK(phi && avector && denmat && invdenmat && tally && reducedpot && out, SINCGPU_EINVAL,
            "null argument");
+  SG_CHECK(out != phi, SINCGPU_EINVAL, "out must not alias phi");
   SG_TRY(sincgpu_getdenmat_dev(h, avector, denmat, invdenmat, 1e-10));
   SG_TRY(sincgpu_get_tworeducedx_dev(h, avector, avector, tally));
-  return sincgpu_orbital_rhs_dev(h, phi, tally, denmat, invdenmat, tre, tim, ztdpot, twoematel, reducedpot,
-                                 out);
+  // the 2-RDM of one A-vector: reducedpot(x,i,k) = conj reducedpot(x,k,i)
+  return orbital_rhs(h->c, (const double2*)phi, (const double2*)tally, (const double2*)denmat,
+                     (const double2*)invdenmat, make_double2(tre, tim), ztdpot, (double2*)twoematel,
+                     (double2*)reducedpot, (double2*)out, true);
 }
 
 int sincgpu_expoavecprop_dev(sincgpu_ctx* h, const double* avec_in, double* avec_out, double t,

@@ -158,7 +158,7 @@ int all_matel(Ctx& c) {
 int get_reducedpot(Ctx& c) {
   CmfState& m = c.cmf;
   return reduced_pot(c, (const double*)c.ws_red.ptr, m.pa.data(), m.pb.data(), (int)m.pa.size(), m.herm,
-                     m.tally[0], m.rp[0]);
+                     m.tally[0], m.rp[0], true);  // 2-RDM of one A-vector
 }
 
 // the CI matrices the sigma product uses: slot 0, or w1 slot1 + w0 slot0

@@ -61,7 +61,7 @@ struct IntCache {
   int* dev = nullptr;
   size_t cap = 0;
 };
-enum IntSlot { IC_PA = 0, IC_PB, IC_LUT, IC_COUNT };
+enum IntSlot { IC_PA = 0, IC_PB, IC_LUT, IC_TMAP, IC_COUNT };
 
 // saved variables of the orbital exponential propagator (expospfprop)
 struct OrbPropState {
@@ -216,9 +216,20 @@ int coulomb_dens(Ctx& c, const double2* dens, int m, double2* red);
 // contract.cu
 int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa,
                const int* h_pb, int npair, const double* Rpl, bool herm, double2* twoematel);
+// tally_herm: the 2-RDM has Gamma(c,d,k,i) = conj Gamma(d,c,i,k) (one A-vector);
+// with a hermitian pair list only the k <= i half of reducedpot is computed and
+// the rest mirrored
 int reduced_pot(Ctx& c, const double* Rpl, const int* h_pa, const int* h_pb, int npair,
-                bool herm, const double2* tally, double2* reducedpot);
+                bool herm, const double2* tally, double2* reducedpot, bool tally_herm = false);
 int reduced_pot_full(Ctx& c, const double2* twoereduced, const double2* tally, double2* reducedpot);
+
+// capi.cu: twoematel + reducedpot of one orbital set, and that followed by
+// actreduced00 (tally_herm: see reduced_pot)
+int mean_field(Ctx& c, const double2* phi, const double2* tally, double2* twoematel, double2* reducedpot,
+               bool tally_herm);
+int orbital_rhs(Ctx& c, const double2* phi, const double2* tally, const double2* denmat, const double2* invdenmat,
+                double2 timefac, double ztdpot, double2* twoematel, double2* reducedpot, double2* out,
+                bool tally_herm);
 
 // ke.cu: out = KE(in) [+ pot*in + zfield*z*in when `extra`]
 int mult_ke(Ctx& c, const double2* in, double2* out, int howmany, bool extra, double zfield);

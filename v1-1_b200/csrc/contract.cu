@@ -244,6 +244,125 @@ __global__ void __launch_bounds__(256, 2) twoe_gemm2_kernel(const double2* __res
   }
 }
 
+// twoematel GEMM with square 16R x 16R tiles (R x R register blocks, 256
+// threads): for 2U <= 16R one tile covers all outputs (R = 7 gives 112 x 112,
+// enough for U = 55), so neither the pair products nor the orbital
+// tiles are recomputed per column tile and padding stays small.  Split-K over x
+// across the SMs; cp.async double buffering of the orbital values and Rpl rows.
+template <int R>
+__global__ void __launch_bounds__(256, 1) twoe_gemm3_kernel(const double2* __restrict__ phi1,
+                                                            const double2* __restrict__ phi2,
+                                                            const int* __restrict__ pa,
+                                                            const int* __restrict__ pb,
+                                                            const double* __restrict__ Rpl, int npair,
+                                                            int nspf, long long G, int ntn,
+                                                            long long xper, double* __restrict__ part) {
+  constexpr int TT = 16 * R;
+  extern __shared__ __align__(16) double dsm[];
+  double* As = dsm;                                   // [TT][TK+1]
+  double* Bs = As + TT * (TK + 1);                    // [2][TT][TK+1]
+  double2* fsm = reinterpret_cast<double2*>(Bs + 2 * TT * (TK + 1));  // [2][2][nspf][TK]
+  int* sa = reinterpret_cast<int*>(fsm + 4 * nspf * TK);
+  int* sb = sa + TT;
+  int* sc = sb + TT;
+  auto f1 = [&](int st, int o, int k) -> double2& { return fsm[((st * 2 + 0) * nspf + o) * TK + k]; };
+  auto f2 = [&](int st, int o, int k) -> double2& { return fsm[((st * 2 + 1) * nspf + o) * TK + k]; };
+  const int M = 2 * npair;
+  const int tm = blockIdx.x / ntn, tn = blockIdx.x % ntn;
+  const int m0 = tm * TT, n0 = tn * TT;
+  const long long xb = blockIdx.y * xper;
+  const long long xe = min(G, xb + xper);
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  for (int i = tid; i < TT; i += 256) {
+    const int m = m0 + i;
+    if (m < M) {
+      const int p = m % npair;
+      sa[i] = pa[p];
+      sb[i] = pb[p];
+      sc[i] = m / npair;
+    } else {
+      sa[i] = 0;
+      sb[i] = 0;
+      sc[i] = -1;
+    }
+  }
+  auto load = [&](int st, long long x0) {
+    for (int i = tid; i < nspf * TK; i += 256) {
+      const int o = i / TK, k = i % TK;
+      const long long x = x0 + k;
+      const bool ok = x < xe;
+      const double2* g1 = ok ? phi1 + (long long)o * G + x : phi1;
+      const double2* g2 = ok ? phi2 + (long long)o * G + x : phi2;
+      cp_async8(&f1(st, o, k), g1, ok);
+      cp_async8(reinterpret_cast<double*>(&f1(st, o, k)) + 1, reinterpret_cast<const double*>(g1) + 1, ok);
+      cp_async8(&f2(st, o, k), g2, ok);
+      cp_async8(reinterpret_cast<double*>(&f2(st, o, k)) + 1, reinterpret_cast<const double*>(g2) + 1, ok);
+    }
+    for (int i = tid; i < TK * TT; i += 256) {
+      const int nn = i / TK, k = i % TK;
+      const int n = n0 + nn;
+      const long long x = x0 + k;
+      const bool ok = n < M && x < xe;
+      cp_async8(&Bs[(st * TT + nn) * (TK + 1) + k], ok ? (const void*)(Rpl + (long long)n * G + x) : (const void*)Rpl,
+                ok);
+    }
+    cp_async_commit();
+  };
+  double acc[R][R];
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+#pragma unroll
+    for (int j = 0; j < R; ++j) acc[i][j] = 0.0;
+  const long long nk = (xe - xb + TK - 1) / TK;
+  __syncthreads();  // sa/sb/sc visible
+  if (nk > 0) load(0, xb);
+  for (long long t = 0; t < nk; ++t) {
+    const int st = (int)(t & 1);
+    if (t + 1 < nk) {
+      load(st ^ 1, xb + (t + 1) * TK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    for (int i = tid; i < TK * TT; i += 256) {
+      const int mm = i / TK, k = i % TK;
+      double v = 0.0;
+      const int comp = sc[mm];
+      if (comp >= 0) {
+        const double2 r = cmulc(f1(st, sa[mm], k), f2(st, sb[mm], k));
+        v = comp == 0 ? r.x : r.y;
+      }
+      As[mm * (TK + 1) + k] = v;
+    }
+    __syncthreads();
+    const double* Bst = Bs + st * TT * (TK + 1);
+#pragma unroll 4
+    for (int k = 0; k < TK; ++k) {
+      double a[R], b[R];
+#pragma unroll
+      for (int i = 0; i < R; ++i) a[i] = As[(tx + 16 * i) * (TK + 1) + k];
+#pragma unroll
+      for (int j = 0; j < R; ++j) b[j] = Bst[(ty + 16 * j) * (TK + 1) + k];
+#pragma unroll
+      for (int i = 0; i < R; ++i)
+#pragma unroll
+        for (int j = 0; j < R; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+  double* out = part + (long long)blockIdx.y * M * M;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int m = m0 + tx + 16 * i;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int n = n0 + ty + 16 * j;
+      if (m < M && n < M) out[(long long)m * M + n] = acc[i][j];
+    }
+  }
+}
+
 // C[m][n] = sum_s part[s][m][n] in split order (deterministic)
 __global__ void split_reduce_kernel(const double* __restrict__ part, int nsplit, long long MM,
                                     double* __restrict__ C) {
@@ -306,10 +425,18 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
   const int n = c.nspf;
   SG_CHECK(n <= kMaxOrb, SINCGPU_ERANGE, "at most %d orbitals (got %d)", kMaxOrb, n);
   const int M = 2 * npair;
-  const int ntm = ceil_div(M, TM), ntn = ceil_div(M, TN);
+  // register block R: the smallest of 2..9 whose 16R tile holds M, else 8 (multi-tile)
+  int R = 8;
+  for (int r = 2; r <= 9; ++r)
+    if (16 * r >= M) {
+      R = r;
+      break;
+    }
+  const int TT = 16 * R;
+  const int ntm = ceil_div(M, TT), ntn = ntm;
   const int ntiles = ntm * ntn;
-  long long target = 2LL * 148;
-  int nsplit = (int)std::max(1LL, std::min((long long)ceil_div(c.G, TK), target / ntiles));
+  long long target = 148;  // one 256-thread CTA per SM (R x R accumulators per thread)
+  int nsplit = (int)std::max(1LL, std::min((long long)ceil_div(c.G, TK), std::max(1LL, target / ntiles)));
   long long xper = ((c.G + nsplit - 1) / nsplit + TK - 1) / TK * TK;
   nsplit = ceil_div(c.G, xper);
   const long long MM = (long long)M * M;
@@ -325,15 +452,35 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
   SG_TRY(cached_ints(c, IC_LUT, lut.data(), (size_t)n * n, &d_lut));
   {
     ProfScope ps(c, ST_TWOE_GEMM);
-    const size_t fbytes = sizeof(double2) * 4 * (size_t)n * TK;
-    static bool attr = false;
-    if (!attr) {
-      SG_CUDA(cudaFuncSetAttribute(twoe_gemm2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(sizeof(double2) * 4 * kMaxOrb * TK)));
-      attr = true;
+    const size_t sbytes = sizeof(double) * 3 * (size_t)TT * (TK + 1) + sizeof(double2) * 4 * (size_t)n * TK +
+                          sizeof(int) * 3 * (size_t)TT;
+    const dim3 grid(ntiles, nsplit);
+#define SG_TWOE_CASE(RR)                                                                                   \
+  case RR: {                                                                                               \
+    static bool attr = false;                                                                              \
+    if (!attr) {                                                                                           \
+      SG_CUDA(cudaFuncSetAttribute(twoe_gemm3_kernel<RR>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
+                                   (int)(sizeof(double) * 3 * 16 * RR * (TK + 1) +                         \
+                                         sizeof(double2) * 4 * kMaxOrb * TK + sizeof(int) * 3 * 16 * RR))); \
+      attr = true;                                                                                         \
+    }                                                                                                      \
+    twoe_gemm3_kernel<RR><<<grid, 256, sbytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl, npair, n, c.G, ntn, \
+                                                          xper, part);                                    \
+    break;                                                                                                 \
+  }
+    switch (R) {
+      SG_TWOE_CASE(2)
+      SG_TWOE_CASE(3)
+      SG_TWOE_CASE(4)
+      SG_TWOE_CASE(5)
+      SG_TWOE_CASE(6)
+      SG_TWOE_CASE(7)
+      SG_TWOE_CASE(8)
+      SG_TWOE_CASE(9)
+      default:
+        break;
     }
-    twoe_gemm2_kernel<<<dim3(ntiles, nsplit), 256, fbytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl, npair,
-                                                                       n, c.G, ntn, xper, part);
+#undef SG_TWOE_CASE
     SG_LAUNCHED();
   }
   ProfScope ps(c, ST_TWOE_FINISH);
@@ -364,6 +511,36 @@ __global__ void build_w_kernel(const double2* __restrict__ tally, const int* __r
   double2 g1 = tally[cc + n * d + tail];
   double2 A, B;
   if (herm && cc != d) {
+    double2 g2 = tally[d + n * cc + tail];
+    A = cadd(g1, g2);
+    double2 df = csub(g1, g2);
+    B = make_double2(-df.y, df.x);
+  } else {
+    A = g1;
+    B = make_double2(-g1.y, g1.x);
+  }
+  double2 v = comp == 0 ? A : B;
+  Wm[idx] = (col & 1) ? v.y : v.x;
+}
+
+// Half-column W: columns c = 2t + {re, im} for the orbital pairs t = (kk, ii),
+// kk <= ii, listed in tmap (kk, ii interleaved).  With a hermitian pair list and a
+// 2-RDM of one A-vector (Gamma(c,d,k,i) = conj Gamma(d,c,i,k)), reducedpot(x,i,k)
+// = conj reducedpot(x,k,i), so these columns determine all of it.
+__global__ void build_w_half_kernel(const double2* __restrict__ tally, const int* __restrict__ pa,
+                                    const int* __restrict__ pb, const int* __restrict__ tmap, int npair, int n,
+                                    int nt, double* __restrict__ Wm) {
+  const int NC = 2 * nt;
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= 2LL * npair * NC) return;
+  int k = (int)(idx / NC), col = (int)(idx % NC);
+  int p = k % npair, comp = k / npair;
+  int cc = pa[p], d = pb[p];
+  const int t = col / 2, kk = tmap[2 * t], ii = tmap[2 * t + 1];
+  long long tail = (long long)n * n * (kk + (long long)n * ii);
+  double2 g1 = tally[cc + n * d + tail];
+  double2 A, B;
+  if (cc != d) {
     double2 g2 = tally[d + n * cc + tail];
     A = cadd(g1, g2);
     double2 df = csub(g1, g2);
@@ -447,6 +624,87 @@ __global__ void __launch_bounds__(256, 2) rp_gemm2_kernel(const double* __restri
   }
 }
 
+// reducedpot GEMM with 128 (x) x 4CG (columns) tiles, 16 x CG threads of 8x4
+// register blocks; CG is chosen per call so that the 2n^2 columns pad least.
+template <int CG, bool HALF>
+__global__ void __launch_bounds__(16 * CG) rp_gemm3_kernel(const double* __restrict__ Rpl,
+                                                           const double* __restrict__ Wm, int K, int NC,
+                                                           long long G, double2* __restrict__ out,
+                                                           const int* __restrict__ tmap, int n) {
+  constexpr int NT = 16 * CG, TNC = 4 * CG;
+  __shared__ __align__(16) double As[2][RK][RM];
+  __shared__ __align__(16) double Bs[2][RK][TNC];
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  const long long x0 = (long long)blockIdx.x * RM;
+  const int c0 = blockIdx.y * TNC;
+  auto load = [&](int st, int k0) {
+    for (int i = tid; i < RK * RM; i += NT) {
+      const int k = i / RM, xx = i % RM;
+      const long long x = x0 + xx;
+      const bool ok = (k0 + k < K) && x < G;
+      cp_async8(&As[st][k][xx], ok ? (const void*)(Rpl + (long long)(k0 + k) * G + x) : (const void*)Rpl, ok);
+    }
+    for (int i = tid; i < RK * TNC; i += NT) {
+      const int k = i / TNC, cc = i % TNC;
+      const bool ok = (k0 + k < K) && (c0 + cc < NC);
+      cp_async8(&Bs[st][k][cc], ok ? (const void*)(Wm + (long long)(k0 + k) * NC + c0 + cc) : (const void*)Wm, ok);
+    }
+    cp_async_commit();
+  };
+  double acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  const int nk = (K + RK - 1) / RK;
+  load(0, 0);
+  for (int t = 0; t < nk; ++t) {
+    const int st = t & 1;
+    if (t + 1 < nk) {
+      load(st ^ 1, (t + 1) * RK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < RK; ++k) {
+      double a[8], b[4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = As[st][k][tx + 16 * i];
+      const double2 b01 = *reinterpret_cast<const double2*>(&Bs[st][k][4 * ty]);
+      const double2 b23 = *reinterpret_cast<const double2*>(&Bs[st][k][4 * ty + 2]);
+      b[0] = b01.x;
+      b[1] = b01.y;
+      b[2] = b23.x;
+      b[3] = b23.y;
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const long long x = x0 + tx + 16 * i;
+    if (x >= G) continue;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int col = c0 + 4 * ty + 2 * h;
+      if (col >= NC) continue;
+      const double2 v = make_double2(acc[i][2 * h], acc[i][2 * h + 1]);
+      if (HALF) {
+        const int t = col / 2, kk = tmap[2 * t], ii = tmap[2 * t + 1];
+        out[(long long)(kk + n * ii) * G + x] = v;
+        if (kk != ii) out[(long long)(ii + n * kk) * G + x] = make_double2(v.x, -v.y);
+      } else {
+        out[(long long)(col / 2) * G + x] = v;
+      }
+    }
+  }
+}
+
 // out[(ki*G + x)] (complex) = sum_k Rpl[k*G+x] * Wm[k][2ki + {0,1}]
 constexpr int RBK = 16;
 __global__ void __launch_bounds__(256) rp_gemm_kernel(const double* __restrict__ Rpl,
@@ -500,31 +758,72 @@ __global__ void __launch_bounds__(256) rp_gemm_kernel(const double* __restrict__
 }
 
 static int reduced_pot_impl(Ctx& c, const double* Rpl, const int* h_pa, const int* h_pb, int npair,
-                            bool herm, const double2* tally, double2* reducedpot) {
+                            bool herm, const double2* tally, double2* reducedpot, bool half) {
   const int n = c.nspf;
-  const int K = 2 * npair, NC = 2 * n * n;
+  half = half && herm;
+  const int nt = n * (n + 1) / 2;
+  const int K = 2 * npair, NC = half ? 2 * nt : 2 * n * n;
   size_t need = sizeof(double) * (size_t)K * NC;
   SG_TRY(c.ws_gemm.ensure(need));
   double* Wm = (double*)c.ws_gemm.ptr;
-  const int *d_pa, *d_pb;
+  const int *d_pa, *d_pb, *d_tmap = nullptr;
   SG_TRY(cached_ints(c, IC_PA, h_pa, npair, &d_pa));
   SG_TRY(cached_ints(c, IC_PB, h_pb, npair, &d_pb));
+  if (half) {
+    std::vector<int> tm;
+    tm.reserve(2 * (size_t)nt);
+    for (int ii = 0; ii < n; ++ii)
+      for (int kk = 0; kk <= ii; ++kk) {
+        tm.push_back(kk);
+        tm.push_back(ii);
+      }
+    SG_TRY(cached_ints(c, IC_TMAP, tm.data(), tm.size(), &d_tmap));
+  }
   {
     ProfScope ps(c, ST_RP_W);
-    build_w_kernel<<<ceil_div((long long)K * NC, 256), 256, 0, c.stream>>>(tally, d_pa, d_pb, npair, n,
-                                                                           herm ? 1 : 0, Wm);
+    if (half)
+      build_w_half_kernel<<<ceil_div((long long)K * NC, 256), 256, 0, c.stream>>>(tally, d_pa, d_pb, d_tmap,
+                                                                                  npair, n, nt, Wm);
+    else
+      build_w_kernel<<<ceil_div((long long)K * NC, 256), 256, 0, c.stream>>>(tally, d_pa, d_pb, npair, n,
+                                                                             herm ? 1 : 0, Wm);
     SG_LAUNCHED();
   }
-  dim3 grid(ceil_div(c.G, RM), ceil_div(NC, RN));
+  // column groups: the CG in {8, 10, 12, 14, 16} (tiles of 4 CG columns) with the
+  // fewest padded columns, the widest on ties
+  int best = 16;
+  long long waste = -1;
+  for (int cg : {16, 14, 12, 10, 8}) {
+    const long long w = (long long)ceil_div(NC, 4 * cg) * 4 * cg - NC;
+    if (waste < 0 || w < waste) {
+      waste = w;
+      best = cg;
+    }
+  }
   ProfScope ps(c, ST_RP_GEMM);
-  rp_gemm2_kernel<<<grid, 256, 0, c.stream>>>(Rpl, Wm, K, NC, c.G, reducedpot);
+  const int gx = ceil_div(c.G, RM);
+#define SG_RP_LAUNCH(CG)                                                                                   \
+  if (half)                                                                                                \
+    rp_gemm3_kernel<CG, true><<<dim3(gx, ceil_div(NC, 4 * CG)), 16 * CG, 0, c.stream>>>(Rpl, Wm, K, NC, c.G, \
+                                                                                        reducedpot, d_tmap, n); \
+  else                                                                                                     \
+    rp_gemm3_kernel<CG, false><<<dim3(gx, ceil_div(NC, 4 * CG)), 16 * CG, 0, c.stream>>>(Rpl, Wm, K, NC, c.G, \
+                                                                                         reducedpot, nullptr, n);
+  switch (best) {
+    case 8: SG_RP_LAUNCH(8) break;
+    case 10: SG_RP_LAUNCH(10) break;
+    case 12: SG_RP_LAUNCH(12) break;
+    case 14: SG_RP_LAUNCH(14) break;
+    default: SG_RP_LAUNCH(16) break;
+  }
+#undef SG_RP_LAUNCH
   SG_LAUNCHED();
   return SINCGPU_OK;
 }
 
 int reduced_pot(Ctx& c, const double* Rpl, const int* h_pa, const int* h_pb, int npair, bool herm,
-                const double2* tally, double2* reducedpot) {
-  return reduced_pot_impl(c, Rpl, h_pa, h_pb, npair, herm, tally, reducedpot);
+                const double2* tally, double2* reducedpot, bool tally_herm) {
+  return reduced_pot_impl(c, Rpl, h_pa, h_pb, npair, herm, tally, reducedpot, tally_herm);
 }
 
 // twoereduced(G, n^2) interleaved -> planar rows for all ordered pairs
@@ -551,7 +850,7 @@ int reduced_pot_full(Ctx& c, const double2* twoereduced, const double2* tally, d
   double* Rpl = (double*)c.ws_conv.ptr;
   to_planar_kernel<<<ceil_div(total, 256), 256, 0, c.stream>>>(twoereduced, total, total, Rpl);
   SG_LAUNCHED();
-  return reduced_pot_impl(c, Rpl, pa.data(), pb.data(), npair, false, tally, reducedpot);
+  return reduced_pot_impl(c, Rpl, pa.data(), pb.data(), npair, false, tally, reducedpot, false);
 }
 
 }  // namespace sincgpu
