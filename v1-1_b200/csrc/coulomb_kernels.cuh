@@ -39,7 +39,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
     const double2* __restrict__ phi1, const double2* __restrict__ phi2, CoulArgs<C> ca) {
   constexpr int P = P1 * P2, S = P1 > P2 ? P1 : P2, TL = lines_for(P);
   __shared__ C roots[P];
-  __shared__ C ex[P * TL];
+  __shared__ C ex[(P + 1) * TL];
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int s = threadIdx.x % S, l = threadIdx.x / S;
@@ -63,7 +63,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
     a[n1] = cvt<C>(v);
   }
   __syncthreads();
-  dft_in_to_out<P1, P2, false, C>(a, b, s, l, TL, ex, roots);
+  dft_in_to_out<P1, P2, false, C, true>(a, b, s, l, TL, ex, roots);
   if (row && s < P1) {
     C* dst = ca.W1 + (((long long)p * N + z) * N + y) * P;
 #pragma unroll
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
     CoulArgs<C> ca, double* __restrict__ Rpl, double2* __restrict__ full, int herm) {
   constexpr int P = P1 * P2, S = P1 > P2 ? P1 : P2, TL = lines_for(P);
   __shared__ C roots[P];
-  __shared__ C ex[P * TL];
+  __shared__ C ex[(P + 1) * TL];
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int s = threadIdx.x % S, l = threadIdx.x / S;
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   for (int n1 = 0; n1 < P1; ++n1)
     a[n1] = (row && s < P2) ? src[s + P2 * n1] : CplxTraits<C>::make(0.0, 0.0);
   __syncthreads();
-  dft_in_to_out<P1, P2, true, C>(a, b, s, l, TL, ex, roots);
+  dft_in_to_out<P1, P2, true, C, true>(a, b, s, l, TL, ex, roots);
   if (!(row && s < P1)) return;
   const long long G = ca.G;
   const long long g0 = (long long)z * N * N + (long long)y * N;

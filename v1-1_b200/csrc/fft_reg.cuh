@@ -51,10 +51,18 @@ struct RegFFT<M, M, INV, C> {
   __device__ __forceinline__ static void run(C (&)[M], const C*, int) {}
 };
 
-// ex: exchange buffer of P*TL complex values for TL lines; element e of line l at ex[e*TL + l].
+// ex: exchange buffer for TL lines.  Element e of line l sits at ex[e*TL + l]
+// (element-major, for kernels whose lanes run over lines: column passes) or, with
+// ROW, at ex[l*(P+1) + e] (line-major, for kernels whose lanes run along a line:
+// row passes), so that consecutive lanes touch consecutive addresses either way.
 // Threads with s >= P2 (step 1) or s >= P1 (step 2) idle in that step.
 // On entry a[] holds D_in (valid for s < P2); on exit b[] holds D_out (valid for s < P1).
-template <int P1, int P2, bool INV, class C>
+template <int P, bool ROW>
+__device__ __forceinline__ int ex_at(int e, int l, int TL) {
+  return ROW ? l * (P + 1) + e : e * TL + l;
+}
+
+template <int P1, int P2, bool INV, class C, bool ROW = false>
 __device__ __forceinline__ void dft_in_to_out(C (&a)[P1], C (&b)[P2], int s, int l, int TL, C* ex,
                                               const C* roots) {
   constexpr int P = P1 * P2;
@@ -64,20 +72,20 @@ __device__ __forceinline__ void dft_in_to_out(C (&a)[P1], C (&b)[P2], int s, int
     for (int k1 = 0; k1 < P1; ++k1) {
       C v = a[k1];
       if (k1 > 0 && s > 0) v = cmul(v, root<INV>(roots, s * k1));
-      ex[(k1 * P2 + s) * TL + l] = v;
+      ex[ex_at<P, ROW>(k1 * P2 + s, l, TL)] = v;
     }
   }
   __syncthreads();
   if (s < P1) {
 #pragma unroll
-    for (int n2 = 0; n2 < P2; ++n2) b[n2] = ex[(s * P2 + n2) * TL + l];
+    for (int n2 = 0; n2 < P2; ++n2) b[n2] = ex[ex_at<P, ROW>(s * P2 + n2, l, TL)];
     RegFFT<P2, 1, INV, C>::run(b, roots, P);
   }
   __syncthreads();
 }
 
 // On entry b[] holds D_out (valid for s < P1); on exit a[] holds D_in (valid for s < P2).
-template <int P1, int P2, bool INV, class C>
+template <int P1, int P2, bool INV, class C, bool ROW = false>
 __device__ __forceinline__ void dft_out_to_in(C (&b)[P2], C (&a)[P1], int s, int l, int TL, C* ex,
                                               const C* roots) {
   constexpr int P = P1 * P2;
@@ -87,13 +95,13 @@ __device__ __forceinline__ void dft_out_to_in(C (&b)[P2], C (&a)[P1], int s, int
     for (int m2 = 0; m2 < P2; ++m2) {
       C v = b[m2];
       if (m2 > 0 && s > 0) v = cmul(v, root<INV>(roots, s * m2));
-      ex[(m2 * P1 + s) * TL + l] = v;
+      ex[ex_at<P, ROW>(m2 * P1 + s, l, TL)] = v;
     }
   }
   __syncthreads();
   if (s < P2) {
 #pragma unroll
-    for (int k1 = 0; k1 < P1; ++k1) a[k1] = ex[(s * P1 + k1) * TL + l];
+    for (int k1 = 0; k1 < P1; ++k1) a[k1] = ex[ex_at<P, ROW>(s * P1 + k1, l, TL)];
     RegFFT<P1, 1, INV, C>::run(a, roots, P);
   }
   __syncthreads();
