@@ -43,9 +43,9 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int s = threadIdx.x % S, l = threadIdx.x / S;
-  const int p = blockIdx.z, z = blockIdx.y, y = blockIdx.x * TL + l;
-  const bool row = y < N;
-  const long long off = (long long)z * N * N + (long long)y * N;
+  const int p = blockIdx.z, f = blockIdx.x * TL + l;  // row f = z*N + y
+  const bool row = f < N * N;
+  const long long off = (long long)f * N;
   const double2* s1;
   const double2* s2 = nullptr;
   if (DENS) {
@@ -65,7 +65,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   __syncthreads();
   dft_in_to_out<P1, P2, false, C, true>(a, b, s, l, TL, ex, roots);
   if (row && s < P1) {
-    C* dst = ca.W1 + (((long long)p * N + z) * N + y) * P;
+    C* dst = ca.W1 + ((long long)p * N * N + f) * P;
 #pragma unroll
     for (int k2 = 0; k2 < P2; ++k2) dst[s + P1 * k2] = b[k2];
   }
@@ -80,8 +80,9 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int l = threadIdx.x % TL, s = threadIdx.x / TL;
-  const int p = blockIdx.z, z = blockIdx.y, kx = blockIdx.x * TL + l;
-  const bool col = kx < P;
+  const int p = blockIdx.z, f = blockIdx.x * TL + l;  // column f = z*P + kx
+  const bool col = f < N * P;
+  const int z = f / P, kx = f - z * P;
   const C* src = ca.W1 + ((long long)p * N + z) * N * P + kx;
   C a[P1], b[P2];
 #pragma unroll
@@ -107,10 +108,10 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int l = threadIdx.x % TL, s = threadIdx.x / TL;
-  const int p = blockIdx.z, ky = blockIdx.y, kx = blockIdx.x * TL + l;
-  const bool col = kx < P;
+  const int p = blockIdx.z, f = blockIdx.x * TL + l;  // column f = ky*P + kx
   const long long zs = (long long)P * P;
-  C* base = ca.W2 + (long long)p * N * zs + (long long)ky * P + kx;
+  const bool col = f < zs;
+  C* base = ca.W2 + (long long)p * N * zs + f;
   C a[P1], b[P2];
 #pragma unroll
   for (int n1 = 0; n1 < P1; ++n1) {
@@ -120,7 +121,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   __syncthreads();
   dft_in_to_out<P1, P2, false, C>(a, b, s, l, TL, ex, roots);
   if (col && s < P1) {
-    const C* kh = ca.khat + (long long)ky * P + kx;
+    const C* kh = ca.khat + f;
 #pragma unroll
     for (int k2 = 0; k2 < P2; ++k2) b[k2] = cmul(b[k2], kh[(long long)(s + P1 * k2) * zs]);
   }
@@ -143,8 +144,9 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int l = threadIdx.x % TL, s = threadIdx.x / TL;
-  const int p = blockIdx.z, z = blockIdx.y, kx = blockIdx.x * TL + l;
-  const bool col = kx < P;
+  const int p = blockIdx.z, f = blockIdx.x * TL + l;  // column f = z*P + kx
+  const bool col = f < N * P;
+  const int z = f / P, kx = f - z * P;
   const C* src = ca.W2 + ((long long)p * N + z) * P * P + kx;
   C a[P1], b[P2];
 #pragma unroll
@@ -172,9 +174,9 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int s = threadIdx.x % S, l = threadIdx.x / S;
-  const int p = blockIdx.z, z = blockIdx.y, y = blockIdx.x * TL + l;
-  const bool row = y < N;
-  const C* src = ca.W1 + (((long long)p * N + z) * N + y) * P;
+  const int p = blockIdx.z, f = blockIdx.x * TL + l;  // row f = z*N + y
+  const bool row = f < N * N;
+  const C* src = ca.W1 + ((long long)p * N * N + f) * P;
   C a[P1], b[P2];
 #pragma unroll
   for (int n1 = 0; n1 < P1; ++n1)
@@ -183,7 +185,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   dft_in_to_out<P1, P2, true, C, true>(a, b, s, l, TL, ex, roots);
   if (!(row && s < P1)) return;
   const long long G = ca.G;
-  const long long g0 = (long long)z * N * N + (long long)y * N;
+  const long long g0 = (long long)f * N;
   const int gp = ca.pair0 + p;
   long long off_ab, off_ba = 0;
   bool mirror = false;
@@ -220,36 +222,39 @@ int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2*
   constexpr int P = P1 * P2, S = P1 > P2 ? P1 : P2, TL = lines_for(P);
   const int N = ca.N;
   const int nthr = S * TL;
-  const int nrow = ceil_div(N, TL), ncol = ceil_div(P, TL);
+  // lines are flattened over the two outer axes so that no lane idles past the
+  // end of a row of lines: rows f = z*N + y (x passes), columns f = z*P + kx
+  // (y passes) and f = ky*P + kx (z pass)
+  const int nrow = ceil_div(N * N, TL), ncol = ceil_div(N * P, TL), nzc = ceil_div(P * P, TL);
   {
     ProfScope ps(c, ST_COUL_FWD_X);
     if (dens)
-      coul_fwd_x_t<P1, P2, true, C><<<dim3(nrow, N, np), nthr, 0, c.stream>>>(src1, nullptr, ca);
+      coul_fwd_x_t<P1, P2, true, C><<<dim3(nrow, 1, np), nthr, 0, c.stream>>>(src1, nullptr, ca);
     else
-      coul_fwd_x_t<P1, P2, false, C><<<dim3(nrow, N, np), nthr, 0, c.stream>>>(src1, src2, ca);
+      coul_fwd_x_t<P1, P2, false, C><<<dim3(nrow, 1, np), nthr, 0, c.stream>>>(src1, src2, ca);
     SG_LAUNCHED();
   }
   {
     ProfScope ps(c, ST_COUL_FWD_Y);
-    coul_fwd_y_t<P1, P2, C><<<dim3(ncol, N, np), nthr, 0, c.stream>>>(ca);
+    coul_fwd_y_t<P1, P2, C><<<dim3(ncol, 1, np), nthr, 0, c.stream>>>(ca);
     SG_LAUNCHED();
   }
   {
     ProfScope ps(c, ST_COUL_Z);
-    coul_z_t<P1, P2, C><<<dim3(ncol, P, np), nthr, 0, c.stream>>>(ca);
+    coul_z_t<P1, P2, C><<<dim3(nzc, 1, np), nthr, 0, c.stream>>>(ca);
     SG_LAUNCHED();
   }
   {
     ProfScope ps(c, ST_COUL_INV_Y);
-    coul_inv_y_t<P1, P2, C><<<dim3(ncol, N, np), nthr, 0, c.stream>>>(ca);
+    coul_inv_y_t<P1, P2, C><<<dim3(ncol, 1, np), nthr, 0, c.stream>>>(ca);
     SG_LAUNCHED();
   }
   {
     ProfScope ps(c, ST_COUL_INV_X);
     if (dens)
-      coul_inv_x_t<P1, P2, true, C><<<dim3(nrow, N, np), nthr, 0, c.stream>>>(ca, Rpl, full, 0);
+      coul_inv_x_t<P1, P2, true, C><<<dim3(nrow, 1, np), nthr, 0, c.stream>>>(ca, Rpl, full, 0);
     else
-      coul_inv_x_t<P1, P2, false, C><<<dim3(nrow, N, np), nthr, 0, c.stream>>>(ca, Rpl, full, herm ? 1 : 0);
+      coul_inv_x_t<P1, P2, false, C><<<dim3(nrow, 1, np), nthr, 0, c.stream>>>(ca, Rpl, full, herm ? 1 : 0);
     SG_LAUNCHED();
   }
   return SINCGPU_OK;
