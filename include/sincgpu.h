@@ -76,6 +76,11 @@ int sincgpu_fft_length(sincgpu_ctx* ctx);
 int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
 
 int sincgpu_synchronize(sincgpu_ctx* ctx);
+/* How host threads wait for the device (process-wide, per device): 0 = CUDA's
+ * default heuristic, 1 = spin, 2 = yield, 3 = block on an OS primitive.  Blocking
+ * keeps many host threads that each wait on their own stream (the request loop's
+ * workers) from burning the host's cores while they wait. */
+int sincgpu_set_sync_mode(int device, int mode);
 
 /* Makes the context enqueue on a caller-owned cudaStream_t (passed as void*).
  * The caller keeps the stream alive for the life of the context. */
@@ -490,6 +495,11 @@ int sincgpu_server_wait(sincgpu_server* server, int id, double* energy0, double*
  * A-vector when it was submitted with keep_state.  Any pointer may be NULL. */
 int sincgpu_server_result_arrays(sincgpu_server* server, int id, double* step_ms, double* energies, double* phi,
                                  double* avector);
+/* Timeline of a finished request in ms since the server was created: times[0] =
+ * submitted, times[1] = admitted to a slot, times[2] = context and CMF state ready
+ * (set-up done), times[3] = finished; step_start[k] = start of CMF step k.  Any
+ * pointer may be NULL. */
+int sincgpu_server_timeline(sincgpu_server* server, int id, double* times, double* step_start);
 /* counts[0..4] = admitted, completed, steps, peak concurrent requests, pending;
  * p50 / p99 of all finished steps' latencies (ms); steps per second between the
  * first admission and the last completion. */

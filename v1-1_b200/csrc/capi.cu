@@ -24,11 +24,18 @@ void set_error(const char* fmt, ...) {
 
 int Workspace::ensure(size_t need) {
   if (need <= bytes) return SINCGPU_OK;
-  if (ptr) cudaFree(ptr);
-  ptr = nullptr;
-  bytes = 0;
+  if (owner) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(*owner, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+      set_error("a workspace would grow to %zu bytes during graph capture (run the call once before capturing)",
+                need);
+      return SINCGPU_ESTATE;
+    }
+  }
+  release();
   size_t want = need + need / 8;
-  if (cudaMalloc(&ptr, want) != cudaSuccess) {
+  const cudaError_t e = owner ? cudaMallocAsync(&ptr, want, *owner) : cudaMalloc(&ptr, want);
+  if (e != cudaSuccess) {
     cudaGetLastError();
     ptr = nullptr;
     set_error("cudaMalloc of %zu bytes failed", want);
@@ -39,21 +46,54 @@ int Workspace::ensure(size_t need) {
 }
 
 void Workspace::release() {
-  if (ptr) cudaFree(ptr);
+  if (ptr) {
+    if (owner)
+      cudaFreeAsync(ptr, *owner);
+    else
+      cudaFree(ptr);
+  }
   ptr = nullptr;
   bytes = 0;
 }
 
+int dalloc(Ctx& c, void** p, size_t bytes) {
+  *p = nullptr;
+  if (cudaMallocAsync(p, std::max<size_t>(bytes, 16), c.stream) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    set_error("device allocation of %zu bytes failed", bytes);
+    return SINCGPU_ENOMEM;
+  }
+  return SINCGPU_OK;
+}
+
+void dfree(Ctx& c, void* p) {
+  if (p) cudaFreeAsync(p, c.stream);
+}
+
+int dupload(Ctx& c, void** dst, const void* src, size_t bytes) {
+  dfree(c, *dst);
+  *dst = nullptr;
+  if (bytes == 0) return SINCGPU_OK;
+  SG_TRY(dalloc(c, dst, bytes));
+  SG_CUDA(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, c.stream));
+  return SINCGPU_OK;
+}
+
+void Ctx::bind_workspaces() {
+  for (Workspace* w : {&ws_fft, &ws_pairs, &ws_gemm, &ws_rhs, &ws_io, &ws_red, &ws_conv, &ws_state, &ws_ci,
+                       &ws_ci2, &ws_kry, &ws_orb, &cmf.ws})
+    w->owner = &stream;
+}
+
 Ctx::~Ctx() {
-  cudaFree(d_kevect);
-  cudaFree(d_ketile);
-  cudaFree(d_pot);
-  cudaFree(d_zdip);
-  cudaFree(d_tcoul);
-  cudaFree(d_khat);
-  cudaFree(d_roots);
-  cudaFree(d_khat32);
-  cudaFree(d_roots32);
+  // stream-ordered frees below follow the context's own work; work that a batch
+  // graph ran on another stream is waited for here
+  if (stream) cudaStreamSynchronize(stream);
+  if (rhs_graph) cudaDeviceSynchronize();
+  for (void* p : {(void*)d_kevect, (void*)d_ketile, (void*)d_pot, (void*)d_zdip, (void*)d_tcoul, (void*)d_khat,
+                  (void*)d_roots, (void*)d_khat32, (void*)d_roots32})
+    dfree(*this, p);
   ws_fft.release();
   ws_pairs.release();
   ws_gemm.release();
@@ -67,10 +107,10 @@ Ctx::~Ctx() {
   ws_kry.release();
   ws_orb.release();
   cmf.ws.release();
-  for (IntCache& ic : icache) cudaFree(ic.dev);
+  for (IntCache& ic : icache) dfree(*this, ic.dev);
   if (rhs_exec) cudaGraphExecDestroy(rhs_exec);
   if (rhs_graph) cudaGraphDestroy(rhs_graph);
-  ci.release();
+  ci.release(stream);
   if (stream && own_stream) cudaStreamDestroy(stream);
 }
 
@@ -81,10 +121,10 @@ int cached_ints(Ctx& c, int slot, const int* h, size_t n, const int** d) {
     return SINCGPU_OK;
   }
   if (n > ic.cap) {
-    cudaFree(ic.dev);
+    dfree(c, ic.dev);
     ic.dev = nullptr;
     ic.cap = 0;
-    SG_CUDA(cudaMalloc(&ic.dev, sizeof(int) * std::max<size_t>(n, 1)));
+    SG_TRY(dalloc(c, &ic.dev, sizeof(int) * std::max<size_t>(n, 1)));
     ic.cap = n;
   }
   ic.host.assign(h, h + n);
@@ -170,6 +210,14 @@ static int ctx_common(sincgpu_ctx* h, int numpoints, double spacing, int numspf,
   SG_CUDA(cudaSetDevice(device));
   SG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
   c.own_stream = true;
+  c.bind_workspaces();
+  // memory the contexts release stays cached in the device's stream-ordered pool
+  // for the next allocations instead of going back to the driver
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   return SINCGPU_OK;
 }
 
@@ -258,13 +306,22 @@ int sincgpu_synchronize(sincgpu_ctx* h) {
   return SINCGPU_OK;
 }
 
+int sincgpu_set_sync_mode(int device, int mode) {
+  static const unsigned flags[] = {cudaDeviceScheduleAuto, cudaDeviceScheduleSpin, cudaDeviceScheduleYield,
+                                   cudaDeviceScheduleBlockingSync};
+  SG_CHECK(mode >= 0 && mode <= 3, SINCGPU_EINVAL, "sync mode %d outside [0,3]", mode);
+  SG_CUDA(cudaSetDevice(device));
+  SG_CUDA(cudaSetDeviceFlags(flags[mode]));
+  return SINCGPU_OK;
+}
+
 int sincgpu_set_stream(sincgpu_ctx* h, void* stream) {
   CTX_CHECK(h);
   Ctx& c = h->c;
-  if (c.own_stream && c.stream) {
-    SG_CUDA(cudaStreamSynchronize(c.stream));
-    SG_CUDA(cudaStreamDestroy(c.stream));
-  }
+  // workspaces are stream-ordered on the context's stream: finish the old
+  // stream's work before later frees are ordered on the new one
+  if (c.stream) SG_CUDA(cudaStreamSynchronize(c.stream));
+  if (c.own_stream && c.stream) SG_CUDA(cudaStreamDestroy(c.stream));
   c.own_stream = false;
   c.stream = (cudaStream_t)stream;
   return SINCGPU_OK;

@@ -20,14 +20,7 @@ namespace sincgpu {
 // ---------------------------------------------------------------------------
 // host: per-element contribution lists and hop ranges, uploaded once
 // ---------------------------------------------------------------------------
-static int upload(void** dst, const void* src, size_t bytes) {
-  if (*dst) cudaFree(*dst);
-  *dst = nullptr;
-  if (bytes == 0) return SINCGPU_OK;
-  SG_CUDA(cudaMalloc(dst, bytes));
-  SG_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
-  return SINCGPU_OK;
-}
+
 
 int ci_attach(Ctx& c, const Walks& w) {
   SG_CHECK(w.nspf == c.nspf, SINCGPU_EINVAL, "walk tables for %d orbitals, context has %d", w.nspf, c.nspf);
@@ -50,8 +43,8 @@ int ci_attach(Ctx& c, const Walks& w) {
         size_t e = (w.singlewalkopspf[2 * k] - 1) + (size_t)n * (w.singlewalkopspf[2 * k + 1] - 1);
         ent[pos[e]++] = make_int2(c1, w.singlewalkdirphase[k] > 0 ? w.singlewalk[k] - 1 : -w.singlewalk[k]);
       }
-    SG_TRY(upload((void**)&s.den_off, off.data(), sizeof(long long) * off.size()));
-    SG_TRY(upload((void**)&s.den_ent, ent.data(), sizeof(int2) * ent.size()));
+    SG_TRY(dupload(c, (void**)&s.den_off, off.data(), sizeof(long long) * off.size()));
+    SG_TRY(dupload(c, (void**)&s.den_ent, ent.data(), sizeof(int2) * ent.size()));
   }
   // 2-RDM lists: each double walk feeds (d1,d2,d3,d4) and (d3,d4,d1,d2)
   {
@@ -79,8 +72,8 @@ int ci_attach(Ctx& c, const Walks& w) {
         ent[pos[e1(k)]++] = v;
         ent[pos[e2(k)]++] = v;
       }
-    SG_TRY(upload((void**)&s.tal_off, off.data(), sizeof(long long) * off.size()));
-    SG_TRY(upload((void**)&s.tal_ent, ent.data(), sizeof(int2) * ent.size()));
+    SG_TRY(dupload(c, (void**)&s.tal_off, off.data(), sizeof(long long) * off.size()));
+    SG_TRY(dupload(c, (void**)&s.tal_ent, ent.data(), sizeof(int2) * ent.size()));
   }
   // walks (compact) and hop ranges for assembly and sigma
   {
@@ -95,8 +88,8 @@ int ci_attach(Ctx& c, const Walks& w) {
       int e = (d[0] - 1) + n * ((d[1] - 1) + n * ((d[2] - 1) + n * (d[3] - 1)));
       didx[k] = w.doublewalkdirphase[k] > 0 ? e : -(e + 1);
     }
-    SG_TRY(upload((void**)&s.sidx, sidx.data(), sizeof(int) * ns));
-    SG_TRY(upload((void**)&s.didx, didx.data(), sizeof(int) * nd));
+    SG_TRY(dupload(c, (void**)&s.sidx, sidx.data(), sizeof(int) * ns));
+    SG_TRY(dupload(c, (void**)&s.didx, didx.data(), sizeof(int) * nd));
     std::vector<long long> swb(s.nsh), dwb(s.ndh);
     std::vector<int> swn(s.nsh), dwn(s.ndh), shop(s.nsh), dhop(s.ndh);
     for (int c1 = 0; c1 < nc; ++c1) {
@@ -111,21 +104,21 @@ int ci_attach(Ctx& c, const Walks& w) {
         dhop[h] = w.doublehop[h] - 1;
       }
     }
-    SG_TRY(upload((void**)&s.swb, swb.data(), sizeof(long long) * s.nsh));
-    SG_TRY(upload((void**)&s.dwb, dwb.data(), sizeof(long long) * s.ndh));
-    SG_TRY(upload((void**)&s.swn, swn.data(), sizeof(int) * s.nsh));
-    SG_TRY(upload((void**)&s.dwn, dwn.data(), sizeof(int) * s.ndh));
-    SG_TRY(upload((void**)&s.shop, shop.data(), sizeof(int) * s.nsh));
-    SG_TRY(upload((void**)&s.dhop, dhop.data(), sizeof(int) * s.ndh));
-    SG_TRY(upload((void**)&s.shop_off, w.singlehop_off.data(), sizeof(long long) * (nc + 1)));
-    SG_TRY(upload((void**)&s.dhop_off, w.doublehop_off.data(), sizeof(long long) * (nc + 1)));
-    if (s.xpot) cudaFree(s.xpot);
-    if (s.xone) cudaFree(s.xone);
-    if (s.xz) cudaFree(s.xz);
+    SG_TRY(dupload(c, (void**)&s.swb, swb.data(), sizeof(long long) * s.nsh));
+    SG_TRY(dupload(c, (void**)&s.dwb, dwb.data(), sizeof(long long) * s.ndh));
+    SG_TRY(dupload(c, (void**)&s.swn, swn.data(), sizeof(int) * s.nsh));
+    SG_TRY(dupload(c, (void**)&s.dwn, dwn.data(), sizeof(int) * s.ndh));
+    SG_TRY(dupload(c, (void**)&s.shop, shop.data(), sizeof(int) * s.nsh));
+    SG_TRY(dupload(c, (void**)&s.dhop, dhop.data(), sizeof(int) * s.ndh));
+    SG_TRY(dupload(c, (void**)&s.shop_off, w.singlehop_off.data(), sizeof(long long) * (nc + 1)));
+    SG_TRY(dupload(c, (void**)&s.dhop_off, w.doublehop_off.data(), sizeof(long long) * (nc + 1)));
+    dfree(c, s.xpot);
+    dfree(c, s.xone);
+    dfree(c, s.xz);
     s.xpot = s.xone = s.xz = nullptr;
-    SG_CUDA(cudaMalloc(&s.xpot, sizeof(double2) * std::max(1LL, s.ndh)));
-    SG_CUDA(cudaMalloc(&s.xone, sizeof(double2) * std::max(1LL, s.nsh)));
-    SG_CUDA(cudaMalloc(&s.xz, sizeof(double2) * std::max(1LL, s.nsh)));
+    SG_TRY(dalloc(c, &s.xpot, sizeof(double2) * std::max(1LL, s.ndh)));
+    SG_TRY(dalloc(c, &s.xone, sizeof(double2) * std::max(1LL, s.nsh)));
+    SG_TRY(dalloc(c, &s.xz, sizeof(double2) * std::max(1LL, s.nsh)));
   }
   // spin sets and projectors (allspinproject=1), when built
   s.spin = false;
@@ -139,14 +132,16 @@ int ci_attach(Ctx& c, const Walks& w) {
     s.maxspinset = w.maxspinsetsize;
     SG_CHECK(s.maxspinset <= 4096, SINCGPU_ERANGE, "spin set of %d configurations exceeds 4096",
              s.maxspinset);
-    SG_TRY(upload((void**)&s.sp_set_off, w.spinset_off.data(), sizeof(long long) * w.spinset_off.size()));
+    SG_TRY(dupload(c, (void**)&s.sp_set_off, w.spinset_off.data(), sizeof(long long) * w.spinset_off.size()));
     // empty tables stay null (upload of 0 bytes); the kernel touches only non-empty ones
-    SG_TRY(upload((void**)&s.sp_sets, sets0.data(), sizeof(int) * sets0.size()));
-    SG_TRY(upload((void**)&s.sp_proj_off, w.spinproj_off.data(), sizeof(long long) * w.spinproj_off.size()));
-    SG_TRY(upload((void**)&s.sp_proj, w.spinproj.data(), sizeof(double) * w.spinproj.size()));
-    SG_TRY(upload((void**)&s.sp_elim, elim0.data(), sizeof(int) * elim0.size()));
+    SG_TRY(dupload(c, (void**)&s.sp_sets, sets0.data(), sizeof(int) * sets0.size()));
+    SG_TRY(dupload(c, (void**)&s.sp_proj_off, w.spinproj_off.data(), sizeof(long long) * w.spinproj_off.size()));
+    SG_TRY(dupload(c, (void**)&s.sp_proj, w.spinproj.data(), sizeof(double) * w.spinproj.size()));
+    SG_TRY(dupload(c, (void**)&s.sp_elim, elim0.data(), sizeof(int) * elim0.size()));
     s.spin = true;
   }
+  // the tables are complete before any other stream (a batch graph) reads them
+  SG_CUDA(cudaStreamSynchronize(c.stream));
   s.attached = true;
   s.assembled = false;
   return SINCGPU_OK;
@@ -201,11 +196,12 @@ int ci_spin_project(Ctx& c, double2* a) {
   return SINCGPU_OK;
 }
 
-void CIState::release() {
+void CIState::release(cudaStream_t stream) {
   void* ptrs[] = {den_off, den_ent, tal_off, tal_ent, sidx, didx, swb, dwb, swn, dwn,
                   shop, dhop, shop_off, dhop_off, xpot, xone, xz,
                   sp_set_off, sp_sets, sp_proj_off, sp_proj, sp_elim};
-  for (void* p : ptrs) cudaFree(p);
+  for (void* p : ptrs)
+    if (p) cudaFreeAsync(p, stream);
   *this = CIState();
 }
 

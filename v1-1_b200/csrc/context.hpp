@@ -8,10 +8,16 @@
 
 namespace sincgpu {
 
+// Device scratch that grows on demand.  With an owner stream (every context
+// workspace) the memory is stream-ordered (cudaMallocAsync / cudaFreeAsync on the
+// context's stream): growing it neither synchronises the device nor stalls the
+// other contexts' streams, which a plain cudaFree would.  Growth is refused while
+// the owner stream is being captured into a graph.
 struct Workspace {
   void* ptr = nullptr;
   size_t bytes = 0;
-  int ensure(size_t need);  // grows (cudaMalloc) when needed
+  cudaStream_t* owner = nullptr;
+  int ensure(size_t need);
   void release();
 };
 
@@ -50,7 +56,7 @@ struct CIState {
   int *sp_sets = nullptr, *sp_elim = nullptr;
   double* sp_proj = nullptr;
   long long numspinconfig = 0;              // spin-adapted dimension
-  void release();
+  void release(cudaStream_t stream);  // stream-ordered frees
 };
 
 // Host integer tables (pair lists, lookup tables) kept on the device and
@@ -170,7 +176,21 @@ struct Ctx {
   Prof prof;
 
   ~Ctx();
+  void bind_workspaces();  // makes every workspace stream-ordered on `stream`
 };
+
+// Stream-ordered device memory on the context's stream (cudaMallocAsync /
+// cudaFreeAsync): allocating and freeing the context's tables neither
+// synchronises the device nor stalls other contexts' streams.
+int dalloc(Ctx& c, void** p, size_t bytes);
+template <class T>
+int dalloc(Ctx& c, T** p, size_t bytes) {
+  return dalloc(c, reinterpret_cast<void**>(p), bytes);
+}
+void dfree(Ctx& c, void* p);
+// (Re)allocates *dst and copies `bytes` from host memory on the context stream
+// (the host buffer may be released on return).
+int dupload(Ctx& c, void** dst, const void* src, size_t bytes);
 
 // Brackets one kernel launch with events on the context stream when profiling.
 struct ProfScope {

@@ -50,7 +50,8 @@ struct Res {
   int status = SINCGPU_OK;
   char err[256] = "";
   double energy0 = 0.0, energy = 0.0, norm = 0.0, dipole = 0.0, wait_ms = 0.0;
-  std::vector<double> step_ms, energies;
+  double t_submit = 0.0, t_admit = 0.0, t_ready = 0.0, t_end = 0.0;  // ms since server creation
+  std::vector<double> step_ms, energies, step_start;
   std::vector<double> phi, avec;
   bool done = false;
 };
@@ -100,6 +101,7 @@ struct sincgpu_server {
   std::vector<std::thread> workers;
   bool stop = false;
   int next_id = 1;
+  double t0 = 0.0;  // creation time (now_ms)
   long long admitted = 0, completed = 0;
   double t_first = -1.0, t_last = 0.0;
 
@@ -129,9 +131,11 @@ void sincgpu_server::run(Req& r, Res& out) {
     rc = sincgpu_cmf_setup(ctx, r.dt, 1, 1e-8, 1e-9, 30, 100, 10, 100, 1.2, 1e-10, 0.0, -1.0);
   if (rc == SINCGPU_OK)
     rc = sincgpu_cmf_pulses(ctx, (int)r.ptype.size(), r.ptype.data(), r.pparams.data());
+  // the request's state buffers are stream-ordered on its context's stream, so
+  // neither their allocation nor their release synchronises the other requests
   if (rc == SINCGPU_OK) {
-    if (cudaMalloc(&dphi, sizeof(double) * 2 * G * r.nspf) != cudaSuccess ||
-        cudaMalloc(&davec, sizeof(double) * 2 * nc) != cudaSuccess) {
+    if (dalloc(ctx->c, &dphi, sizeof(double) * 2 * G * r.nspf) != SINCGPU_OK ||
+        dalloc(ctx->c, &davec, sizeof(double) * 2 * nc) != SINCGPU_OK) {
       set_error("out of device memory for the initial state");
       rc = SINCGPU_ENOMEM;
     }
@@ -145,12 +149,15 @@ void sincgpu_server::run(Req& r, Res& out) {
     rc = SINCGPU_EINVAL;
   }
   if (rc == SINCGPU_OK) {
-    cudaMemcpy(dphi, r.phi.data(), sizeof(double) * r.phi.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(davec, r.avec.data(), sizeof(double) * r.avec.size(), cudaMemcpyHostToDevice);
+    cudaMemcpyAsync(dphi, r.phi.data(), sizeof(double) * r.phi.size(), cudaMemcpyHostToDevice, ctx->c.stream);
+    cudaMemcpyAsync(davec, r.avec.data(), sizeof(double) * r.avec.size(), cudaMemcpyHostToDevice,
+                    ctx->c.stream);
     rc = sincgpu_cmf_init_dev(ctx, dphi, davec, &out.energy0);
   }
+  out.t_ready = now_ms() - this->t0;
   for (int k = 0; rc == SINCGPU_OK && k < r.nsteps; ++k) {
     const double t0 = now_ms();
+    out.step_start.push_back(t0 - this->t0);
     double e = 0.0, nn = 0.0;
     rc = sincgpu_cmf_step(ctx, r.dt * k, r.dt * (k + 1), &e, &nn, nullptr, nullptr);
     out.step_ms.push_back(now_ms() - t0);
@@ -168,13 +175,18 @@ void sincgpu_server::run(Req& r, Res& out) {
     out.avec.resize(2 * (size_t)nc);
     rc = sincgpu_cmf_state_dev(ctx, dphi, davec);
     if (rc == SINCGPU_OK) {
-      cudaMemcpy(out.phi.data(), dphi, sizeof(double) * out.phi.size(), cudaMemcpyDeviceToHost);
-      cudaMemcpy(out.avec.data(), davec, sizeof(double) * out.avec.size(), cudaMemcpyDeviceToHost);
+      cudaMemcpyAsync(out.phi.data(), dphi, sizeof(double) * out.phi.size(), cudaMemcpyDeviceToHost,
+                      ctx->c.stream);
+      cudaMemcpyAsync(out.avec.data(), davec, sizeof(double) * out.avec.size(), cudaMemcpyDeviceToHost,
+                      ctx->c.stream);
+      cudaStreamSynchronize(ctx->c.stream);
     }
   }
   if (rc != SINCGPU_OK) fail(rc);
-  cudaFree(dphi);
-  cudaFree(davec);
+  if (ctx) {
+    dfree(ctx->c, dphi);
+    dfree(ctx->c, davec);
+  }
   if (walks) sincgpu_walks_destroy(walks);
   if (ctx) sincgpu_destroy(ctx);
 }
@@ -208,7 +220,10 @@ void sincgpu_server::worker() {
     }
     auto out = std::make_unique<Res>();
     out->wait_ms = now_ms() - r->t_submit;
+    out->t_submit = r->t_submit - t0;
+    out->t_admit = now_ms() - t0;
     run(*r, *out);
+    out->t_end = now_ms() - t0;
     {
       std::lock_guard<std::mutex> lk(mu);
       reserved -= r->est;
@@ -233,12 +248,19 @@ int sincgpu_server_create(sincgpu_server** out, int device, long long hbm_budget
   using namespace sincgpu;
   SG_CHECK(out && max_active >= 1 && max_active <= 64, SINCGPU_EINVAL, "bad argument");
   SG_CUDA(cudaSetDevice(device));
+  // memory cached in the stream-ordered pool by earlier contexts counts as free
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    SG_CUDA(cudaDeviceSynchronize());
+    cudaMemPoolTrimTo(pool, 0);
+  }
   size_t fr = 0, tot = 0;
   SG_CUDA(cudaMemGetInfo(&fr, &tot));
   auto s = std::make_unique<sincgpu_server>();
   s->device = device;
   s->budget = hbm_budget > 0 ? std::min<long long>(hbm_budget, (long long)fr) : (long long)(0.85 * fr);
   s->max_active = max_active;
+  s->t0 = now_ms();
   for (int i = 0; i < max_active; ++i) s->workers.emplace_back([p = s.get()] { p->worker(); });
   *out = s.release();
   return SINCGPU_OK;
@@ -322,6 +344,22 @@ int sincgpu_server_result_arrays(sincgpu_server* s, int id, double* step_ms, dou
     SG_CHECK(!r.avec.empty(), SINCGPU_ESTATE, "request %d kept no state", id);
     std::copy(r.avec.begin(), r.avec.end(), avector);
   }
+  return SINCGPU_OK;
+}
+
+int sincgpu_server_timeline(sincgpu_server* s, int id, double* times, double* step_start) {
+  using namespace sincgpu;
+  SG_CHECK(s, SINCGPU_EINVAL, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  SG_CHECK(s->res.count(id) && s->res[id]->done, SINCGPU_ESTATE, "request %d not finished", id);
+  const Res& r = *s->res[id];
+  if (times) {
+    times[0] = r.t_submit;
+    times[1] = r.t_admit;
+    times[2] = r.t_ready;
+    times[3] = r.t_end;
+  }
+  if (step_start) std::copy(r.step_start.begin(), r.step_start.end(), step_start);
   return SINCGPU_OK;
 }
 

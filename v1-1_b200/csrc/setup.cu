@@ -59,9 +59,7 @@ int choose_plan(Ctx& c) {
     long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)P;
     roots[m] = make_double2((double)cosl(ang), (double)sinl(ang));
   }
-  if (c.d_roots) cudaFree(c.d_roots);
-  SG_CUDA(cudaMalloc(&c.d_roots, sizeof(double2) * P));
-  SG_CUDA(cudaMemcpy(c.d_roots, roots.data(), sizeof(double2) * P, cudaMemcpyHostToDevice));
+  SG_TRY(dupload(c, (void**)&c.d_roots, roots.data(), sizeof(double2) * P));
   return SINCGPU_OK;
 }
 
@@ -91,12 +89,8 @@ static int build_kinetic(Ctx& c) {
   std::vector<double> tile((size_t)S * S, 0.0);
   for (int j = 0; j < N; ++j)
     for (int l = 0; l < N; ++l) tile[(size_t)j * S + l] = ke[(j - l) + N - 1];
-  if (c.d_kevect) cudaFree(c.d_kevect);
-  if (c.d_ketile) cudaFree(c.d_ketile);
-  SG_CUDA(cudaMalloc(&c.d_kevect, sizeof(double) * ke.size()));
-  SG_CUDA(cudaMalloc(&c.d_ketile, sizeof(double) * tile.size()));
-  SG_CUDA(cudaMemcpy(c.d_kevect, ke.data(), sizeof(double) * ke.size(), cudaMemcpyHostToDevice));
-  SG_CUDA(cudaMemcpy(c.d_ketile, tile.data(), sizeof(double) * tile.size(), cudaMemcpyHostToDevice));
+  SG_TRY(dupload(c, (void**)&c.d_kevect, ke.data(), sizeof(double) * ke.size()));
+  SG_TRY(dupload(c, (void**)&c.d_ketile, tile.data(), sizeof(double) * tile.size()));
   return SINCGPU_OK;
 }
 
@@ -254,45 +248,42 @@ static int build_tcoul(Ctx& c, int nbig, int ns) {
          *d_E = nullptr;
   int rc = SINCGPU_OK;
   auto cleanup = [&]() {
-    cudaFree(d_alltt); cudaFree(d_x); cudaFree(d_y); cudaFree(d_V); cudaFree(d_VT); cudaFree(d_E);
+    for (double* p : {d_alltt, d_x, d_y, d_V, d_VT, d_E}) dfree(c, p);
   };
   do {
-    if (cudaMalloc(&d_alltt, sizeof(double) * alltt.size()) != cudaSuccess ||
-        cudaMalloc(&d_x, sizeof(double) * ncube) != cudaSuccess ||
-        cudaMalloc(&d_y, sizeof(double) * ncube) != cudaSuccess ||
-        cudaMalloc(&d_V, sizeof(double) * NS * NS) != cudaSuccess ||
-        cudaMalloc(&d_VT, sizeof(double) * NS * NS) != cudaSuccess ||
-        cudaMalloc(&d_E, sizeof(double) * NS) != cudaSuccess) {
-      set_error("cudaMalloc failed in getinverse");
+    if (dupload(c, (void**)&d_alltt, alltt.data(), sizeof(double) * alltt.size()) != SINCGPU_OK ||
+        dalloc(c, &d_x, sizeof(double) * ncube) != SINCGPU_OK ||
+        dalloc(c, &d_y, sizeof(double) * ncube) != SINCGPU_OK ||
+        dupload(c, (void**)&d_V, V.data(), sizeof(double) * NS * NS) != SINCGPU_OK ||
+        dupload(c, (void**)&d_VT, VT.data(), sizeof(double) * NS * NS) != SINCGPU_OK ||
+        dupload(c, (void**)&d_E, E.data(), sizeof(double) * NS) != SINCGPU_OK) {
+      set_error("device allocation failed in getinverse");
       rc = SINCGPU_ENOMEM;
       break;
     }
-    cudaMemcpy(d_alltt, alltt.data(), sizeof(double) * alltt.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(d_V, V.data(), sizeof(double) * NS * NS, cudaMemcpyHostToDevice);
-    cudaMemcpy(d_VT, VT.data(), sizeof(double) * NS * NS, cudaMemcpyHostToDevice);
-    cudaMemcpy(d_E, E.data(), sizeof(double) * NS, cudaMemcpyHostToDevice);
     const int tb = 256;
     const int gb = ceil_div(ncube, tb);
-    tr_kernel<<<gb, tb>>>(d_x, d_alltt, ns, nbig, delta, d3);
+    cudaStream_t st = c.stream;
+    tr_kernel<<<gb, tb, 0, st>>>(d_x, d_alltt, ns, nbig, delta, d3);
     // QQ = TOOTHEIGMULT(TR, W^T): axis 3, 2, 1
-    mode_mult_kernel<<<gb, tb>>>(d_x, d_y, d_VT, NS, 2);
-    mode_mult_kernel<<<gb, tb>>>(d_y, d_x, d_VT, NS, 1);
-    mode_mult_kernel<<<gb, tb>>>(d_x, d_y, d_VT, NS, 0);
-    divide_eigs_kernel<<<gb, tb>>>(d_y, d_E, NS);
-    mode_mult_kernel<<<gb, tb>>>(d_y, d_x, d_V, NS, 2);
-    mode_mult_kernel<<<gb, tb>>>(d_x, d_y, d_V, NS, 1);
-    mode_mult_kernel<<<gb, tb>>>(d_y, d_x, d_V, NS, 0);  // Q in d_x
+    mode_mult_kernel<<<gb, tb, 0, st>>>(d_x, d_y, d_VT, NS, 2);
+    mode_mult_kernel<<<gb, tb, 0, st>>>(d_y, d_x, d_VT, NS, 1);
+    mode_mult_kernel<<<gb, tb, 0, st>>>(d_x, d_y, d_VT, NS, 0);
+    divide_eigs_kernel<<<gb, tb, 0, st>>>(d_y, d_E, NS);
+    mode_mult_kernel<<<gb, tb, 0, st>>>(d_y, d_x, d_V, NS, 2);
+    mode_mult_kernel<<<gb, tb, 0, st>>>(d_x, d_y, d_V, NS, 1);
+    mode_mult_kernel<<<gb, tb, 0, st>>>(d_y, d_x, d_V, NS, 0);  // Q in d_x
     const int W = 2 * N - 1;
     const long long nw = (long long)W * W * W;
-    if (c.d_tcoul) cudaFree(c.d_tcoul);
+    dfree(c, c.d_tcoul);
     c.d_tcoul = nullptr;
-    if (cudaMalloc(&c.d_tcoul, sizeof(double) * nw) != cudaSuccess) {
-      set_error("cudaMalloc failed for the Coulomb table");
+    if (dalloc(c, &c.d_tcoul, sizeof(double) * nw) != SINCGPU_OK) {
+      set_error("device allocation failed for the Coulomb table");
       rc = SINCGPU_ENOMEM;
       break;
     }
-    assemble_t_kernel<<<ceil_div(nw, tb), tb>>>(c.d_tcoul, d_x, N, ns, delta, d3);
-    cudaError_t e = cudaDeviceSynchronize();
+    assemble_t_kernel<<<ceil_div(nw, tb), tb, 0, st>>>(c.d_tcoul, d_x, N, ns, delta, d3);
+    cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
       set_error("getinverse kernels: %s", cudaGetErrorString(e));
       rc = SINCGPU_ECUDA;
@@ -366,16 +357,16 @@ static int build_pot(Ctx& c, int sqrt32) {
   double mid = (pts[0] + pts[N - 1]) / 2.0;
   for (int i = 0; i < N; ++i) pts[i] -= mid;
   double* d_pts = nullptr;
-  SG_CUDA(cudaMalloc(&d_pts, sizeof(double) * N));
-  cudaMemcpy(d_pts, pts.data(), sizeof(double) * N, cudaMemcpyHostToDevice);
-  if (c.d_pot) cudaFree(c.d_pot);
-  if (c.d_zdip) cudaFree(c.d_zdip);
-  SG_CUDA(cudaMalloc(&c.d_pot, sizeof(double) * c.G));
-  SG_CUDA(cudaMalloc(&c.d_zdip, sizeof(double) * c.G));
-  pot_kernel<<<ceil_div(c.G, 256), 256>>>(c.d_pot, c.d_tcoul, cen, N, c.spacing, sqrt32);
-  zdip_kernel<<<ceil_div(c.G, 256), 256>>>(c.d_zdip, d_pts, N);
-  cudaError_t e = cudaDeviceSynchronize();
-  cudaFree(d_pts);
+  SG_TRY(dupload(c, (void**)&d_pts, pts.data(), sizeof(double) * N));
+  dfree(c, c.d_pot);
+  dfree(c, c.d_zdip);
+  c.d_pot = c.d_zdip = nullptr;
+  SG_TRY(dalloc(c, &c.d_pot, sizeof(double) * c.G));
+  SG_TRY(dalloc(c, &c.d_zdip, sizeof(double) * c.G));
+  pot_kernel<<<ceil_div(c.G, 256), 256, 0, c.stream>>>(c.d_pot, c.d_tcoul, cen, N, c.spacing, sqrt32);
+  zdip_kernel<<<ceil_div(c.G, 256), 256, 0, c.stream>>>(c.d_zdip, d_pts, N);
+  dfree(c, d_pts);
+  cudaError_t e = cudaStreamSynchronize(c.stream);
   SG_CHECK(e == cudaSuccess, SINCGPU_ECUDA, "potential kernels: %s", cudaGetErrorString(e));
   // nuclear repulsion (sinc_extraproject.f90:290-300)
   double nr = 0.0;
@@ -463,13 +454,14 @@ __global__ void fft_full_axis_kernel(double2* __restrict__ data, FftPlan plan,
 int make_khat(Ctx& c) {
   const int P = c.P;
   const long long P3 = (long long)P * P * P;
-  if (c.d_khat) cudaFree(c.d_khat);
-  cudaFree(c.d_khat32);  // FP32 copies follow the FP64 tables
-  cudaFree(c.d_roots32);
+  dfree(c, c.d_khat);
+  dfree(c, c.d_khat32);  // FP32 copies follow the FP64 tables
+  dfree(c, c.d_roots32);
+  c.d_khat = nullptr;
   c.d_khat32 = nullptr;
   c.d_roots32 = nullptr;
-  SG_CUDA(cudaMalloc(&c.d_khat, sizeof(double2) * P3));
-  embed_kernel<<<ceil_div(P3, 256), 256>>>(c.d_khat, c.d_tcoul, c.N, P);
+  SG_TRY(dalloc(c, &c.d_khat, sizeof(double2) * P3));
+  embed_kernel<<<ceil_div(P3, 256), 256, 0, c.stream>>>(c.d_khat, c.d_tcoul, c.N, P);
   SG_LAUNCHED();
   size_t sm0 = sizeof(double2) * (P + 2 * 8 * (P + 1));
   size_t sm1 = sizeof(double2) * (P + 2 * P * c.tx);
@@ -479,15 +471,16 @@ int make_khat(Ctx& c) {
   constexpr int kSmemOptIn = 227 * 1024;
   SG_CHECK(smax <= (size_t)kSmemOptIn, SINCGPU_ERANGE, "kernel-spectrum FFT needs %zu bytes of shared memory", smax);
   SG_CUDA(cudaFuncSetAttribute(fft_full_axis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemOptIn));
-  fft_full_axis_kernel<<<ceil_div((long long)P * P, 8), 128, sm0>>>(c.d_khat, c.plan, c.d_roots, 0, c.tx, 1.0);
+  fft_full_axis_kernel<<<ceil_div((long long)P * P, 8), 128, sm0, c.stream>>>(c.d_khat, c.plan, c.d_roots, 0,
+                                                                              c.tx, 1.0);
   SG_LAUNCHED();
   dim3 g1(ceil_div(P, c.tx), P);
-  fft_full_axis_kernel<<<g1, 128, sm1>>>(c.d_khat, c.plan, c.d_roots, 1, c.tx, 1.0);
+  fft_full_axis_kernel<<<g1, 128, sm1, c.stream>>>(c.d_khat, c.plan, c.d_roots, 1, c.tx, 1.0);
   SG_LAUNCHED();
   const double inv = 1.0 / ((double)P * (double)P * (double)P);
-  fft_full_axis_kernel<<<g1, 128, sm1>>>(c.d_khat, c.plan, c.d_roots, 2, c.tx, inv);
+  fft_full_axis_kernel<<<g1, 128, sm1, c.stream>>>(c.d_khat, c.plan, c.d_roots, 2, c.tx, inv);
   SG_LAUNCHED();
-  SG_CUDA(cudaDeviceSynchronize());
+  SG_CUDA(cudaStreamSynchronize(c.stream));
   return SINCGPU_OK;
 }
 
@@ -501,13 +494,13 @@ int ensure_fp32_tables(Ctx& c) {
   if (c.d_khat32 && c.d_roots32) return SINCGPU_OK;  // no stream work once built (graph capture)
   const long long P3 = (long long)c.P * c.P * c.P;
   if (!c.d_khat32) {
-    SG_CUDA(cudaMalloc(&c.d_khat32, sizeof(float2) * P3));
+    SG_TRY(dalloc(c, &c.d_khat32, sizeof(float2) * P3));
     narrow_kernel<<<std::min<long long>(ceil_div(P3, 256), 148 * 16), 256, 0, c.stream>>>(c.d_khat32,
                                                                                         c.d_khat, P3);
     SG_LAUNCHED();
   }
   if (!c.d_roots32) {
-    SG_CUDA(cudaMalloc(&c.d_roots32, sizeof(float2) * c.P));
+    SG_TRY(dalloc(c, &c.d_roots32, sizeof(float2) * c.P));
     narrow_kernel<<<1, 256, 0, c.stream>>>(c.d_roots32, c.d_roots, c.P);
     SG_LAUNCHED();
   }
@@ -523,7 +516,7 @@ int build_tables(Ctx& c, int toothnbig, int toothnsmall, int flags) {
   SG_TRY(build_pot(c, (flags & 1) ? 1 : 0));
   if (flags & 2) {  // notwoflag (sincproject.f90:330-332)
     const long long W = 2LL * c.N - 1;
-    SG_CUDA(cudaMemset(c.d_tcoul, 0, sizeof(double) * W * W * W));
+    SG_CUDA(cudaMemsetAsync(c.d_tcoul, 0, sizeof(double) * W * W * W, c.stream));
   }
   SG_TRY(make_khat(c));
   return SINCGPU_OK;
@@ -547,29 +540,27 @@ int build_tables_from_arrays(Ctx& c, const double2* threed_two_host, const doubl
   const long long M3 = 8LL * N * N * N;
   const long long W = 2LL * N - 1;
   double2* d_t2 = nullptr;
-  SG_CUDA(cudaMalloc(&d_t2, sizeof(double2) * M3));
-  cudaMemcpy(d_t2, threed_two_host, sizeof(double2) * M3, cudaMemcpyHostToDevice);
-  if (c.d_tcoul) cudaFree(c.d_tcoul);
-  SG_CUDA(cudaMalloc(&c.d_tcoul, sizeof(double) * W * W * W));
-  take_threed_kernel<<<ceil_div(W * W * W, 256), 256>>>(c.d_tcoul, d_t2, N);
-  cudaError_t e = cudaDeviceSynchronize();
-  cudaFree(d_t2);
+  SG_TRY(dupload(c, (void**)&d_t2, threed_two_host, sizeof(double2) * M3));
+  dfree(c, c.d_tcoul);
+  c.d_tcoul = nullptr;
+  SG_TRY(dalloc(c, &c.d_tcoul, sizeof(double) * W * W * W));
+  take_threed_kernel<<<ceil_div(W * W * W, 256), 256, 0, c.stream>>>(c.d_tcoul, d_t2, N);
+  dfree(c, d_t2);
+  cudaError_t e = cudaStreamSynchronize(c.stream);
   SG_CHECK(e == cudaSuccess, SINCGPU_ECUDA, "threed_two upload: %s", cudaGetErrorString(e));
-  if (c.d_pot) cudaFree(c.d_pot);
-  if (c.d_zdip) cudaFree(c.d_zdip);
-  SG_CUDA(cudaMalloc(&c.d_pot, sizeof(double) * c.G));
-  SG_CUDA(cudaMalloc(&c.d_zdip, sizeof(double) * c.G));
-  SG_CUDA(cudaMemcpy(c.d_pot, pot_host, sizeof(double) * c.G, cudaMemcpyHostToDevice));
+  dfree(c, c.d_zdip);
+  c.d_zdip = nullptr;
+  SG_TRY(dupload(c, (void**)&c.d_pot, pot_host, sizeof(double) * c.G));
+  SG_TRY(dalloc(c, &c.d_zdip, sizeof(double) * c.G));
   std::vector<double> pts(N);
   for (int i = 0; i < N; ++i) pts[i] = (i + 1) * c.spacing;
   double mid = (pts[0] + pts[N - 1]) / 2.0;
   for (int i = 0; i < N; ++i) pts[i] -= mid;
   double* d_pts = nullptr;
-  SG_CUDA(cudaMalloc(&d_pts, sizeof(double) * N));
-  cudaMemcpy(d_pts, pts.data(), sizeof(double) * N, cudaMemcpyHostToDevice);
-  zdip_kernel<<<ceil_div(c.G, 256), 256>>>(c.d_zdip, d_pts, N);
-  e = cudaDeviceSynchronize();
-  cudaFree(d_pts);
+  SG_TRY(dupload(c, (void**)&d_pts, pts.data(), sizeof(double) * N));
+  zdip_kernel<<<ceil_div(c.G, 256), 256, 0, c.stream>>>(c.d_zdip, d_pts, N);
+  dfree(c, d_pts);
+  e = cudaStreamSynchronize(c.stream);
   SG_CHECK(e == cudaSuccess, SINCGPU_ECUDA, "zdip: %s", cudaGetErrorString(e));
   SG_TRY(make_khat(c));
   return SINCGPU_OK;

@@ -103,11 +103,13 @@ _SIGS = {
     "sincgpu_batch_launch": ([_P, _P], _I),
     "sincgpu_batch_destroy": ([_P], _I),
     "sincgpu_autotune_rhs": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
+    "sincgpu_set_sync_mode": ([_I, _I], _I),
     "sincgpu_server_create": ([C.POINTER(_P), _I, _LL, _I], _I),
     "sincgpu_server_submit": ([_P, _P, _P], _I),
     "sincgpu_server_wait": ([_P, _I, _P, _P, _P, _P, _P], _I),
     "sincgpu_server_result_arrays": ([_P, _I, _P, _P, _P, _P], _I),
     "sincgpu_server_stats": ([_P, _P, _P, _P, _P], _I),
+    "sincgpu_server_timeline": ([_P, _I, _P, _P], _I),
     "sincgpu_server_destroy": ([_P], _I),
     "sincgpu_save_spfs": ([C.c_char_p, _P, _I, _P], _I),
     "sincgpu_load_spfs": ([C.c_char_p, _P, _P, _P, _LL], _I),

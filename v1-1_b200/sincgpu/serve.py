@@ -25,6 +25,7 @@ _SIGS = {
     "sincgpu_server_wait": ([_P, _I, _P, _P, _P, _P, _P], _I),
     "sincgpu_server_result_arrays": ([_P, _I, _P, _P, _P, _P], _I),
     "sincgpu_server_stats": ([_P, _P, _P, _P, _P], _I),
+    "sincgpu_server_timeline": ([_P, _I, _P, _P], _I),
     "sincgpu_server_destroy": ([_P], _I),
 }
 
@@ -76,9 +77,14 @@ class Server:
         av = np.zeros(nc, dtype=np.complex128) if keep else None
         _call("sincgpu_server_result_arrays", self._h, int(rid), steps.ctypes.data, energies.ctypes.data,
               None if phi is None else phi.ctypes.data, None if av is None else av.ctypes.data)
+        times = np.zeros(4)
+        starts = np.zeros(max(ns.value, 1))
+        _call("sincgpu_server_timeline", self._h, int(rid), times.ctypes.data, starts.ctypes.data)
         return {"energy0": e0.value, "energy": e.value, "norm": nn.value, "dipole_z": d.value,
                 "nsteps": ns.value, "step_ms": steps[:ns.value], "energies": energies[:ns.value],
-                "phi": phi, "avector": av}
+                "phi": phi, "avector": av,
+                "timeline_ms": dict(zip(("submitted", "admitted", "ready", "finished"), times.tolist())),
+                "step_start_ms": starts[:ns.value]}
 
     def stats(self) -> dict:
         cnt = np.zeros(5, dtype=np.int64)
