@@ -519,8 +519,14 @@ def served_form(local, fp32, count, nsteps):
         res = [srv.wait(i) for i in ids]
         wall = time.perf_counter() - t0
         st = srv.stats()
+    later = np.concatenate([r["step_ms"][1:] for r in res if len(r["step_ms"]) > 1])
+    setup = np.array([r["timeline_ms"]["ready"] - r["timeline_ms"]["admitted"] for r in res])
+    queued = np.array([r["timeline_ms"]["admitted"] - r["timeline_ms"]["submitted"] for r in res])
     return {"requests": count, "steps_per_request": nsteps, "dt_au": 0.05, "arrival_rate_per_s": 20.0,
             "p50_step_ms": st["p50_ms"], "p99_step_ms": st["p99_ms"], "steps_per_s": st["steps_per_s"],
+            "p99_step_ms_after_first_step": float(np.percentile(later, 99)) if later.size else None,
+            "setup_ms_p50": float(np.median(setup)), "setup_ms_max": float(setup.max()),
+            "queue_wait_ms_p50": float(np.median(queued)),
             "peak_concurrent": st["peak_active"], "completed": st["completed"], "wall_s": wall,
             "mean_request_s": float(np.mean([len(r["step_ms"]) and r["step_ms"].sum() / 1e3 for r in res])),
             "workload": "inputs.served_requests: odd 21^3-41^3 grids, 2-4 electrons, 4-8 orbitals, <= 1000 "
