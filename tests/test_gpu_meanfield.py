@@ -88,6 +88,25 @@ def test_call_twoe_matel00_general(he):
     assert relerr(mat, mat_ref) < TOL
 
 
+@pytest.mark.parametrize("nspf,general", [(12, False), (9, True)])
+def test_call_twoe_matel00_multitile(built_lib, nspf, general):
+    """Pair lists longer than one GEMM tile (2U = 156 hermitian, 2n^2 = 162 general):
+    only the upper-triangle tiles of the symmetric pair matrix are computed and the
+    lower ones mirrored."""
+    from sincgpu import SincProject
+    sysm = orc.SincSystem(21, 0.4, [[0, 0, 0]], [2.0])
+    gpu = SincProject(21, 0.4, [[0, 0, 0]], [2.0], nspf)
+    try:
+        phi = orc.seeded_orbitals(sysm, nspf, seed=21)
+        phi2 = orc.seeded_orbitals(sysm, nspf, seed=22) if general else phi
+        mat_ref, red_ref = sysm.call_twoe_matel00(phi, phi2)
+        mat, red = gpu.call_twoe_matel00(phi, phi2) if general else gpu.call_twoe_matel00(phi)
+        assert relerr(red, red_ref) < TOL
+        assert relerr(mat, mat_ref) < TOL
+    finally:
+        gpu.close()
+
+
 def test_mult_ke(he, h2):
     for sysm, gpu in ((he[0], he[1]), h2):
         rng = np.random.default_rng(5)

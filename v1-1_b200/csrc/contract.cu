@@ -268,7 +268,14 @@ __global__ void __launch_bounds__(256, 1) twoe_gemm3_kernel(const double2* __res
   auto f1 = [&](int st, int o, int k) -> double2& { return fsm[((st * 2 + 0) * nspf + o) * TK + k]; };
   auto f2 = [&](int st, int o, int k) -> double2& { return fsm[((st * 2 + 1) * nspf + o) * TK + k]; };
   const int M = 2 * npair;
-  const int tm = blockIdx.x / ntn, tn = blockIdx.x % ntn;
+  // upper-triangle tiles only (tm <= tn): C = A^T K A is symmetric, the lower
+  // tiles are mirrored in split_reduce_kernel
+  int tm = 0, rem = blockIdx.x;
+  while (rem >= ntn - tm) {
+    rem -= ntn - tm;
+    ++tm;
+  }
+  const int tn = tm + rem;
   const int m0 = tm * TT, n0 = tn * TT;
   const long long xb = blockIdx.y * xper;
   const long long xe = min(G, xb + xper);
@@ -363,13 +370,20 @@ __global__ void __launch_bounds__(256, 1) twoe_gemm3_kernel(const double2* __res
   }
 }
 
-// C[m][n] = sum_s part[s][m][n] in split order (deterministic)
-__global__ void split_reduce_kernel(const double* __restrict__ part, int nsplit, long long MM,
+// C[m][n] = sum_s part[s][m][n] in split order (deterministic); elements of the
+// lower-triangle tiles (tile(m) > tile(n), never computed) are read mirrored
+__global__ void split_reduce_kernel(const double* __restrict__ part, int nsplit, int M, int TT,
                                     double* __restrict__ C) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long MM = (long long)M * M;
   if (i >= MM) return;
+  long long src = i;
+  if (TT < M) {
+    const int m = (int)(i / M), n = (int)(i % M);
+    if (m / TT > n / TT) src = (long long)n * M + m;
+  }
   double s = 0.0;
-  for (int k = 0; k < nsplit; ++k) s += part[(long long)k * MM + i];
+  for (int k = 0; k < nsplit; ++k) s += part[(long long)k * MM + src];
   C[i] = s;
 }
 
@@ -426,15 +440,13 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
   SG_CHECK(n <= kMaxOrb, SINCGPU_ERANGE, "at most %d orbitals (got %d)", kMaxOrb, n);
   const int M = 2 * npair;
   // register block R: the smallest of 2..9 whose 16R tile holds M, else 8 (multi-tile)
-  int R = 8;
+  // tile edge 16R with the least padding of M (ties: the larger tile)
+  int R = 2;
   for (int r = 2; r <= 9; ++r)
-    if (16 * r >= M) {
-      R = r;
-      break;
-    }
+    if (ceil_div(M, 16 * r) * 16 * r <= ceil_div(M, 16 * R) * 16 * R) R = r;
   const int TT = 16 * R;
   const int ntm = ceil_div(M, TT), ntn = ntm;
-  const int ntiles = ntm * ntn;
+  const int ntiles = ntm * (ntm + 1) / 2;  // upper triangle
   long long target = 148;  // one 256-thread CTA per SM (R x R accumulators per thread)
   int nsplit = (int)std::max(1LL, std::min((long long)ceil_div(c.G, TK), std::max(1LL, target / ntiles)));
   long long xper = ((c.G + nsplit - 1) / nsplit + TK - 1) / TK * TK;
@@ -484,7 +496,7 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
     SG_LAUNCHED();
   }
   ProfScope ps(c, ST_TWOE_FINISH);
-  split_reduce_kernel<<<ceil_div(MM, 256), 256, 0, c.stream>>>(part, nsplit, MM, C);
+  split_reduce_kernel<<<ceil_div(MM, 256), 256, 0, c.stream>>>(part, nsplit, M, TT, C);
   SG_LAUNCHED();
   const long long n4 = (long long)n * n * n * n;
   twoe_assemble_kernel<<<ceil_div(n4, 256), 256, 0, c.stream>>>(C, d_lut, npair, n, herm ? 1 : 0,
