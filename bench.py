@@ -340,6 +340,7 @@ def precision_form(proj, torch, stream, flush, step, out, mat, steps, world, dis
     torch.cuda.synchronize()
     out64, mat64 = out.clone(), mat.clone()
     proj.set_option("coulomb_fp32", 1)
+    proj.set_option("contract_tf32", 1)
     try:
         for _ in range(3):
             step()
@@ -365,11 +366,14 @@ def precision_form(proj, torch, stream, flush, step, out, mat, steps, world, dis
         res = {"plain": {"coulomb": "fp64", "rhs_rel_err": 0.0},
                "mixed_fp32_coulomb": {
                    "value": world * steps / (total_ms / 1e3), "unit": UNIT,
-                   "ms_per_step": total_ms / steps, "coulomb": "fp32 (complex64 FFT passes, fp64 products "
-                                                               "and contractions)",
+                   "ms_per_step": total_ms / steps,
+                   "coulomb": "fp32 (complex64 FFT passes; pair products formed in fp64)",
+                   "contractions": "reducedpot on the tensor cores (tcgen05 kind::tf32, 3xTF32, fp32 "
+                                   "accumulation); twoematel fp64",
                    "rhs_rel_err_vs_fp64": rel(out, out64), "twoematel_rel_err_vs_fp64": rel(mat, mat64)}}
     finally:
         proj.set_option("coulomb_fp32", 0)
+        proj.set_option("contract_tf32", 0)
     return res
 
 
@@ -456,6 +460,7 @@ def batched_form(torch, local, stream, count):
     tuned = {}
     for p, _, b in made:
         p.set_option("coulomb_fp32", 1)
+        p.set_option("contract_tf32", 1)
         key = (p.N, p.nspf)
         if key in tuned:
             p.set_option("coul_chunk", tuned[key])
@@ -479,7 +484,8 @@ def batched_form(torch, local, stream, count):
         "batched_fp64_graph": {"value": count / (batched_plain_ms / 1e3), "unit": "evals/s",
                                "ms_per_round": batched_plain_ms},
         "batched_mixed_graph": {"value": count / (mixed_ms / 1e3), "unit": "evals/s", "ms_per_round": mixed_ms,
-                                "coulomb": "fp32 passes, fp64 products and contractions",
+                                "coulomb": "fp32 passes, fp64 pair products",
+                                "contractions": "reducedpot 3xTF32 on the tensor cores, twoematel fp64",
                                 "rhs_rel_err_max_vs_fp64": rhs_err,
                                 "two_electron_energy_dev_max_hartree": de},
         "mixed_batched_vs_plain_sequential": plain_ms / mixed_ms,

@@ -72,8 +72,18 @@ int sincgpu_get_tables(sincgpu_ctx* ctx, double* tempcoulomb, double* pot, doubl
 /* Padded FFT length P (>= 2N-1) used for the Toeplitz convolution. */
 int sincgpu_fft_length(sincgpu_ctx* ctx);
 
-/* Tuning knobs: "coul_chunk" (pairs per Coulomb pass sequence, 0 = auto). */
+/* Options: "coul_chunk" (pairs per Coulomb pass sequence, 0 = auto);
+ * "coulomb_fp32" (1: the Coulomb passes in FP32, the precision form);
+ * "contract_tf32" (1: the reducedpot contraction on the tensor cores as 3xTF32
+ * with FP32 accumulation, the precision form). */
 int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
+
+/* C(M x N, row-major) = A(M x K, row-major) * B(N x K, row-major)^T on the
+ * tensor cores (tcgen05 kind::tf32, 3xTF32 split, FP32 accumulation), device
+ * pointers.  The contraction kernel of the precision form, exposed for checks;
+ * *timed_out (may be NULL) is set when the kernel gave up waiting for its MMAs. */
+int sincgpu_gemm_tf32x3_dev(sincgpu_ctx* ctx, const double* A, const double* B, double* C, long long M, int N,
+                            int K, int* timed_out);
 
 int sincgpu_synchronize(sincgpu_ctx* ctx);
 /* How host threads wait for the device (process-wide, per device): 0 = CUDA's
@@ -479,7 +489,7 @@ typedef struct sincgpu_request {
   const double* pulseparams; /* 8 per pulse */
   int nsteps;
   double dt;
-  int coulomb_fp32;          /* precision form of the Coulomb passes */
+  int coulomb_fp32;          /* precision form: FP32 Coulomb passes and 3xTF32 tensor-core reducedpot */
   int keep_state;            /* keep the final orbitals and A-vector for sincgpu_server_result_arrays */
   const double* phi;
   const double* avector;

@@ -82,7 +82,7 @@ int dupload(Ctx& c, void** dst, const void* src, size_t bytes) {
 
 void Ctx::bind_workspaces() {
   for (Workspace* w : {&ws_fft, &ws_pairs, &ws_gemm, &ws_rhs, &ws_io, &ws_red, &ws_conv, &ws_state, &ws_ci,
-                       &ws_ci2, &ws_kry, &ws_orb, &cmf.ws})
+                       &ws_ci2, &ws_kry, &ws_orb, &ws_tcerr, &cmf.ws})
     w->owner = &stream;
 }
 
@@ -106,6 +106,7 @@ Ctx::~Ctx() {
   ws_ci2.release();
   ws_kry.release();
   ws_orb.release();
+  ws_tcerr.release();
   cmf.ws.release();
   for (IntCache& ic : icache) dfree(*this, ic.dev);
   if (rhs_exec) cudaGraphExecDestroy(rhs_exec);
@@ -294,6 +295,11 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
     SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "coulomb_fp32 must be 0 or 1");
     if (value) SG_TRY(ensure_fp32_tables(h->c));
     h->c.coul_fp32 = (int)value;
+    return SINCGPU_OK;
+  }
+  if (!strcmp(name, "contract_tf32")) {
+    SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "contract_tf32 must be 0 or 1");
+    h->c.contract_tf32 = (int)value;
     return SINCGPU_OK;
   }
   set_error("unknown option '%s'", name);

@@ -165,6 +165,7 @@ struct Ctx {
   Workspace ws_ci, ws_ci2;  // CI scratch (KE phi + partials; summed one-body matrix)
   Workspace ws_kry;         // Krylov basis, Hessenberg, Pade output
   Workspace ws_orb;         // orbital Krylov basis and Jacobian state
+  Workspace ws_tcerr;       // timeout flag of the tensor-core contractions
   OrbPropState orb;
   CIState ci;
   CmfState cmf;
@@ -173,11 +174,18 @@ struct Ctx {
   cudaGraphExec_t rhs_exec = nullptr;
   int coul_chunk = 0;   // pairs per pass sequence (0 = automatic)
   int coul_fp32 = 0;    // 1: Coulomb passes in FP32 (precision form), 0: FP64
+  int contract_tf32 = 0;  // 1: reducedpot contraction as 3xTF32 on the tensor cores
   Prof prof;
 
   ~Ctx();
   void bind_workspaces();  // makes every workspace stream-ordered on `stream`
 };
+
+// Tensor-core (3xTF32) contractions of the precision form (contract_tc.cu).
+int rp_gemm_tf32(Ctx& c, const double* Rpl, const double* Wm, int K, int NC, const int* d_tmap,
+                 double2* reducedpot);
+int tc_error_reset(Ctx& c);
+int tc_error_read(Ctx& c, int* flag);
 
 // Stream-ordered device memory on the context's stream (cudaMallocAsync /
 // cudaFreeAsync): allocating and freeing the context's tables neither

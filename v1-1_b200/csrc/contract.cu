@@ -813,6 +813,7 @@ static int reduced_pot_impl(Ctx& c, const double* Rpl, const int* h_pa, const in
     }
   }
   ProfScope ps(c, ST_RP_GEMM);
+  if (c.contract_tf32) return rp_gemm_tf32(c, Rpl, Wm, K, NC, half ? d_tmap : nullptr, reducedpot);
   const int gx = ceil_div(c.G, RM);
 #define SG_RP_LAUNCH(CG)                                                                                   \
   if (half)                                                                                                \

@@ -1,0 +1,273 @@
+// Tensor-core (tcgen05, kind::tf32) contractions of the precision form.
+//
+// C[m][n] = sum_k A[m][k] B[n][k] with FP64 inputs split as v = hi + lo (both
+// tf32) and three MMAs per K step, hi*hi + hi*lo + lo*hi, accumulated in FP32 in
+// tensor memory ("3xTF32": about 2^-21 relative per product, the FP32 level of the
+// precision form's Coulomb potentials).  One CTA of 128 threads owns a 128-row x
+// NT-column tile (NT <= 256, a multiple of 16): the threads stage K chunks of A
+// and B into shared memory (two stages, the split done while staging), thread 0
+// issues the MMAs and commits them to an mbarrier, and the epilogue reads the
+// accumulator rows back from tensor memory (one row per thread).
+//
+// Used for get_reducedpot0's contraction (SRC/mean.f90:556-558, reducedpot =
+// R x Gamma) when the context option contract_tf32 is set.
+#include <algorithm>
+#include "context.hpp"
+#include "umma.cuh"
+#include "../../include/sincgpu.h"
+
+namespace sincgpu {
+
+namespace {
+
+constexpr uint32_t kWaitLimit = 1u << 26;  // mbarrier polls before a wait is declared stuck
+
+// Generic epilogue: C[m * ldm + n * ldn] = D[m][n] (FP64), for the self test.
+struct StoreEpi {
+  double* C;
+  long long ldm, ldn;
+  __device__ void operator()(long long m, int n, float v) const { C[m * ldm + (long long)n * ldn] = (double)v; }
+};
+
+// reducedpot epilogue: columns 2t, 2t+1 are Re, Im of the orbital pair t; with
+// `tmap` only pairs kk <= ii are computed and reducedpot(x, ii, kk) is the
+// conjugate of reducedpot(x, kk, ii).
+struct RedpotEpi {
+  double2* out;
+  long long G;
+  const int* tmap;
+  int n;
+};
+
+template <int KC>
+struct TileSmem {
+  static constexpr int kA = KC * 128;  // u32 per A tile (hi or lo)
+  __host__ __device__ static constexpr size_t bytes(int NT) {
+    return sizeof(uint32_t) * 2 * (2 * (size_t)kA + 2 * (size_t)KC * NT);
+  }
+};
+
+// Stages rows m0.. of A and columns n0.. of B, K range [k0, k0 + KC), split into
+// tf32 hi / lo, in the chunk-major K-major core-matrix layout of umma.cuh.
+template <int KC>
+__device__ __forceinline__ void stage_tile(uint32_t* base, int NT, const double* __restrict__ A, long long lam,
+                                           long long lak, long long M, long long m0, const double* __restrict__ B,
+                                           long long lbn, long long lbk, int Ntot, int n0, int K, int k0) {
+  uint32_t* Ahi = base;
+  uint32_t* Alo = Ahi + TileSmem<KC>::kA;
+  uint32_t* Bhi = Alo + TileSmem<KC>::kA;
+  uint32_t* Blo = Bhi + KC * NT;
+  const int tid = threadIdx.x;
+  const long long m = m0 + tid;
+#pragma unroll
+  for (int c = 0; c < KC / 4; ++c) {
+    uint4 h, l;
+    uint32_t* hp = &h.x;
+    uint32_t* lp = &l.x;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = k0 + 4 * c + j;
+      const double v = (m < M && k < K) ? A[m * lam + (long long)k * lak] : 0.0;
+      umma::split_tf32(v, hp[j], lp[j]);
+    }
+    *reinterpret_cast<uint4*>(Ahi + (c * 128 + tid) * 4) = h;
+    *reinterpret_cast<uint4*>(Alo + (c * 128 + tid) * 4) = l;
+  }
+  for (int idx = tid; idx < (KC / 4) * NT; idx += 128) {
+    const int c = idx / NT, r = idx - c * NT;
+    const int nn = n0 + r;
+    uint4 h, l;
+    uint32_t* hp = &h.x;
+    uint32_t* lp = &l.x;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = k0 + 4 * c + j;
+      const double v = (nn < Ntot && k < K) ? B[(long long)nn * lbn + (long long)k * lbk] : 0.0;
+      umma::split_tf32(v, hp[j], lp[j]);
+    }
+    *reinterpret_cast<uint4*>(Bhi + (c * NT + r) * 4) = h;
+    *reinterpret_cast<uint4*>(Blo + (c * NT + r) * 4) = l;
+  }
+}
+
+template <class Epi>
+__device__ __forceinline__ void apply_epi(const Epi& e, long long m, long long M, int n, int Ntot,
+                                          const float (&v)[8]);
+
+template <>
+__device__ __forceinline__ void apply_epi<StoreEpi>(const StoreEpi& e, long long m, long long M, int n, int Ntot,
+                                                    const float (&v)[8]) {
+  if (m >= M) return;
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    if (n + j < Ntot) e(m, n + j, v[j]);
+}
+
+template <>
+__device__ __forceinline__ void apply_epi<RedpotEpi>(const RedpotEpi& e, long long m, long long M, int n,
+                                                     int Ntot, const float (&v)[8]) {
+  if (m >= M) return;
+#pragma unroll
+  for (int j = 0; j < 8; j += 2) {
+    const int col = n + j;
+    if (col >= Ntot) break;
+    const int t = col / 2;
+    const double2 z = make_double2((double)v[j], (double)v[j + 1]);
+    if (e.tmap) {
+      const int kk = e.tmap[2 * t], ii = e.tmap[2 * t + 1];
+      e.out[(long long)(kk + e.n * ii) * e.G + m] = z;
+      if (kk != ii) e.out[(long long)(ii + e.n * kk) * e.G + m] = make_double2(z.x, -z.y);
+    } else {
+      e.out[(long long)t * e.G + m] = z;
+    }
+  }
+}
+
+template <int KC, class Epi>
+__global__ void __launch_bounds__(128) gemm_tf32x3_kernel(const double* __restrict__ A, long long lam,
+                                                          long long lak, long long M,
+                                                          const double* __restrict__ B, long long lbn,
+                                                          long long lbk, int Ntot, int K, int NT,
+                                                          uint32_t tmem_cols, Epi epi, int* __restrict__ err) {
+  extern __shared__ __align__(128) uint32_t tsm[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const long long m0 = (long long)blockIdx.x * 128;
+  const int n0 = blockIdx.y * NT;
+  const size_t stage_u32 = TileSmem<KC>::bytes(NT) / sizeof(uint32_t) / 2;
+  uint32_t* st[2] = {tsm, tsm + stage_u32};
+  if (warp == 0) umma::tmem_alloc(&tmem_base, tmem_cols);
+  if (tid == 0) {
+    umma::mbar_init(&mbar[0], 1);
+    umma::mbar_init(&mbar[1], 1);
+  }
+  const int nch = (K + KC - 1) / KC;
+  stage_tile<KC>(st[0], NT, A, lam, lak, M, m0, B, lbn, lbk, Ntot, n0, K, 0);
+  umma::fence_smem_to_async();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  const uint32_t idesc = umma::idesc_tf32(128, NT);
+  bool ok = true;
+  for (int ch = 0; ch < nch; ++ch) {
+    const int s = ch & 1;
+    if (tid == 0) {
+      const uint32_t a_hi = umma::smem_u32(st[s]);
+      const uint32_t a_lo = a_hi + 4u * TileSmem<KC>::kA;
+      const uint32_t b_hi = a_lo + 4u * TileSmem<KC>::kA;
+      const uint32_t b_lo = b_hi + 4u * KC * NT;
+#pragma unroll
+      for (int ks = 0; ks < KC / 8; ++ks) {
+        const uint32_t ao = ks * 2 * 128 * 16, bo = ks * 2 * NT * 16;
+        const uint64_t ah = umma::desc_kmajor(a_hi + ao, 128 * 16, 128);
+        const uint64_t al = umma::desc_kmajor(a_lo + ao, 128 * 16, 128);
+        const uint64_t bh = umma::desc_kmajor(b_hi + bo, NT * 16, 128);
+        const uint64_t bl = umma::desc_kmajor(b_lo + bo, NT * 16, 128);
+        umma::mma_tf32(tmem, ah, bh, idesc, ch > 0 || ks > 0);
+        umma::mma_tf32(tmem, ah, bl, idesc, true);
+        umma::mma_tf32(tmem, al, bh, idesc, true);
+      }
+      umma::commit(&mbar[s]);
+    }
+    if (ch + 1 < nch) {
+      // the other stage was read by the MMAs of chunk ch - 1
+      if (ch >= 1 && ok) ok = umma::mbar_wait(&mbar[s ^ 1], ((ch - 1) >> 1) & 1, kWaitLimit);
+      if (ok) stage_tile<KC>(st[s ^ 1], NT, A, lam, lak, M, m0, B, lbn, lbk, Ntot, n0, K, (ch + 1) * KC);
+      umma::fence_smem_to_async();
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+  }
+  // MMAs complete in issue order: the last commit covers all of them
+  if (ok) ok = umma::mbar_wait(&mbar[(nch - 1) & 1], ((nch - 1) >> 1) & 1, kWaitLimit);
+  if (!ok) {
+    atomicExch(err, 1);
+    umma::mbar_wait(&mbar[(nch - 1) & 1], ((nch - 1) >> 1) & 1, kWaitLimit);
+  }
+  umma::fence_after_sync();
+  if (ok) {
+    const long long m = m0 + 32 * warp + lane;
+    for (int c0 = 0; c0 < NT; c0 += 8) {
+      float v[8];
+      umma::tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+      umma::tmem_ld_wait();
+      apply_epi(epi, m, M, n0 + c0, Ntot, v);
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, tmem_cols);
+}
+
+constexpr int kKC = 16;
+constexpr int kSmemDyn = 224 * 1024;  // dynamic limit (the static mbarriers take the rest of 227 KB)
+
+// smem_min: dynamic shared memory to reserve at least (the self test reserves
+// more than its tiles need, so that every descriptor address stays inside the
+// CTA's allocation).
+template <class Epi>
+int launch_tf32x3(Ctx& c, const double* A, long long lam, long long lak, long long M, const double* B,
+                  long long lbn, long long lbk, int Ntot, int K, const Epi& epi, size_t smem_min = 0) {
+  SG_CHECK(M >= 1 && Ntot >= 1 && K >= 1, SINCGPU_EINVAL, "empty tensor-core contraction");
+  const int ntile = ceil_div(Ntot, 256);
+  const int NT = ceil_div(ceil_div(Ntot, ntile), 16) * 16;
+  const uint32_t cols = NT <= 32 ? 32 : NT <= 64 ? 64 : NT <= 128 ? 128 : 256;
+  const size_t smem = std::max(TileSmem<kKC>::bytes(NT), std::min<size_t>(smem_min, kSmemDyn));
+  // process-wide attribute, one fixed value (thread-safe static initialisation)
+  static const cudaError_t attr = cudaFuncSetAttribute(gemm_tf32x3_kernel<kKC, Epi>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDyn);
+  SG_CUDA(attr);
+  SG_TRY(c.ws_tcerr.ensure(sizeof(int)));
+  int* err = (int*)c.ws_tcerr.ptr;
+  const dim3 grid((unsigned)ceil_div(M, 128), (unsigned)ntile);
+  gemm_tf32x3_kernel<kKC, Epi><<<grid, 128, smem, c.stream>>>(A, lam, lak, M, B, lbn, lbk, Ntot, K, NT, cols, epi,
+                                                              err);
+  SG_LAUNCHED();
+  return SINCGPU_OK;
+}
+
+}  // namespace
+
+int tc_error_reset(Ctx& c) {
+  SG_TRY(c.ws_tcerr.ensure(sizeof(int)));
+  SG_CUDA(cudaMemsetAsync(c.ws_tcerr.ptr, 0, sizeof(int), c.stream));
+  return SINCGPU_OK;
+}
+
+int tc_error_read(Ctx& c, int* flag) {
+  *flag = 0;
+  if (!c.ws_tcerr.ptr) return SINCGPU_OK;
+  SG_CUDA(cudaMemcpyAsync(flag, c.ws_tcerr.ptr, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  SG_CUDA(cudaStreamSynchronize(c.stream));
+  return SINCGPU_OK;
+}
+
+// reducedpot[(kk + n ii) G + x] = sum_k Rpl[k G + x] Wm[k NC + col] (col = 2t + re/im)
+int rp_gemm_tf32(Ctx& c, const double* Rpl, const double* Wm, int K, int NC, const int* d_tmap,
+                 double2* reducedpot) {
+  RedpotEpi e{reducedpot, c.G, d_tmap, c.nspf};
+  return launch_tf32x3(c, Rpl, 1, c.G, c.G, Wm, 1, NC, NC, K, e);
+}
+
+}  // namespace sincgpu
+
+using namespace sincgpu;
+
+extern "C" int sincgpu_gemm_tf32x3_dev(sincgpu_ctx* h, const double* A, const double* B, double* C, long long M,
+                                       int N, int K, int* timed_out) {
+  CTX_CHECK(h);
+  Ctx& c = h->c;
+  SG_CHECK(A && B && C, SINCGPU_EINVAL, "null matrix");
+  SG_CHECK(M >= 1 && N >= 1 && K >= 1, SINCGPU_EINVAL, "bad sizes");
+  SG_TRY(tc_error_reset(c));
+  StoreEpi e{C, N, 1};
+  SG_TRY(launch_tf32x3(c, A, K, 1, M, B, K, 1, N, K, e, 200 * 1024));
+  int flag = 0;
+  SG_TRY(tc_error_read(c, &flag));
+  if (timed_out) *timed_out = flag;
+  SG_CHECK(!flag, SINCGPU_ECUDA, "tensor-core contraction timed out waiting for its MMAs");
+  return SINCGPU_OK;
+}

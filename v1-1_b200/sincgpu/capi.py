@@ -104,6 +104,7 @@ _SIGS = {
     "sincgpu_batch_destroy": ([_P], _I),
     "sincgpu_autotune_rhs": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
     "sincgpu_set_sync_mode": ([_I, _I], _I),
+    "sincgpu_gemm_tf32x3_dev": ([_P, _P, _P, _P, _LL, _I, _I, _P], _I),
     "sincgpu_server_create": ([C.POINTER(_P), _I, _LL, _I], _I),
     "sincgpu_server_submit": ([_P, _P, _P], _I),
     "sincgpu_server_wait": ([_P, _I, _P, _P, _P, _P, _P], _I),
@@ -538,6 +539,16 @@ class SincProject:
     # --------------------------------------------------- device-resident
     def twoe_matel_dev(self, phi1, phi2, twoematel, twoereduced=None):
         _call("sincgpu_twoe_matel_dev", self._h, _ptr(phi1), _ptr(phi2), _ptr(twoematel), _ptr(twoereduced))
+
+    def gemm_tf32x3_dev(self, a, b, out) -> int:
+        """out = a b^T on the tensor cores (3xTF32, FP32 accumulation); a (M, K),
+        b (N, K), out (M, N) row-major float64 device tensors.  Returns the
+        timeout flag (0 when the MMAs completed)."""
+        m, k = a.shape
+        t = _I(0)
+        _call("sincgpu_gemm_tf32x3_dev", self._h, _ptr(a), _ptr(b), _ptr(out), int(m), int(b.shape[0]), int(k),
+              C.byref(t))
+        return t.value
 
     def mult_ke_dev(self, inp, out, howmany):
         _call("sincgpu_mult_ke_dev", self._h, _ptr(inp), _ptr(out), int(howmany))
