@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="only the warm-up and timed evaluations (profiling runs)")
+    ap.add_argument("--profile-precision-form", action="store_true",
+                    help="with --no-extras: time the precision form (FP32 Coulomb passes, 3xTF32 "
+                         "tensor-core reducedpot) instead of the FP64 form")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--batched-count", type=int, default=64)
@@ -232,6 +235,11 @@ def main():
     def step():
         proj.orbital_rhs_avec_dev(phi, avec, den, inv, tally, mat, red, out)
 
+    if args.profile_precision_form:
+        if not args.no_extras:
+            raise SystemExit("--profile-precision-form is a profiling mode: use it with --no-extras")
+        proj.set_option("coulomb_fp32", 1)
+        proj.set_option("contract_tf32", 1)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()

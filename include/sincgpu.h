@@ -75,13 +75,19 @@ int sincgpu_fft_length(sincgpu_ctx* ctx);
 /* Options: "coul_chunk" (pairs per Coulomb pass sequence, 0 = auto);
  * "coulomb_fp32" (1: the Coulomb passes in FP32, the precision form);
  * "contract_tf32" (1: the reducedpot contraction on the tensor cores as 3xTF32
- * with FP32 accumulation, the precision form). */
+ * with FP32 accumulation, the precision form); "coul_tma" (the Coulomb z pass
+ * with TMA-staged slabs: 1 on, 0 off, -1 automatic = on for FFT lengths >= 128). */
 int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
 
 /* C(M x N, row-major) = A(M x K, row-major) * B(N x K, row-major)^T on the
  * tensor cores (tcgen05 kind::tf32, 3xTF32 split, FP32 accumulation), device
  * pointers.  The contraction kernel of the precision form, exposed for checks;
  * *timed_out (may be NULL) is set when the kernel gave up waiting for its MMAs. */
+/* flags[0..1]: 1 when a tensor-core contraction / a TMA-staged Coulomb z pass gave
+ * up waiting for its MMAs or slab loads (bounded waits) since the context was
+ * created; synchronises the context's stream. */
+int sincgpu_kernel_timeouts(sincgpu_ctx* ctx, int* flags);
+
 int sincgpu_gemm_tf32x3_dev(sincgpu_ctx* ctx, const double* A, const double* B, double* C, long long M, int N,
                             int K, int* timed_out);
 

@@ -107,6 +107,22 @@ def test_call_twoe_matel00_multitile(built_lib, nspf, general):
         gpu.close()
 
 
+def test_coulomb_tma_z_pass_matches_plain(h2):
+    """The TMA-staged persistent z pass (default) against the plain z pass on the
+    same densities: same transforms, the kernel spectrum's real part only (its
+    imaginary part is rounding noise), so agreement to 1e-14; no timeouts."""
+    sysm, gpu = h2
+    rng = np.random.default_rng(7)
+    dens = rng.standard_normal((sysm.G, 3)) + 1j * rng.standard_normal((sysm.G, 3))
+    gpu.set_option("coul_tma", 0)
+    plain = gpu.op_tinv(dens)
+    gpu.set_option("coul_tma", 1)
+    staged = gpu.op_tinv(dens)
+    assert relerr(staged, plain) < 1e-14
+    assert relerr(staged, sysm.op_tinv(dens)) < TOL
+    assert gpu.kernel_timeouts() == [0, 0]
+
+
 def test_mult_ke(he, h2):
     for sysm, gpu in ((he[0], he[1]), h2):
         rng = np.random.default_rng(5)

@@ -297,6 +297,11 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
     h->c.coul_fp32 = (int)value;
     return SINCGPU_OK;
   }
+  if (!strcmp(name, "coul_tma")) {
+    SG_CHECK(value >= -1 && value <= 1, SINCGPU_EINVAL, "coul_tma must be -1, 0 or 1");
+    h->c.coul_tma = (int)value;
+    return SINCGPU_OK;
+  }
   if (!strcmp(name, "contract_tf32")) {
     SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "contract_tf32 must be 0 or 1");
     h->c.contract_tf32 = (int)value;

@@ -165,7 +165,7 @@ struct Ctx {
   Workspace ws_ci, ws_ci2;  // CI scratch (KE phi + partials; summed one-body matrix)
   Workspace ws_kry;         // Krylov basis, Hessenberg, Pade output
   Workspace ws_orb;         // orbital Krylov basis and Jacobian state
-  Workspace ws_tcerr;       // timeout flag of the tensor-core contractions
+  Workspace ws_tcerr;       // timeout flags: [0] tensor-core contractions, [1] TMA z pass
   OrbPropState orb;
   CIState ci;
   CmfState cmf;
@@ -175,6 +175,7 @@ struct Ctx {
   int coul_chunk = 0;   // pairs per pass sequence (0 = automatic)
   int coul_fp32 = 0;    // 1: Coulomb passes in FP32 (precision form), 0: FP64
   int contract_tf32 = 0;  // 1: reducedpot contraction as 3xTF32 on the tensor cores
+  int coul_tma = -1;      // TMA-staged persistent z pass: 1 on, 0 off, -1 automatic
   Prof prof;
 
   ~Ctx();
@@ -185,6 +186,9 @@ struct Ctx {
 int rp_gemm_tf32(Ctx& c, const double* Rpl, const double* Wm, int K, int NC, const int* d_tmap,
                  double2* reducedpot);
 int tc_error_reset(Ctx& c);
+// Device flags (zeroed once) that kernels with bounded waits set when a wait gave
+// up: [0] tensor-core contractions, [1] TMA-staged Coulomb z pass.
+int timeout_flags(Ctx& c, int** flags);
 int tc_error_read(Ctx& c, int* flag);
 
 // Stream-ordered device memory on the context's stream (cudaMallocAsync /

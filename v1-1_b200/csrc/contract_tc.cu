@@ -220,8 +220,8 @@ int launch_tf32x3(Ctx& c, const double* A, long long lam, long long lak, long lo
   static const cudaError_t attr = cudaFuncSetAttribute(gemm_tf32x3_kernel<kKC, Epi>,
                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDyn);
   SG_CUDA(attr);
-  SG_TRY(c.ws_tcerr.ensure(sizeof(int)));
-  int* err = (int*)c.ws_tcerr.ptr;
+  int* err = nullptr;
+  SG_TRY(timeout_flags(c, &err));
   const dim3 grid((unsigned)ceil_div(M, 128), (unsigned)ntile);
   gemm_tf32x3_kernel<kKC, Epi><<<grid, 128, smem, c.stream>>>(A, lam, lak, M, B, lbn, lbk, Ntot, K, NT, cols, epi,
                                                               err);
@@ -231,9 +231,19 @@ int launch_tf32x3(Ctx& c, const double* A, long long lam, long long lak, long lo
 
 }  // namespace
 
+int timeout_flags(Ctx& c, int** flags) {
+  if (!c.ws_tcerr.ptr) {
+    SG_TRY(c.ws_tcerr.ensure(64));
+    SG_CUDA(cudaMemsetAsync(c.ws_tcerr.ptr, 0, 64, c.stream));
+  }
+  *flags = (int*)c.ws_tcerr.ptr;
+  return SINCGPU_OK;
+}
+
 int tc_error_reset(Ctx& c) {
-  SG_TRY(c.ws_tcerr.ensure(sizeof(int)));
-  SG_CUDA(cudaMemsetAsync(c.ws_tcerr.ptr, 0, sizeof(int), c.stream));
+  int* f = nullptr;
+  SG_TRY(timeout_flags(c, &f));
+  SG_CUDA(cudaMemsetAsync(f, 0, sizeof(int), c.stream));
   return SINCGPU_OK;
 }
 
@@ -255,6 +265,17 @@ int rp_gemm_tf32(Ctx& c, const double* Rpl, const double* Wm, int K, int NC, con
 }  // namespace sincgpu
 
 using namespace sincgpu;
+
+extern "C" int sincgpu_kernel_timeouts(sincgpu_ctx* h, int* flags) {
+  CTX_CHECK(h);
+  Ctx& c = h->c;
+  SG_CHECK(flags, SINCGPU_EINVAL, "null flags");
+  flags[0] = flags[1] = 0;
+  if (!c.ws_tcerr.ptr) return SINCGPU_OK;
+  SG_CUDA(cudaMemcpyAsync(flags, c.ws_tcerr.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  SG_CUDA(cudaStreamSynchronize(c.stream));
+  return SINCGPU_OK;
+}
 
 extern "C" int sincgpu_gemm_tf32x3_dev(sincgpu_ctx* h, const double* A, const double* B, double* C, long long M,
                                        int N, int K, int* timed_out) {

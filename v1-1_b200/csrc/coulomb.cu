@@ -20,6 +20,7 @@
 // in FP32 (float2) with FP64 inputs and outputs.
 #include <algorithm>
 #include <vector>
+#include <cudaTypedefs.h>
 #include "coulomb_kernels.cuh"
 
 namespace sincgpu {
@@ -42,11 +43,12 @@ int fft_length_for(int min_len, int* p1, int* p2) {
 
 template <class C>
 static int coul_dispatch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2* s1,
-                         const double2* s2, double* Rpl, double2* full, bool herm) {
+                         const double2* s2, double* Rpl, double2* full, bool herm,
+                         const CUtensorMap* zmap = nullptr, int* err = nullptr) {
   switch (c.P) {
 #define SINCGPU_CASE(P, A, B) \
   case P:                     \
-    return coul_launch<A, B, C>(c, ca, np, dens, s1, s2, Rpl, full, herm);
+    return coul_launch<A, B, C>(c, ca, np, dens, s1, s2, Rpl, full, herm, zmap, err);
     SINCGPU_FFT_LENGTHS(SINCGPU_CASE)
 #undef SINCGPU_CASE
     default:
@@ -67,6 +69,42 @@ template <>
 const double2* khat_of<double2>(const Ctx& c) { return c.d_khat; }
 template <>
 const float2* khat_of<float2>(const Ctx& c) { return c.d_khat32; }
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// Tensor map of a W2 chunk for the TMA-staged z pass: [pair < np][z < N][2 P^2
+// reals], box (2 TL reals, N, 1).  False when the layout breaks a TMA rule (row
+// stride or base not 16-byte aligned, box too tall) or the driver has no encoder.
+template <class C>
+static bool make_zmap(const Ctx& c, const C* W2, int np, CUtensorMap* map) {
+  using R = typename CplxTraits<C>::Real;
+  const int N = c.N, P = c.P;
+  const int TL = lines_for_z<C>(P);
+  const size_t plane = sizeof(C) * (size_t)P * P;
+  if (plane % 16 || reinterpret_cast<uintptr_t>(W2) % 16 || N > 256 || 2 * TL > 256) return false;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+  if (!enc) return false;
+  const cuuint64_t dims[3] = {2ull * P * P, (cuuint64_t)N, (cuuint64_t)np};
+  const cuuint64_t strides[2] = {plane, plane * N};
+  const cuuint32_t box[3] = {(cuuint32_t)(2 * TL), (cuuint32_t)N, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(map, sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                         const_cast<C*>(W2), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
 
 template <class C>
 static int coul_run_t(Ctx& c, const double2* src1, const double2* src2, const int* h_pa,
@@ -96,12 +134,26 @@ static int coul_run_t(Ctx& c, const double2* src1, const double2* src2, const in
   ca.W1 = (C*)c.ws_fft.ptr;
   ca.W2 = ca.W1 + (long long)chunk * N * N * P;
   ca.npair_total = npair;
+  // TMA-staged z pass: one map over the chunk's W2 (the last, shorter chunk
+  // only addresses its first pairs)
+  // automatic choice: measured faster for the long lines of P >= 128 (162: z pass
+  // 9.9 -> 8.1 ms FP64, 4.8 -> 4.1 ms FP32 per evaluation of the 81^3 / 16-orbital
+  // workload) and slower at P = 81 (0.23 -> 0.25 ms), where fewer resident warps
+  // per SM cost more than the staging saves
+  CUtensorMap zmap;
+  const bool want_tma = c.coul_tma > 0 || (c.coul_tma < 0 && P >= 128);
+  const bool use_tma = want_tma && make_zmap<C>(c, ca.W2, chunk, &zmap);
+  int* err = nullptr;
+  if (use_tma) {
+    SG_TRY(timeout_flags(c, &err));
+    err += 1;
+  }
   for (int p0 = 0; p0 < npair; p0 += chunk) {
     const int np = std::min(chunk, npair - p0);
     ca.pair0 = p0;
     ca.pa = d_pa ? d_pa + p0 : nullptr;
     ca.pb = d_pb ? d_pb + p0 : nullptr;
-    SG_TRY(coul_dispatch(c, ca, np, dens, src1, src2, Rpl, full, herm));
+    SG_TRY(coul_dispatch(c, ca, np, dens, src1, src2, Rpl, full, herm, use_tma ? &zmap : nullptr, err));
   }
   return SINCGPU_OK;
 }

@@ -5,14 +5,28 @@
 // FP32, and the potentials are widened back to FP64 on output).  See coulomb.cu
 // for the algorithm and the passes.
 #pragma once
+#include <algorithm>
 #include "context.hpp"
 #include "fft_reg.cuh"
+#include "tma.cuh"
 
 namespace sincgpu {
 
-// lines (rows or columns) per CTA; fewer for long lines to stay within 48 KB of
-// static shared memory
-constexpr int lines_for(int P) { return P <= 128 ? 16 : 8; }
+// lines (rows or columns) per CTA of the x and y passes: fewer for long lines to
+// stay within 48 KB of static shared memory
+__host__ __device__ constexpr int lines_for(int P) { return P <= 128 ? 16 : 8; }
+
+// lines per CTA of the z pass (forward, spectrum multiply, inverse: the most
+// arithmetic per loaded line): the most of 32, 16, 8 whose exchange buffer and
+// twiddle table fit in 46 KB, so that a CTA is a whole number of warps where the
+// line length allows (measured: 9.9 vs 11.8 ms per evaluation on the 162-point
+// grid, neutral on the 81-point one; the x and y passes were slower with more).
+template <class C>
+__host__ __device__ constexpr int lines_for_z(int P) {
+  return ((P + 1) * 32 + P) * (int)sizeof(C) <= 46 * 1024   ? 32
+         : ((P + 1) * 16 + P) * (int)sizeof(C) <= 46 * 1024 ? 16
+                                                             : 8;
+}
 
 template <class C>
 struct CoulArgs {
@@ -101,8 +115,8 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
 
 // CZ: W2 columns along z (z < N): forward, * khat, inverse, z < N written back
 template <int P1, int P2, class C>
-__global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul_z_t(CoulArgs<C> ca) {
-  constexpr int P = P1 * P2, TL = lines_for(P);
+__global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_z<C>(P1 * P2)) coul_z_t(CoulArgs<C> ca) {
+  constexpr int P = P1 * P2, TL = lines_for_z<C>(P);
   __shared__ C roots[P];
   __shared__ C ex[P * TL];
   load_roots(roots, ca.roots, P);
@@ -131,6 +145,94 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
     for (int m1 = 0; m1 < P1; ++m1) {
       const int z = s + P2 * m1;
       if (z < N) base[z * zs] = a[m1];
+    }
+  }
+}
+
+// CZ with TMA-staged slabs: a persistent CTA walks its tiles of TL consecutive
+// (ky, kx) columns; the tile's N z-planes (an N x TL slab of W2) arrive in shared
+// memory by one tiled bulk tensor load, two tiles ahead of the computation (two
+// buffers, one mbarrier each), so the transforms never wait on global loads of
+// W2.  The kernel spectrum is real (the Coulomb kernel is real and even): its
+// real part for the thread's frequencies is loaded before the slab is awaited.
+// Same arithmetic as coul_z_t otherwise.  `err` is set when a slab never
+// arrives (bounded waits; the CTA then stops instead of hanging).
+template <int P1, int P2, class C>
+__global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_z<C>(P1 * P2))
+    coul_z_tma_t(CoulArgs<C> ca, const __grid_constant__ CUtensorMap zmap, int ntiles_f, int ntiles,
+                 size_t slab_stride, int* __restrict__ err) {
+  using R = typename CplxTraits<C>::Real;
+  constexpr int P = P1 * P2, TL = lines_for_z<C>(P);
+  constexpr uint32_t kLimit = 1u << 26;
+  __shared__ C roots[P];
+  __shared__ C ex[P * TL];
+  __shared__ __align__(8) uint64_t full[2];
+  extern __shared__ __align__(128) unsigned char slab_raw[];
+  load_roots(roots, ca.roots, P);
+  const int N = ca.N;
+  const int tid = threadIdx.x, l = tid % TL, s = tid / TL;
+  const long long zs = (long long)P * P;
+  const uint32_t slab_bytes = (uint32_t)(N * TL * sizeof(C));
+  auto slab = [&](int b) { return reinterpret_cast<C*>(slab_raw + b * slab_stride); };
+  auto issue = [&](int t, int b) {
+    const int p = t / ntiles_f, f0 = (t - p * ntiles_f) * TL;
+    tma::mbar_arrive_expect_tx(&full[b], slab_bytes);
+    tma::load_3d(slab(b), &zmap, 2 * f0, 0, p, &full[b]);
+  };
+  if (tid == 0) {
+    tma::mbar_init(&full[0], 1);
+    tma::mbar_init(&full[1], 1);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    if (blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
+  }
+  int i = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+    const int b = i & 1;
+    const int p = t / ntiles_f, f = (t - p * ntiles_f) * TL + l;
+    const bool col = f < zs;
+    R kh[P2];
+    if (col && s < P1) {
+      const R* khr = reinterpret_cast<const R*>(ca.khat + f);
+#pragma unroll
+      for (int k2 = 0; k2 < P2; ++k2) kh[k2] = khr[2 * (long long)(s + P1 * k2) * zs];
+    }
+    const bool arrived = tma::mbar_wait(&full[b], (i >> 1) & 1, kLimit);
+    if (__syncthreads_or(!arrived)) {
+      if (tid == 0) {
+        atomicExch(err, 1);
+        // let the other buffer's load (if any) land before the CTA leaves
+        tma::mbar_wait(&full[b ^ 1], ((i + 1) >> 1) & 1, kLimit);
+      }
+      return;
+    }
+    C a[P1], bb[P2];
+    const C* sl = slab(b);
+#pragma unroll
+    for (int n1 = 0; n1 < P1; ++n1) {
+      const int z = s + P2 * n1;
+      a[n1] = (col && s < P2 && z < N) ? sl[z * TL + l] : CplxTraits<C>::make(0.0, 0.0);
+    }
+    __syncthreads();  // the slab is read: its buffer takes the tile two steps ahead
+    if (tid == 0 && t + 2 * (int)gridDim.x < ntiles) {
+      tma::fence_proxy_async();
+      issue(t + 2 * gridDim.x, b);
+    }
+    dft_in_to_out<P1, P2, false, C>(a, bb, s, l, TL, ex, roots);
+    if (col && s < P1) {
+#pragma unroll
+      for (int k2 = 0; k2 < P2; ++k2) bb[k2] = CplxTraits<C>::make(bb[k2].x * kh[k2], bb[k2].y * kh[k2]);
+    }
+    dft_out_to_in<P1, P2, true, C>(bb, a, s, l, TL, ex, roots);
+    if (col && s < P2) {
+      C* base = ca.W2 + (long long)p * N * zs + f;
+#pragma unroll
+      for (int m1 = 0; m1 < P1; ++m1) {
+        const int z = s + P2 * m1;
+        if (z < N) base[z * zs] = a[m1];
+      }
     }
   }
 }
@@ -215,17 +317,21 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   }
 }
 
-// Launches the five passes for one chunk of np pairs.
+// Launches the five passes for one chunk of np pairs.  With `zmap` (a tensor map
+// of the chunk's W2 as [pair][z][2 P^2 reals]) the z pass is the TMA-staged
+// persistent kernel, else the plain one.
 template <int P1, int P2, class C>
 int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2* src1,
-                const double2* src2, double* Rpl, double2* full, bool herm) {
+                const double2* src2, double* Rpl, double2* full, bool herm, const CUtensorMap* zmap,
+                int* err) {
   constexpr int P = P1 * P2, S = P1 > P2 ? P1 : P2, TL = lines_for(P);
   const int N = ca.N;
   const int nthr = S * TL;
   // lines are flattened over the two outer axes so that no lane idles past the
   // end of a row of lines: rows f = z*N + y (x passes), columns f = z*P + kx
   // (y passes) and f = ky*P + kx (z pass)
-  const int nrow = ceil_div(N * N, TL), ncol = ceil_div(N * P, TL), nzc = ceil_div(P * P, TL);
+  constexpr int TLZ = lines_for_z<C>(P);
+  const int nrow = ceil_div(N * N, TL), ncol = ceil_div(N * P, TL), nzc = ceil_div(P * P, TLZ);
   {
     ProfScope ps(c, ST_COUL_FWD_X);
     if (dens)
@@ -241,7 +347,29 @@ int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2*
   }
   {
     ProfScope ps(c, ST_COUL_Z);
-    coul_z_t<P1, P2, C><<<dim3(nzc, 1, np), nthr, 0, c.stream>>>(ca);
+    if (zmap) {
+      const size_t slab_stride = ((size_t)N * TLZ * sizeof(C) + 127) / 128 * 128;
+      const size_t dyn = 2 * slab_stride;
+      static const cudaError_t attr = [] {
+        cudaFuncAttributes fa{};
+        cudaError_t e = cudaFuncGetAttributes(&fa, coul_z_tma_t<P1, P2, C>);
+        if (e == cudaSuccess)
+          e = cudaFuncSetAttribute(coul_z_tma_t<P1, P2, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(227 * 1024 - fa.sharedSizeBytes));
+        return e;
+      }();
+      SG_CUDA(attr);
+      int occ = 0;  // resident CTAs per SM at this slab size
+      SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, coul_z_tma_t<P1, P2, C>, S * TLZ, dyn));
+      occ = std::max(occ, 1);
+      int nsm = 148;
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device);
+      const int ntf = nzc, ntiles = nzc * np;
+      const int grid = std::min(ntiles, nsm * occ);
+      coul_z_tma_t<P1, P2, C><<<grid, S * TLZ, dyn, c.stream>>>(ca, *zmap, ntf, ntiles, slab_stride, err);
+    } else {
+      coul_z_t<P1, P2, C><<<dim3(nzc, 1, np), S * TLZ, 0, c.stream>>>(ca);
+    }
     SG_LAUNCHED();
   }
   {
@@ -270,17 +398,19 @@ int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2*
 #define SINCGPU_DECLARE_LAUNCH(P, A, B)                                                             \
   extern template int coul_launch<A, B, double2>(Ctx&, const CoulArgs<double2>&, int, bool,         \
                                                  const double2*, const double2*, double*, double2*, \
-                                                 bool);                                            \
+                                                 bool, const CUtensorMap*, int*);                  \
   extern template int coul_launch<A, B, float2>(Ctx&, const CoulArgs<float2>&, int, bool,           \
                                                 const double2*, const double2*, double*, double2*,  \
-                                                bool);
+                                                bool, const CUtensorMap*, int*);
 SINCGPU_FFT_LENGTHS(SINCGPU_DECLARE_LAUNCH)
 #undef SINCGPU_DECLARE_LAUNCH
 
 #define SINCGPU_INSTANTIATE_LAUNCH(P, A, B)                                                       \
   template int coul_launch<A, B, double2>(Ctx&, const CoulArgs<double2>&, int, bool,              \
-                                          const double2*, const double2*, double*, double2*, bool); \
+                                          const double2*, const double2*, double*, double2*, bool,  \
+                                          const CUtensorMap*, int*);                                \
   template int coul_launch<A, B, float2>(Ctx&, const CoulArgs<float2>&, int, bool,                \
-                                         const double2*, const double2*, double*, double2*, bool);
+                                         const double2*, const double2*, double*, double2*, bool,   \
+                                         const CUtensorMap*, int*);
 
 }  // namespace sincgpu

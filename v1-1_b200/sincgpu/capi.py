@@ -105,6 +105,7 @@ _SIGS = {
     "sincgpu_autotune_rhs": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
     "sincgpu_set_sync_mode": ([_I, _I], _I),
     "sincgpu_gemm_tf32x3_dev": ([_P, _P, _P, _P, _LL, _I, _I, _P], _I),
+    "sincgpu_kernel_timeouts": ([_P, _P], _I),
     "sincgpu_server_create": ([C.POINTER(_P), _I, _LL, _I], _I),
     "sincgpu_server_submit": ([_P, _P, _P], _I),
     "sincgpu_server_wait": ([_P, _I, _P, _P, _P, _P, _P], _I),
@@ -549,6 +550,12 @@ class SincProject:
         _call("sincgpu_gemm_tf32x3_dev", self._h, _ptr(a), _ptr(b), _ptr(out), int(m), int(b.shape[0]), int(k),
               C.byref(t))
         return t.value
+
+    def kernel_timeouts(self) -> list:
+        """[tensor-core contraction, TMA z pass] timeout flags (0 = never)."""
+        f = np.zeros(2, dtype=np.int32)
+        _call("sincgpu_kernel_timeouts", self._h, f.ctypes.data)
+        return f.tolist()
 
     def mult_ke_dev(self, inp, out, howmany):
         _call("sincgpu_mult_ke_dev", self._h, _ptr(inp), _ptr(out), int(howmany))
