@@ -3,11 +3,12 @@
 // C[m][n] = sum_k A[m][k] B[n][k] with FP64 inputs split as v = hi + lo (both
 // tf32) and three MMAs per K step, hi*hi + hi*lo + lo*hi, accumulated in FP32 in
 // tensor memory ("3xTF32": about 2^-21 relative per product, the FP32 level of the
-// precision form's Coulomb potentials).  One CTA of 128 threads owns a 128-row x
+// precision form's Coulomb potentials).  One CTA of 256 threads owns a 128-row x
 // NT-column tile (NT <= 256, a multiple of 16): the threads stage K chunks of A
 // and B into shared memory (two stages, the split done while staging), thread 0
 // issues the MMAs and commits them to an mbarrier, and the epilogue reads the
-// accumulator rows back from tensor memory (one row per thread).
+// accumulator back from tensor memory (a row per thread, half the columns per
+// warpgroup).
 //
 // Used for get_reducedpot0's contraction (SRC/mean.f90:556-558, reducedpot =
 // R x Gamma) when the context option contract_tf32 is set.
@@ -48,7 +49,9 @@ struct TileSmem {
 };
 
 // Stages rows m0.. of A and columns n0.. of B, K range [k0, k0 + KC), split into
-// tf32 hi / lo, in the chunk-major K-major core-matrix layout of umma.cuh.
+// tf32 hi / lo, in the chunk-major K-major core-matrix layout of umma.cuh.  Warps
+// 0-3 stage A (one row per thread), warps 4-7 stage B; every thread issues all of
+// its global loads before the first split, so a warp has KC loads in flight.
 template <int KC>
 __device__ __forceinline__ void stage_tile(uint32_t* base, int NT, const double* __restrict__ A, long long lam,
                                            long long lak, long long M, long long m0, const double* __restrict__ B,
@@ -58,35 +61,52 @@ __device__ __forceinline__ void stage_tile(uint32_t* base, int NT, const double*
   uint32_t* Bhi = Alo + TileSmem<KC>::kA;
   uint32_t* Blo = Bhi + KC * NT;
   const int tid = threadIdx.x;
-  const long long m = m0 + tid;
+  if (tid < 128) {
+    const long long m = m0 + tid;
+    double v[KC];
 #pragma unroll
-  for (int c = 0; c < KC / 4; ++c) {
-    uint4 h, l;
-    uint32_t* hp = &h.x;
-    uint32_t* lp = &l.x;
+    for (int k = 0; k < KC; ++k) v[k] = (m < M && k0 + k < K) ? A[m * lam + (long long)(k0 + k) * lak] : 0.0;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int k = k0 + 4 * c + j;
-      const double v = (m < M && k < K) ? A[m * lam + (long long)k * lak] : 0.0;
-      umma::split_tf32(v, hp[j], lp[j]);
+    for (int c = 0; c < KC / 4; ++c) {
+      uint4 h, l;
+      umma::split_tf32(v[4 * c + 0], h.x, l.x);
+      umma::split_tf32(v[4 * c + 1], h.y, l.y);
+      umma::split_tf32(v[4 * c + 2], h.z, l.z);
+      umma::split_tf32(v[4 * c + 3], h.w, l.w);
+      *reinterpret_cast<uint4*>(Ahi + (c * 128 + tid) * 4) = h;
+      *reinterpret_cast<uint4*>(Alo + (c * 128 + tid) * 4) = l;
     }
-    *reinterpret_cast<uint4*>(Ahi + (c * 128 + tid) * 4) = h;
-    *reinterpret_cast<uint4*>(Alo + (c * 128 + tid) * 4) = l;
-  }
-  for (int idx = tid; idx < (KC / 4) * NT; idx += 128) {
-    const int c = idx / NT, r = idx - c * NT;
-    const int nn = n0 + r;
-    uint4 h, l;
-    uint32_t* hp = &h.x;
-    uint32_t* lp = &l.x;
+  } else {
+    constexpr int kMaxIt = KC * 256 / 4 / 128;  // (KC / 4) * NT / 128 for NT <= 256
+    const int t2 = tid - 128;
+    const int nit = ((KC / 4) * NT + 127) / 128;
+    double v[kMaxIt][4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int k = k0 + 4 * c + j;
-      const double v = (nn < Ntot && k < K) ? B[(long long)nn * lbn + (long long)k * lbk] : 0.0;
-      umma::split_tf32(v, hp[j], lp[j]);
+    for (int it = 0; it < kMaxIt; ++it) {
+      const int idx = t2 + 128 * it;
+      const int c = idx / NT, r = idx - c * NT;
+      const int nn = n0 + r;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = k0 + 4 * c + j;
+        v[it][j] = (it < nit && c < KC / 4 && nn < Ntot && k < K) ? B[(long long)nn * lbn + (long long)k * lbk]
+                                                                 : 0.0;
+      }
     }
-    *reinterpret_cast<uint4*>(Bhi + (c * NT + r) * 4) = h;
-    *reinterpret_cast<uint4*>(Blo + (c * NT + r) * 4) = l;
+#pragma unroll
+    for (int it = 0; it < kMaxIt; ++it) {
+      const int idx = t2 + 128 * it;
+      const int c = idx / NT, r = idx - c * NT;
+      if (it < nit && c < KC / 4) {
+        uint4 h, l;
+        umma::split_tf32(v[it][0], h.x, l.x);
+        umma::split_tf32(v[it][1], h.y, l.y);
+        umma::split_tf32(v[it][2], h.z, l.z);
+        umma::split_tf32(v[it][3], h.w, l.w);
+        *reinterpret_cast<uint4*>(Bhi + (c * NT + r) * 4) = h;
+        *reinterpret_cast<uint4*>(Blo + (c * NT + r) * 4) = l;
+      }
+    }
   }
 }
 
@@ -124,7 +144,7 @@ __device__ __forceinline__ void apply_epi<RedpotEpi>(const RedpotEpi& e, long lo
 }
 
 template <int KC, class Epi>
-__global__ void __launch_bounds__(128) gemm_tf32x3_kernel(const double* __restrict__ A, long long lam,
+__global__ void __launch_bounds__(256) gemm_tf32x3_kernel(const double* __restrict__ A, long long lam,
                                                           long long lak, long long M,
                                                           const double* __restrict__ B, long long lbn,
                                                           long long lbk, int Ntot, int K, int NT,
@@ -189,10 +209,13 @@ __global__ void __launch_bounds__(128) gemm_tf32x3_kernel(const double* __restri
   }
   umma::fence_after_sync();
   if (ok) {
-    const long long m = m0 + 32 * warp + lane;
-    for (int c0 = 0; c0 < NT; c0 += 8) {
+    // warp w reads accumulator rows 32 (w % 4) .. + 31 (its tensor-memory lane
+    // quarter) and columns [h NT / 2, (h + 1) NT / 2), h = w / 4
+    const int q = warp & 3, h = warp >> 2;
+    const long long m = m0 + 32 * q + lane;
+    for (int c0 = h * (NT / 2); c0 < (h + 1) * (NT / 2); c0 += 8) {
       float v[8];
-      umma::tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+      umma::tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
       umma::tmem_ld_wait();
       apply_epi(epi, m, M, n0 + c0, Ntot, v);
     }
@@ -223,7 +246,7 @@ int launch_tf32x3(Ctx& c, const double* A, long long lam, long long lak, long lo
   int* err = nullptr;
   SG_TRY(timeout_flags(c, &err));
   const dim3 grid((unsigned)ceil_div(M, 128), (unsigned)ntile);
-  gemm_tf32x3_kernel<kKC, Epi><<<grid, 128, smem, c.stream>>>(A, lam, lak, M, B, lbn, lbk, Ntot, K, NT, cols, epi,
+  gemm_tf32x3_kernel<kKC, Epi><<<grid, 256, smem, c.stream>>>(A, lam, lak, M, B, lbn, lbk, Ntot, K, NT, cols, epi,
                                                               err);
   SG_LAUNCHED();
   return SINCGPU_OK;
