@@ -370,21 +370,33 @@ __global__ void __launch_bounds__(256, 1) twoe_gemm3_kernel(const double2* __res
   }
 }
 
-// C[m][n] = sum_s part[s][m][n] in split order (deterministic); elements of the
-// lower-triangle tiles (tile(m) > tile(n), never computed) are read mirrored
-__global__ void split_reduce_kernel(const double* __restrict__ part, int nsplit, int M, int TT,
-                                    double* __restrict__ C) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+// C[m][n] = sum_s part[s][m][n] (deterministic): a CTA owns 32 consecutive
+// elements; its 8 warps sum interleaved eighths of the split range (warp g takes
+// splits g, g + 8, ...) in a fixed order and warp 0 adds the eight partial sums in
+// order.  Elements of the lower-triangle tiles (tile(m) > tile(n), never computed)
+// are read mirrored.
+__global__ void __launch_bounds__(256) split_reduce_kernel(const double* __restrict__ part, int nsplit, int M,
+                                                           int TT, double* __restrict__ C) {
+  __shared__ double acc[8][32];
+  const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
   const long long MM = (long long)M * M;
-  if (i >= MM) return;
+  const long long i = (long long)blockIdx.x * 32 + lane;
   long long src = i;
-  if (TT < M) {
+  if (i < MM && TT < M) {
     const int m = (int)(i / M), n = (int)(i % M);
     if (m / TT > n / TT) src = (long long)n * M + m;
   }
   double s = 0.0;
-  for (int k = 0; k < nsplit; ++k) s += part[(long long)k * MM + src];
-  C[i] = s;
+  if (i < MM)
+    for (int k = g; k < nsplit; k += 8) s += part[(long long)k * MM + src];
+  acc[g][lane] = s;
+  __syncthreads();
+  if (g == 0 && i < MM) {
+    double t = acc[0][lane];
+#pragma unroll
+    for (int q = 1; q < 8; ++q) t += acc[q][lane];
+    C[i] = t;
+  }
 }
 
 // twoematel(a1,b1,a2,b2) from C = [[UR,US],[VR,VS]]
@@ -496,7 +508,7 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
     SG_LAUNCHED();
   }
   ProfScope ps(c, ST_TWOE_FINISH);
-  split_reduce_kernel<<<ceil_div(MM, 256), 256, 0, c.stream>>>(part, nsplit, M, TT, C);
+  split_reduce_kernel<<<ceil_div(MM, 32), 256, 0, c.stream>>>(part, nsplit, M, TT, C);
   SG_LAUNCHED();
   const long long n4 = (long long)n * n * n * n;
   twoe_assemble_kernel<<<ceil_div(n4, 256), 256, 0, c.stream>>>(C, d_lut, npair, n, herm ? 1 : 0,

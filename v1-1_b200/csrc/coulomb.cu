@@ -90,7 +90,7 @@ template <class C>
 static bool make_zmap(const Ctx& c, const C* W2, int np, CUtensorMap* map) {
   using R = typename CplxTraits<C>::Real;
   const int N = c.N, P = c.P;
-  const int TL = lines_for_z<C>(P);
+  const int TL = lines_for_ztma<C>(P);
   const size_t plane = sizeof(C) * (size_t)P * P;
   if (plane % 16 || reinterpret_cast<uintptr_t>(W2) % 16 || N > 256 || 2 * TL > 256) return false;
   PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();

@@ -27,6 +27,12 @@ __host__ __device__ constexpr int lines_for_z(int P) {
          : ((P + 1) * 16 + P) * (int)sizeof(C) <= 46 * 1024 ? 16
                                                              : 8;
 }
+// lines per tile of the TMA-staged z pass (measured: capping it at 16 made the FP32
+// pass on the 162-point grid slower, 4.1 -> 5.1 ms, and did not rescue P = 81)
+template <class C>
+__host__ __device__ constexpr int lines_for_ztma(int P) {
+  return lines_for_z<C>(P);
+}
 
 template <class C>
 struct CoulArgs {
@@ -158,11 +164,11 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_z<C>(P1 * P2))
 // Same arithmetic as coul_z_t otherwise.  `err` is set when a slab never
 // arrives (bounded waits; the CTA then stops instead of hanging).
 template <int P1, int P2, class C>
-__global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_z<C>(P1 * P2))
+__global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_ztma<C>(P1 * P2))
     coul_z_tma_t(CoulArgs<C> ca, const __grid_constant__ CUtensorMap zmap, int ntiles_f, int ntiles,
                  size_t slab_stride, int* __restrict__ err) {
   using R = typename CplxTraits<C>::Real;
-  constexpr int P = P1 * P2, TL = lines_for_z<C>(P);
+  constexpr int P = P1 * P2, TL = lines_for_ztma<C>(P);
   constexpr uint32_t kLimit = 1u << 26;
   __shared__ C roots[P];
   __shared__ C ex[P * TL];
@@ -348,7 +354,8 @@ int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2*
   {
     ProfScope ps(c, ST_COUL_Z);
     if (zmap) {
-      const size_t slab_stride = ((size_t)N * TLZ * sizeof(C) + 127) / 128 * 128;
+      constexpr int TLT = lines_for_ztma<C>(P);
+      const size_t slab_stride = ((size_t)N * TLT * sizeof(C) + 127) / 128 * 128;
       const size_t dyn = 2 * slab_stride;
       static const cudaError_t attr = [] {
         cudaFuncAttributes fa{};
@@ -360,13 +367,13 @@ int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2*
       }();
       SG_CUDA(attr);
       int occ = 0;  // resident CTAs per SM at this slab size
-      SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, coul_z_tma_t<P1, P2, C>, S * TLZ, dyn));
+      SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, coul_z_tma_t<P1, P2, C>, S * TLT, dyn));
       occ = std::max(occ, 1);
       int nsm = 148;
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device);
-      const int ntf = nzc, ntiles = nzc * np;
+      const int ntf = ceil_div(P * P, TLT), ntiles = ntf * np;
       const int grid = std::min(ntiles, nsm * occ);
-      coul_z_tma_t<P1, P2, C><<<grid, S * TLZ, dyn, c.stream>>>(ca, *zmap, ntf, ntiles, slab_stride, err);
+      coul_z_tma_t<P1, P2, C><<<grid, S * TLT, dyn, c.stream>>>(ca, *zmap, ntf, ntiles, slab_stride, err);
     } else {
       coul_z_t<P1, P2, C><<<dim3(nzc, 1, np), S * TLZ, 0, c.stream>>>(ca);
     }
