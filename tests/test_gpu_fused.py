@@ -93,3 +93,38 @@ def test_avec_reducedpot_mirror_equals_full(li):
     torch.cuda.synchronize()
     err = float((rp_half - rp_full).abs().max() / rp_full.abs().max())
     assert err < 1e-13
+
+
+def test_reducedpot_dmma_matches_dfma(built_lib):
+    """The FP64 tensor-core (DMMA) reducedpot and twoematel GEMMs against the
+    register-tiled DFMA ones on the same mean-field inputs: both FP64, different
+    summation order."""
+    import torch
+    from oracle import sinc_oracle as orc
+    from sincgpu import SincProject, WalkTables
+    n = 7
+    p = SincProject(21, 0.4, [[0, 0, 0]], [2.0], n)
+    try:
+        sysm = orc.SincSystem(21, 0.4, [[0, 0, 0]], [2.0])
+        phi = torch.from_numpy(np.ascontiguousarray(orc.seeded_orbitals(sysm, n, seed=9).T)).cuda()
+        w = WalkTables(2, n, 0)
+        p.ci_attach(w)
+        rng = np.random.default_rng(10)
+        av = rng.standard_normal(w.numconfig) + 1j * rng.standard_normal(w.numconfig)
+        av = torch.from_numpy(av / np.linalg.norm(av)).cuda()
+        cx = dict(dtype=torch.complex128, device="cuda")
+        bufs = [torch.empty((n, n), **cx), torch.empty((n, n), **cx), torch.empty((n,) * 4, **cx),
+                torch.empty((n,) * 4, **cx), torch.empty((n, n, sysm.G), **cx), torch.empty((n, sysm.G), **cx)]
+        p.set_option("rp_dmma", 0)
+        p.set_option("twoe_dmma", 0)
+        p.orbital_rhs_avec_dev(phi, av, *bufs)
+        ref, ref_mat = bufs[4].clone(), bufs[3].clone()
+        p.set_option("rp_dmma", 1)
+        p.set_option("twoe_dmma", 1)
+        p.orbital_rhs_avec_dev(phi, av, *bufs)
+        err = (bufs[4] - ref).abs().max().item() / ref.abs().max().item()
+        assert err < 1e-13, err
+        err = (bufs[3] - ref_mat).abs().max().item() / ref_mat.abs().max().item()
+        assert err < 1e-13, err
+    finally:
+        p.close()

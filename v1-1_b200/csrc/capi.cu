@@ -297,6 +297,16 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
     h->c.coul_fp32 = (int)value;
     return SINCGPU_OK;
   }
+  if (!strcmp(name, "twoe_dmma")) {
+    SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "twoe_dmma must be 0 or 1");
+    h->c.twoe_dmma = (int)value;
+    return SINCGPU_OK;
+  }
+  if (!strcmp(name, "rp_dmma")) {
+    SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "rp_dmma must be 0 or 1");
+    h->c.rp_dmma = (int)value;
+    return SINCGPU_OK;
+  }
   if (!strcmp(name, "coul_tma")) {
     SG_CHECK(value >= -1 && value <= 1, SINCGPU_EINVAL, "coul_tma must be -1, 0 or 1");
     h->c.coul_tma = (int)value;

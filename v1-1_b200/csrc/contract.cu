@@ -32,6 +32,14 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool val
   int n = valid ? 8 : 0;
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
 }
+// D (8 x 8, two values per lane) += A (8 x 4) B (4 x 8) on the FP64 tensor cores;
+// lane g * 4 + t holds A[g][t], B[t][g] and D[g][2t], D[g][2t + 1]
+__device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
@@ -249,8 +257,12 @@ __global__ void __launch_bounds__(256, 2) twoe_gemm2_kernel(const double2* __res
 // enough for U = 55), so neither the pair products nor the orbital
 // tiles are recomputed per column tile and padding stays small.  Split-K over x
 // across the SMs; cp.async double buffering of the orbital values and Rpl rows.
-template <int R>
-__global__ void __launch_bounds__(256, 1) twoe_gemm3_kernel(const double2* __restrict__ phi1,
+// DMMA = true: the same tiles on the FP64 tensor cores (mma.sync m8n8k4 f64):
+// R warps, warp w owns rows 16w..16w+15 of the tile and all its columns (2 x 2R
+// fragments of 8 x 8), shared-memory rows padded to TK + 4 doubles (4 mod 16) so
+// the fragment loads are conflict-free.
+template <int R, bool DMMA>
+__global__ void __launch_bounds__(DMMA ? 32 * R : 256, 1) twoe_gemm3_kernel(const double2* __restrict__ phi1,
                                                             const double2* __restrict__ phi2,
                                                             const int* __restrict__ pa,
                                                             const int* __restrict__ pb,
@@ -258,10 +270,12 @@ __global__ void __launch_bounds__(256, 1) twoe_gemm3_kernel(const double2* __res
                                                             int nspf, long long G, int ntn,
                                                             long long xper, double* __restrict__ part) {
   constexpr int TT = 16 * R;
+  constexpr int TS = DMMA ? TK + 4 : TK + 1;  // shared-memory row stride (doubles)
+  constexpr int NTH = DMMA ? 32 * R : 256;
   extern __shared__ __align__(16) double dsm[];
-  double* As = dsm;                                   // [TT][TK+1]
-  double* Bs = As + TT * (TK + 1);                    // [2][TT][TK+1]
-  double2* fsm = reinterpret_cast<double2*>(Bs + 2 * TT * (TK + 1));  // [2][2][nspf][TK]
+  double* As = dsm;                                   // [TT][TS]
+  double* Bs = As + TT * TS;                          // [2][TT][TS]
+  double2* fsm = reinterpret_cast<double2*>(Bs + 2 * TT * TS);  // [2][2][nspf][TK]
   int* sa = reinterpret_cast<int*>(fsm + 4 * nspf * TK);
   int* sb = sa + TT;
   int* sc = sb + TT;
@@ -280,7 +294,7 @@ __global__ void __launch_bounds__(256, 1) twoe_gemm3_kernel(const double2* __res
   const long long xb = blockIdx.y * xper;
   const long long xe = min(G, xb + xper);
   const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-  for (int i = tid; i < TT; i += 256) {
+  for (int i = tid; i < TT; i += NTH) {
     const int m = m0 + i;
     if (m < M) {
       const int p = m % npair;
@@ -294,7 +308,7 @@ __global__ void __launch_bounds__(256, 1) twoe_gemm3_kernel(const double2* __res
     }
   }
   auto load = [&](int st, long long x0) {
-    for (int i = tid; i < nspf * TK; i += 256) {
+    for (int i = tid; i < nspf * TK; i += NTH) {
       const int o = i / TK, k = i % TK;
       const long long x = x0 + k;
       const bool ok = x < xe;
@@ -305,21 +319,26 @@ __global__ void __launch_bounds__(256, 1) twoe_gemm3_kernel(const double2* __res
       cp_async8(&f2(st, o, k), g2, ok);
       cp_async8(reinterpret_cast<double*>(&f2(st, o, k)) + 1, reinterpret_cast<const double*>(g2) + 1, ok);
     }
-    for (int i = tid; i < TK * TT; i += 256) {
+    for (int i = tid; i < TK * TT; i += NTH) {
       const int nn = i / TK, k = i % TK;
       const int n = n0 + nn;
       const long long x = x0 + k;
       const bool ok = n < M && x < xe;
-      cp_async8(&Bs[(st * TT + nn) * (TK + 1) + k], ok ? (const void*)(Rpl + (long long)n * G + x) : (const void*)Rpl,
-                ok);
+      cp_async8(&Bs[(st * TT + nn) * TS + k], ok ? (const void*)(Rpl + (long long)n * G + x) : (const void*)Rpl, ok);
     }
     cp_async_commit();
   };
-  double acc[R][R];
+  double acc[DMMA ? 1 : R][DMMA ? 1 : R];
+  double dacc[DMMA ? 2 : 1][DMMA ? 2 * R : 1][2];
 #pragma unroll
-  for (int i = 0; i < R; ++i)
+  for (int i = 0; i < (DMMA ? 1 : R); ++i)
 #pragma unroll
-    for (int j = 0; j < R; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < (DMMA ? 1 : R); ++j) acc[i][j] = 0.0;
+#pragma unroll
+  for (int i = 0; i < (DMMA ? 2 : 1); ++i)
+#pragma unroll
+    for (int j = 0; j < (DMMA ? 2 * R : 1); ++j) dacc[i][j][0] = dacc[i][j][1] = 0.0;
+  const int warp = tid >> 5, g8 = (tid & 31) >> 2, t4 = tid & 3;
   const long long nk = (xe - xb + TK - 1) / TK;
   __syncthreads();  // sa/sb/sc visible
   if (nk > 0) load(0, xb);
@@ -332,7 +351,7 @@ __global__ void __launch_bounds__(256, 1) twoe_gemm3_kernel(const double2* __res
       cp_async_wait<0>();
     }
     __syncthreads();
-    for (int i = tid; i < TK * TT; i += 256) {
+    for (int i = tid; i < TK * TT; i += NTH) {
       const int mm = i / TK, k = i % TK;
       double v = 0.0;
       const int comp = sc[mm];
@@ -340,32 +359,60 @@ __global__ void __launch_bounds__(256, 1) twoe_gemm3_kernel(const double2* __res
         const double2 r = cmulc(f1(st, sa[mm], k), f2(st, sb[mm], k));
         v = comp == 0 ? r.x : r.y;
       }
-      As[mm * (TK + 1) + k] = v;
+      As[mm * TS + k] = v;
     }
     __syncthreads();
-    const double* Bst = Bs + st * TT * (TK + 1);
+    const double* Bst = Bs + st * TT * TS;
+    if constexpr (DMMA) {
+#pragma unroll
+      for (int k4 = 0; k4 < TK; k4 += 4) {
+        double a[2], b[2 * R];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) a[r] = As[(16 * warp + 8 * r + g8) * TS + k4 + t4];
+#pragma unroll
+        for (int j = 0; j < 2 * R; ++j) b[j] = Bst[(8 * j + g8) * TS + k4 + t4];
+#pragma unroll
+        for (int r = 0; r < 2; ++r)
+#pragma unroll
+          for (int j = 0; j < 2 * R; ++j) dmma_884(dacc[r][j], a[r], b[j]);
+      }
+    } else {
 #pragma unroll 4
-    for (int k = 0; k < TK; ++k) {
-      double a[R], b[R];
+      for (int k = 0; k < TK; ++k) {
+        double a[R], b[R];
 #pragma unroll
-      for (int i = 0; i < R; ++i) a[i] = As[(tx + 16 * i) * (TK + 1) + k];
+        for (int i = 0; i < R; ++i) a[i] = As[(tx + 16 * i) * TS + k];
 #pragma unroll
-      for (int j = 0; j < R; ++j) b[j] = Bst[(ty + 16 * j) * (TK + 1) + k];
+        for (int j = 0; j < R; ++j) b[j] = Bst[(ty + 16 * j) * TS + k];
 #pragma unroll
-      for (int i = 0; i < R; ++i)
+        for (int i = 0; i < R; ++i)
 #pragma unroll
-        for (int j = 0; j < R; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+          for (int j = 0; j < R; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+      }
     }
     __syncthreads();
   }
   double* out = part + (long long)blockIdx.y * M * M;
+  if constexpr (DMMA) {
 #pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const int m = m0 + tx + 16 * i;
+    for (int r = 0; r < 2; ++r) {
+      const int m = m0 + 16 * warp + 8 * r + g8;
 #pragma unroll
-    for (int j = 0; j < R; ++j) {
-      const int n = n0 + ty + 16 * j;
-      if (m < M && n < M) out[(long long)m * M + n] = acc[i][j];
+      for (int j = 0; j < 2 * R; ++j) {
+        const int n = n0 + 8 * j + 2 * t4;
+        if (m < M && n < M) out[(long long)m * M + n] = dacc[r][j][0];
+        if (m < M && n + 1 < M) out[(long long)m * M + n + 1] = dacc[r][j][1];
+      }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int m = m0 + tx + 16 * i;
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        const int n = n0 + ty + 16 * j;
+        if (m < M && n < M) out[(long long)m * M + n] = acc[i][j];
+      }
     }
   }
 }
@@ -476,22 +523,27 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
   SG_TRY(cached_ints(c, IC_LUT, lut.data(), (size_t)n * n, &d_lut));
   {
     ProfScope ps(c, ST_TWOE_GEMM);
-    const size_t sbytes = sizeof(double) * 3 * (size_t)TT * (TK + 1) + sizeof(double2) * 4 * (size_t)n * TK +
+    const int TS = c.twoe_dmma ? TK + 4 : TK + 1;
+    const size_t sbytes = sizeof(double) * 3 * (size_t)TT * TS + sizeof(double2) * 4 * (size_t)n * TK +
                           sizeof(int) * 3 * (size_t)TT;
     const dim3 grid(ntiles, nsplit);
-#define SG_TWOE_CASE(RR)                                                                                   \
-  case RR: {                                                                                               \
-    static bool attr = false;                                                                              \
-    if (!attr) {                                                                                           \
-      SG_CUDA(cudaFuncSetAttribute(twoe_gemm3_kernel<RR>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
-                                   (int)(sizeof(double) * 3 * 16 * RR * (TK + 1) +                         \
-                                         sizeof(double2) * 4 * kMaxOrb * TK + sizeof(int) * 3 * 16 * RR))); \
-      attr = true;                                                                                         \
-    }                                                                                                      \
-    twoe_gemm3_kernel<RR><<<grid, 256, sbytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl, npair, n, c.G, ntn, \
-                                                          xper, part);                                    \
-    break;                                                                                                 \
+#define SG_TWOE_LAUNCH(RR, DM)                                                                             \
+  {                                                                                                        \
+    static const cudaError_t attr = cudaFuncSetAttribute(                                                  \
+        twoe_gemm3_kernel<RR, DM>, cudaFuncAttributeMaxDynamicSharedMemorySize,                            \
+        (int)(sizeof(double) * 3 * 16 * RR * (TK + 4) + sizeof(double2) * 4 * kMaxOrb * TK +                \
+              sizeof(int) * 3 * 16 * RR));                                                                 \
+    SG_CUDA(attr);                                                                                         \
+    twoe_gemm3_kernel<RR, DM><<<grid, DM ? 32 * RR : 256, sbytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl,   \
+                                                                          npair, n, c.G, ntn, xper, part); \
   }
+#define SG_TWOE_CASE(RR)                \
+  case RR:                              \
+    if (c.twoe_dmma)                    \
+      SG_TWOE_LAUNCH(RR, true)          \
+    else                                \
+      SG_TWOE_LAUNCH(RR, false)         \
+    break;
     switch (R) {
       SG_TWOE_CASE(2)
       SG_TWOE_CASE(3)
@@ -505,6 +557,7 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
         break;
     }
 #undef SG_TWOE_CASE
+#undef SG_TWOE_LAUNCH
     SG_LAUNCHED();
   }
   ProfScope ps(c, ST_TWOE_FINISH);
@@ -729,6 +782,95 @@ __global__ void __launch_bounds__(16 * CG) rp_gemm3_kernel(const double* __restr
   }
 }
 
+// reducedpot GEMM on the FP64 tensor cores (mma.sync m8n8k4 f64, the FP64 tensor
+// path of sm_100a): CTA tile 128 (x) x 64 (columns), 8 warps of 32 x 32 (4 x 4
+// MMA tiles, 32 accumulators per thread), K in chunks of 8 with a three-stage
+// cp.async pipeline.  Shared-memory rows are padded to 4 (mod 16) doubles so that
+// the fragment loads (lane g + 4t reads row t, column g) are free of bank
+// conflicts.  The accumulator pair (2t, 2t+1) of a fragment is one complex
+// column pair (Re, Im) of reducedpot.
+constexpr int DM = 128, DN = 64, DK = 8, DST = 3;
+constexpr int DAS = DM + 4, DBS = DN + 4;
+
+
+template <bool HALF>
+__global__ void __launch_bounds__(256) rp_dmma_kernel(const double* __restrict__ Rpl, const double* __restrict__ Wm,
+                                                      int K, int NC, long long G, double2* __restrict__ out,
+                                                      const int* __restrict__ tmap, int n) {
+  __shared__ __align__(16) double As[DST][DK][DAS];
+  __shared__ __align__(16) double Bs[DST][DK][DBS];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
+  const long long x0 = (long long)blockIdx.x * DM;
+  const int c0 = blockIdx.y * DN;
+  const int nk = (K + DK - 1) / DK;
+  auto load = [&](int st, int k0) {
+    for (int i = tid; i < DK * DM; i += 256) {
+      const int k = i / DM, xx = i % DM;
+      const long long x = x0 + xx;
+      const bool ok = (k0 + k < K) && x < G;
+      cp_async8(&As[st][k][xx], ok ? (const void*)(Rpl + (long long)(k0 + k) * G + x) : (const void*)Rpl, ok);
+    }
+    for (int i = tid; i < DK * DN; i += 256) {
+      const int k = i / DN, cc = i % DN;
+      const bool ok = (k0 + k < K) && (c0 + cc < NC);
+      cp_async8(&Bs[st][k][cc], ok ? (const void*)(Wm + (long long)(k0 + k) * NC + c0 + cc) : (const void*)Wm, ok);
+    }
+    cp_async_commit();
+  };
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  load(0, 0);
+  if (nk > 1) load(1, DK);
+  for (int kc = 0; kc < nk; ++kc) {
+    const int st = kc % DST;
+    if (kc + 2 < nk) {
+      load((kc + 2) % DST, (kc + 2) * DK);
+      cp_async_wait<2>();
+    } else if (kc + 1 < nk) {
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k4 = 0; k4 < DK; k4 += 4) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[st][k4 + t][wm + 8 * i + g];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[st][k4 + t][wn + 8 * j + g];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma_884(acc[i][j], a[i], b[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const long long x = x0 + wm + 8 * i + g;
+    if (x >= G) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int col = c0 + wn + 8 * j + 2 * t;
+      if (col >= NC) continue;
+      const double2 v = make_double2(acc[i][j][0], acc[i][j][1]);
+      if (HALF) {
+        const int tt = col / 2, kk = tmap[2 * tt], ii = tmap[2 * tt + 1];
+        out[(long long)(kk + n * ii) * G + x] = v;
+        if (kk != ii) out[(long long)(ii + n * kk) * G + x] = make_double2(v.x, -v.y);
+      } else {
+        out[(long long)(col / 2) * G + x] = v;
+      }
+    }
+  }
+}
+
 // out[(ki*G + x)] (complex) = sum_k Rpl[k*G+x] * Wm[k][2ki + {0,1}]
 constexpr int RBK = 16;
 __global__ void __launch_bounds__(256) rp_gemm_kernel(const double* __restrict__ Rpl,
@@ -826,6 +968,15 @@ static int reduced_pot_impl(Ctx& c, const double* Rpl, const int* h_pa, const in
   }
   ProfScope ps(c, ST_RP_GEMM);
   if (c.contract_tf32) return rp_gemm_tf32(c, Rpl, Wm, K, NC, half ? d_tmap : nullptr, reducedpot);
+  if (c.rp_dmma) {
+    const dim3 grid((unsigned)ceil_div(c.G, DM), (unsigned)ceil_div(NC, DN));
+    if (half)
+      rp_dmma_kernel<true><<<grid, 256, 0, c.stream>>>(Rpl, Wm, K, NC, c.G, reducedpot, d_tmap, n);
+    else
+      rp_dmma_kernel<false><<<grid, 256, 0, c.stream>>>(Rpl, Wm, K, NC, c.G, reducedpot, nullptr, n);
+    SG_LAUNCHED();
+    return SINCGPU_OK;
+  }
   const int gx = ceil_div(c.G, RM);
 #define SG_RP_LAUNCH(CG)                                                                                   \
   if (half)                                                                                                \
