@@ -23,8 +23,8 @@
 
 namespace sincgpu {
 
-constexpr int BM = 64, BN = 64, BK = 16;
 constexpr int kMaxOrb = 32;
+constexpr int TK = 16;  // x points per K stage of the twoematel GEMM
 
 // 8-byte asynchronous global->shared copy (zero-fill when !valid)
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
@@ -49,209 +49,6 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // A(x,m): m <  npair -> Re(phi1_{pa} conj(phi2_{pb}))(x),  m >= npair -> Im
 // B(x,n): Rpl[n*G + x]
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) twoe_gemm_kernel(const double2* __restrict__ phi1,
-                                                        const double2* __restrict__ phi2,
-                                                        const int* __restrict__ pa,
-                                                        const int* __restrict__ pb,
-                                                        const double* __restrict__ Rpl, int npair,
-                                                        int nspf, long long G, int ntn,
-                                                        long long xper, double* __restrict__ part) {
-  __shared__ double As[BK][BM + 1];
-  __shared__ double Bs[BK][BN + 1];
-  __shared__ double2 f1[kMaxOrb][BK];
-  __shared__ double2 f2[kMaxOrb][BK];
-  __shared__ int sa[BM], sb[BM], sc[BM];
-  const int M = 2 * npair;
-  const int tm = blockIdx.x / ntn, tn = blockIdx.x % ntn;
-  const int m0 = tm * BM, n0 = tn * BN;
-  const int split = blockIdx.y;
-  const long long xb = split * xper;
-  const long long xe = min(G, xb + xper);
-  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-  if (tid < BM) {
-    int m = m0 + tid;
-    if (m < M) {
-      int p = m % npair;
-      sa[tid] = pa[p];
-      sb[tid] = pb[p];
-      sc[tid] = m / npair;
-    } else {
-      sa[tid] = 0;
-      sb[tid] = 0;
-      sc[tid] = -1;
-    }
-  }
-  double acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  for (long long x0 = xb; x0 < xe; x0 += BK) {
-    __syncthreads();
-    // orbitals at the BK points of this k-tile
-    for (int i = tid; i < nspf * BK; i += 256) {
-      int o = i / BK, k = i % BK;
-      long long x = x0 + k;
-      bool ok = x < xe;
-      f1[o][k] = ok ? phi1[(long long)o * G + x] : make_double2(0, 0);
-      f2[o][k] = ok ? phi2[(long long)o * G + x] : make_double2(0, 0);
-    }
-    for (int i = tid; i < BK * BN; i += 256) {
-      int k = i / BN, nn = i % BN;  // consecutive threads -> consecutive n (rows of Rpl)
-      int n = n0 + nn;
-      long long x = x0 + k;
-      Bs[k][nn] = (n < M && x < xe) ? Rpl[(long long)n * G + x] : 0.0;
-    }
-    __syncthreads();
-    for (int i = tid; i < BK * BM; i += 256) {
-      int mm = i / BK, k = i % BK;
-      double v = 0.0;
-      int comp = sc[mm];
-      if (comp >= 0) {
-        double2 r = cmulc(f1[sa[mm]][k], f2[sb[mm]][k]);
-        v = comp == 0 ? r.x : r.y;
-      }
-      As[k][mm] = v;
-    }
-    __syncthreads();
-#pragma unroll 8
-    for (int k = 0; k < BK; ++k) {
-      double a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[k][tx + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[k][ty + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
-  }
-  double* out = part + (long long)split * M * M;
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    int m = m0 + tx + 16 * i;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      int n = n0 + ty + 16 * j;
-      if (m < M && n < M) out[(long long)m * M + n] = acc[i][j];
-    }
-  }
-}
-
-// twoematel GEMM, 128 (m) x 64 (n) tiles, 8x4 register blocks, split-K over x.
-// The B tile (Rpl rows) and the orbital values of the next k-tile are fetched with
-// cp.async while the current tile is multiplied; the A tile (real/imaginary parts
-// of the pair products) is formed in shared memory from the orbital values.
-constexpr int TM = 128, TN = 64, TK = 16;
-__global__ void __launch_bounds__(256, 2) twoe_gemm2_kernel(const double2* __restrict__ phi1,
-                                                            const double2* __restrict__ phi2,
-                                                            const int* __restrict__ pa,
-                                                            const int* __restrict__ pb,
-                                                            const double* __restrict__ Rpl, int npair,
-                                                            int nspf, long long G, int ntn,
-                                                            long long xper, double* __restrict__ part) {
-  // m-major / n-major tiles padded to TK+1: the fastest thread index walks k in the
-  // writes and rows in the FMA reads, both without bank conflicts
-  __shared__ __align__(16) double As[TM][TK + 1];
-  __shared__ __align__(16) double Bs[2][TN][TK + 1];
-  extern __shared__ __align__(16) double2 fsm[];  // [2 stages][2 sets][nspf][TK]
-  __shared__ int sa[TM], sb[TM], sc[TM];
-  auto f1 = [&](int st, int o, int k) -> double2& { return fsm[((st * 2 + 0) * nspf + o) * TK + k]; };
-  auto f2 = [&](int st, int o, int k) -> double2& { return fsm[((st * 2 + 1) * nspf + o) * TK + k]; };
-  const int M = 2 * npair;
-  const int tm = blockIdx.x / ntn, tn = blockIdx.x % ntn;
-  const int m0 = tm * TM, n0 = tn * TN;
-  const long long xb = blockIdx.y * xper;
-  const long long xe = min(G, xb + xper);
-  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-  for (int i = tid; i < TM; i += 256) {
-    int m = m0 + i;
-    if (m < M) {
-      int p = m % npair;
-      sa[i] = pa[p];
-      sb[i] = pb[p];
-      sc[i] = m / npair;
-    } else {
-      sa[i] = 0;
-      sb[i] = 0;
-      sc[i] = -1;
-    }
-  }
-  auto load = [&](int st, long long x0) {
-    for (int i = tid; i < nspf * TK; i += 256) {
-      int o = i / TK, k = i % TK;
-      long long x = x0 + k;
-      bool ok = x < xe;
-      const double2* g1 = ok ? phi1 + (long long)o * G + x : phi1;
-      const double2* g2 = ok ? phi2 + (long long)o * G + x : phi2;
-      cp_async8(&f1(st, o, k), g1, ok);
-      cp_async8(reinterpret_cast<double*>(&f1(st, o, k)) + 1, reinterpret_cast<const double*>(g1) + 1, ok);
-      cp_async8(&f2(st, o, k), g2, ok);
-      cp_async8(reinterpret_cast<double*>(&f2(st, o, k)) + 1, reinterpret_cast<const double*>(g2) + 1, ok);
-    }
-    for (int i = tid; i < TK * TN; i += 256) {
-      int nn = i / TK, k = i % TK;  // consecutive threads along x
-      int n = n0 + nn;
-      long long x = x0 + k;
-      bool ok = n < M && x < xe;
-      cp_async8(&Bs[st][nn][k], ok ? (const void*)(Rpl + (long long)n * G + x) : (const void*)Rpl, ok);
-    }
-    cp_async_commit();
-  };
-  double acc[8][4];
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  const long long nk = (xe - xb + TK - 1) / TK;
-  if (nk > 0) load(0, xb);
-  for (long long t = 0; t < nk; ++t) {
-    const int st = (int)(t & 1);
-    if (t + 1 < nk) {
-      load(st ^ 1, xb + (t + 1) * TK);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncthreads();
-    for (int i = tid; i < TK * TM; i += 256) {
-      int mm = i / TK, k = i % TK;
-      double v = 0.0;
-      const int comp = sc[mm];
-      if (comp >= 0) {
-        double2 r = cmulc(f1(st, sa[mm], k), f2(st, sb[mm], k));
-        v = comp == 0 ? r.x : r.y;
-      }
-      As[mm][k] = v;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < TK; ++k) {
-      double a[8], b[4];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) a[i] = As[tx + 16 * i][k];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[st][ty + 16 * j][k];
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
-    __syncthreads();
-  }
-  double* out = part + (long long)blockIdx.y * M * M;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int m = m0 + tx + 16 * i;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int n = n0 + ty + 16 * j;
-      if (m < M && n < M) out[(long long)m * M + n] = acc[i][j];
-    }
-  }
-}
-
 // twoematel GEMM with square 16R x 16R tiles (R x R register blocks, 256
 // threads): for 2U <= 16R one tile covers all outputs (R = 7 gives 112 x 112,
 // enough for U = 55), so neither the pair products nor the orbital
@@ -630,76 +427,7 @@ __global__ void build_w_half_kernel(const double2* __restrict__ tally, const int
   Wm[idx] = (col & 1) ? v.y : v.x;
 }
 
-// reducedpot GEMM, 128 (x) x 64 (columns) tiles, 8x4 register blocks, two-stage
-// cp.async pipeline over k (pair components).
-constexpr int RM = 128, RN = 64, RK = 16;
-__global__ void __launch_bounds__(256, 2) rp_gemm2_kernel(const double* __restrict__ Rpl,
-                                                       const double* __restrict__ Wm, int K, int NC,
-                                                       long long G, double2* __restrict__ out) {
-  __shared__ __align__(16) double As[2][RK][RM];
-  __shared__ __align__(16) double Bs[2][RK][RN];
-  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-  const long long x0 = (long long)blockIdx.x * RM;
-  const int c0 = blockIdx.y * RN;
-  auto load = [&](int st, int k0) {
-    for (int i = tid; i < RK * RM; i += 256) {
-      int k = i / RM, xx = i % RM;
-      long long x = x0 + xx;
-      bool ok = (k0 + k < K) && x < G;
-      cp_async8(&As[st][k][xx], ok ? (const void*)(Rpl + (long long)(k0 + k) * G + x) : (const void*)Rpl, ok);
-    }
-    for (int i = tid; i < RK * RN; i += 256) {
-      int k = i / RN, cc = i % RN;
-      bool ok = (k0 + k < K) && (c0 + cc < NC);
-      cp_async8(&Bs[st][k][cc], ok ? (const void*)(Wm + (long long)(k0 + k) * NC + c0 + cc) : (const void*)Wm, ok);
-    }
-    cp_async_commit();
-  };
-  double acc[8][4];
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  const int nk = (K + RK - 1) / RK;
-  load(0, 0);
-  for (int t = 0; t < nk; ++t) {
-    const int st = t & 1;
-    if (t + 1 < nk) {
-      load(st ^ 1, (t + 1) * RK);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < RK; ++k) {
-      double a[8], b[4];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) a[i] = As[st][k][tx + 16 * i];
-      const double2 b01 = *reinterpret_cast<const double2*>(&Bs[st][k][4 * ty]);
-      const double2 b23 = *reinterpret_cast<const double2*>(&Bs[st][k][4 * ty + 2]);
-      b[0] = b01.x;
-      b[1] = b01.y;
-      b[2] = b23.x;
-      b[3] = b23.y;
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const long long x = x0 + tx + 16 * i;
-    if (x >= G) continue;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int col = c0 + 4 * ty + 2 * h;
-      if (col < NC) out[(long long)(col / 2) * G + x] = make_double2(acc[i][2 * h], acc[i][2 * h + 1]);
-    }
-  }
-}
+constexpr int RM = 128, RK = 16;
 
 // reducedpot GEMM with 128 (x) x 4CG (columns) tiles, 16 x CG threads of 8x4
 // register blocks; CG is chosen per call so that the 2n^2 columns pad least.
@@ -867,58 +595,6 @@ __global__ void __launch_bounds__(256) rp_dmma_kernel(const double* __restrict__
       } else {
         out[(long long)(col / 2) * G + x] = v;
       }
-    }
-  }
-}
-
-// out[(ki*G + x)] (complex) = sum_k Rpl[k*G+x] * Wm[k][2ki + {0,1}]
-constexpr int RBK = 16;
-__global__ void __launch_bounds__(256) rp_gemm_kernel(const double* __restrict__ Rpl,
-                                                      const double* __restrict__ Wm, int K, int NC,
-                                                      long long G, double2* __restrict__ out) {
-  __shared__ double As[RBK][BM + 2];
-  __shared__ double Bs[RBK][BN + 2];
-  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-  const long long x0 = (long long)blockIdx.x * BM;
-  const int c0 = blockIdx.y * BN;
-  double acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  for (int k0 = 0; k0 < K; k0 += RBK) {
-    __syncthreads();
-    for (int i = tid; i < RBK * BM; i += 256) {
-      int k = i / BM, xx = i % BM;
-      long long x = x0 + xx;
-      As[k][xx] = (k0 + k < K && x < G) ? Rpl[(long long)(k0 + k) * G + x] : 0.0;
-    }
-    for (int i = tid; i < RBK * BN; i += 256) {
-      int k = i / BN, cc = i % BN;
-      Bs[k][cc] = (k0 + k < K && c0 + cc < NC) ? Wm[(long long)(k0 + k) * NC + c0 + cc] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < RBK; ++k) {
-      double a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[k][tx + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[k][4 * ty + j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    long long x = x0 + tx + 16 * i;
-    if (x >= G) continue;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      int col = c0 + 4 * ty + 2 * h;
-      if (col < NC) out[(long long)(col / 2) * G + x] = make_double2(acc[i][2 * h], acc[i][2 * h + 1]);
     }
   }
 }
