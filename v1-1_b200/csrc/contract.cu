@@ -55,11 +55,11 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // tiles are recomputed per column tile and padding stays small.  Split-K over x
 // across the SMs; cp.async double buffering of the orbital values and Rpl rows.
 // DMMA = true: the same tiles on the FP64 tensor cores (mma.sync m8n8k4 f64):
-// R warps, warp w owns rows 16w..16w+15 of the tile and all its columns (2 x 2R
-// fragments of 8 x 8), shared-memory rows padded to TK + 4 doubles (4 mod 16) so
-// the fragment loads are conflict-free.
+// 2R warps, warp w owns rows 16 (w / 2) .. + 15 of the tile and half of its
+// columns (2 x R fragments of 8 x 8), shared-memory rows padded to TK + 4 doubles
+// (4 mod 16) so the fragment loads are conflict-free.
 template <int R, bool DMMA>
-__global__ void __launch_bounds__(DMMA ? 32 * R : 256, 1) twoe_gemm3_kernel(const double2* __restrict__ phi1,
+__global__ void __launch_bounds__(DMMA ? 64 * R : 256, 1) twoe_gemm3_kernel(const double2* __restrict__ phi1,
                                                             const double2* __restrict__ phi2,
                                                             const int* __restrict__ pa,
                                                             const int* __restrict__ pb,
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(DMMA ? 32 * R : 256, 1) twoe_gemm3_kernel(cons
                                                             long long xper, double* __restrict__ part) {
   constexpr int TT = 16 * R;
   constexpr int TS = DMMA ? TK + 4 : TK + 1;  // shared-memory row stride (doubles)
-  constexpr int NTH = DMMA ? 32 * R : 256;
+  constexpr int NTH = DMMA ? 64 * R : 256;
   extern __shared__ __align__(16) double dsm[];
   double* As = dsm;                                   // [TT][TS]
   double* Bs = As + TT * TS;                          // [2][TT][TS]
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(DMMA ? 32 * R : 256, 1) twoe_gemm3_kernel(cons
     cp_async_commit();
   };
   double acc[DMMA ? 1 : R][DMMA ? 1 : R];
-  double dacc[DMMA ? 2 : 1][DMMA ? 2 * R : 1][2];
+  double dacc[DMMA ? 2 : 1][DMMA ? R : 1][2];
 #pragma unroll
   for (int i = 0; i < (DMMA ? 1 : R); ++i)
 #pragma unroll
@@ -134,8 +134,9 @@ __global__ void __launch_bounds__(DMMA ? 32 * R : 256, 1) twoe_gemm3_kernel(cons
 #pragma unroll
   for (int i = 0; i < (DMMA ? 2 : 1); ++i)
 #pragma unroll
-    for (int j = 0; j < (DMMA ? 2 * R : 1); ++j) dacc[i][j][0] = dacc[i][j][1] = 0.0;
-  const int warp = tid >> 5, g8 = (tid & 31) >> 2, t4 = tid & 3;
+    for (int j = 0; j < (DMMA ? R : 1); ++j) dacc[i][j][0] = dacc[i][j][1] = 0.0;
+  const int wrow = 16 * ((tid >> 5) >> 1), wcol = 8 * R * ((tid >> 5) & 1);
+  const int g8 = (tid & 31) >> 2, t4 = tid & 3;
   const long long nk = (xe - xb + TK - 1) / TK;
   __syncthreads();  // sa/sb/sc visible
   if (nk > 0) load(0, xb);
@@ -163,15 +164,15 @@ __global__ void __launch_bounds__(DMMA ? 32 * R : 256, 1) twoe_gemm3_kernel(cons
     if constexpr (DMMA) {
 #pragma unroll
       for (int k4 = 0; k4 < TK; k4 += 4) {
-        double a[2], b[2 * R];
+        double a[2], b[R];
 #pragma unroll
-        for (int r = 0; r < 2; ++r) a[r] = As[(16 * warp + 8 * r + g8) * TS + k4 + t4];
+        for (int r = 0; r < 2; ++r) a[r] = As[(wrow + 8 * r + g8) * TS + k4 + t4];
 #pragma unroll
-        for (int j = 0; j < 2 * R; ++j) b[j] = Bst[(8 * j + g8) * TS + k4 + t4];
+        for (int j = 0; j < R; ++j) b[j] = Bst[(wcol + 8 * j + g8) * TS + k4 + t4];
 #pragma unroll
         for (int r = 0; r < 2; ++r)
 #pragma unroll
-          for (int j = 0; j < 2 * R; ++j) dmma_884(dacc[r][j], a[r], b[j]);
+          for (int j = 0; j < R; ++j) dmma_884(dacc[r][j], a[r], b[j]);
       }
     } else {
 #pragma unroll 4
@@ -193,10 +194,10 @@ __global__ void __launch_bounds__(DMMA ? 32 * R : 256, 1) twoe_gemm3_kernel(cons
   if constexpr (DMMA) {
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
-      const int m = m0 + 16 * warp + 8 * r + g8;
+      const int m = m0 + wrow + 8 * r + g8;
 #pragma unroll
-      for (int j = 0; j < 2 * R; ++j) {
-        const int n = n0 + 8 * j + 2 * t4;
+      for (int j = 0; j < R; ++j) {
+        const int n = n0 + wcol + 8 * j + 2 * t4;
         if (m < M && n < M) out[(long long)m * M + n] = dacc[r][j][0];
         if (m < M && n + 1 < M) out[(long long)m * M + n + 1] = dacc[r][j][1];
       }
@@ -331,7 +332,7 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
         (int)(sizeof(double) * 3 * 16 * RR * (TK + 4) + sizeof(double2) * 4 * kMaxOrb * TK +                \
               sizeof(int) * 3 * 16 * RR));                                                                 \
     SG_CUDA(attr);                                                                                         \
-    twoe_gemm3_kernel<RR, DM><<<grid, DM ? 32 * RR : 256, sbytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl,   \
+    twoe_gemm3_kernel<RR, DM><<<grid, DM ? 64 * RR : 256, sbytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl,   \
                                                                           npair, n, c.G, ntn, xper, part); \
   }
 #define SG_TWOE_CASE(RR)                \
@@ -522,7 +523,7 @@ constexpr int DAS = DM + 4, DBS = DN + 4;
 
 
 template <bool HALF>
-__global__ void __launch_bounds__(256) rp_dmma_kernel(const double* __restrict__ Rpl, const double* __restrict__ Wm,
+__global__ void __launch_bounds__(256, 3) rp_dmma_kernel(const double* __restrict__ Rpl, const double* __restrict__ Wm,
                                                       int K, int NC, long long G, double2* __restrict__ out,
                                                       const int* __restrict__ tmap, int n) {
   __shared__ __align__(16) double As[DST][DK][DAS];
