@@ -20,7 +20,6 @@
 namespace sincgpu {
 
 constexpr int TXO = 32;          // grid points per tile (lanes)
-constexpr int NYO = 8;           // warps per block
 constexpr int kMaxOrbRhs = 32;   // largest orbital count of these kernels
 constexpr int kRhsSmemMax = 64 * 1024;
 
@@ -30,20 +29,20 @@ __device__ __forceinline__ void cfma(double2& acc, double2 v, double2 m) {  // a
 }
 
 // out(x,i) = sum_j in(x,j) mat(j,i)   (column-major n x n complex mat)
-__global__ void __launch_bounds__(TXO * NYO) mix_kernel(const double2* __restrict__ in,
+__global__ void __launch_bounds__(TXO * kMaxOrbRhs) mix_kernel(const double2* __restrict__ in,
                                                         const double2* __restrict__ mat, int n, long long G,
                                                         double2* __restrict__ out) {
   extern __shared__ double2 rsm[];
   double2* sm = rsm;            // n*n
   double2* tin = rsm + n * n;   // n x TXO
   const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
-  for (int e = tid; e < n * n; e += TXO * NYO) sm[e] = mat[e];
+  for (int e = tid; e < n * n; e += TXO * blockDim.y) sm[e] = mat[e];
   const long long x = blockIdx.x * (long long)TXO + lx;
   const bool ok = x < G;
-  for (int j = ty; j < n; j += NYO) tin[j * TXO + lx] = ok ? in[(long long)j * G + x] : make_double2(0.0, 0.0);
+  for (int j = ty; j < n; j += blockDim.y) tin[j * TXO + lx] = ok ? in[(long long)j * G + x] : make_double2(0.0, 0.0);
   __syncthreads();
   if (!ok) return;
-  for (int i = ty; i < n; i += NYO) {
+  for (int i = ty; i < n; i += blockDim.y) {
     double2 acc = make_double2(0.0, 0.0);
     for (int j = 0; j < n; ++j) cfma(acc, tin[j * TXO + lx], sm[j + n * i]);
     out[(long long)i * G + x] = acc;
@@ -52,7 +51,7 @@ __global__ void __launch_bounds__(TXO * NYO) mix_kernel(const double2* __restric
 
 // s_i = acc(x,i) + sum_k V(x,k,i) phi_k(x) over i in [i0, i0+ni); then, when
 // `dentime`, t_i = timefac * sum_j s_j inv(j,i) (all n orbitals present).
-__global__ void __launch_bounds__(TXO * NYO) redpot_kernel(const double2* __restrict__ phi,
+__global__ void __launch_bounds__(TXO * kMaxOrbRhs) redpot_kernel(const double2* __restrict__ phi,
                                                            const double2* __restrict__ V,
                                                            const double2* __restrict__ acc_in,
                                                            const double2* __restrict__ inv, double2 timefac,
@@ -64,13 +63,13 @@ __global__ void __launch_bounds__(TXO * NYO) redpot_kernel(const double2* __rest
   double2* ss = sph + n * TXO;         // n x TXO (dentime)
   const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
   if (dentime)
-    for (int e = tid; e < n * n; e += TXO * NYO) sinv[e] = inv[e];
+    for (int e = tid; e < n * n; e += TXO * blockDim.y) sinv[e] = inv[e];
   const long long x = blockIdx.x * (long long)TXO + lx;
   const bool ok = x < G;
-  for (int k = ty; k < n; k += NYO) sph[k * TXO + lx] = ok ? phi[(long long)k * G + x] : make_double2(0.0, 0.0);
+  for (int k = ty; k < n; k += blockDim.y) sph[k * TXO + lx] = ok ? phi[(long long)k * G + x] : make_double2(0.0, 0.0);
   __syncthreads();
   if (ok) {
-    for (int ii = ty; ii < ni; ii += NYO) {
+    for (int ii = ty; ii < ni; ii += blockDim.y) {
       double2 a = acc_in ? acc_in[(long long)ii * G + x] : make_double2(0.0, 0.0);
       const double2* Vi = V + (long long)n * ii * G + x;  // V(x,k,i): column k + n*ii
 #pragma unroll 4
@@ -83,7 +82,7 @@ __global__ void __launch_bounds__(TXO * NYO) redpot_kernel(const double2* __rest
   if (!dentime) return;
   __syncthreads();
   if (!ok) return;
-  for (int i = ty; i < n; i += NYO) {
+  for (int i = ty; i < n; i += blockDim.y) {
     double2 a = make_double2(0.0, 0.0);
     for (int j = 0; j < n; ++j) cfma(a, ss[j * TXO + lx], sinv[j + n * i]);
     out[(long long)i * G + x] = cmul(timefac, a);
@@ -91,23 +90,23 @@ __global__ void __launch_bounds__(TXO * NYO) redpot_kernel(const double2* __rest
 }
 
 // partial[blk][j + n*i] = sum_{x in blk} conj(P_j(x)) T_i(x); block blk covers
-// DCH consecutive points, warp w the rows j = w, w + NYO, ...
+// DCH consecutive points, warp w the rows j = w, w + (warps per block), ...
 constexpr int DCH = 128;
-__global__ void __launch_bounds__(TXO * NYO) dots_kernel(const double2* __restrict__ Pm,
+__global__ void __launch_bounds__(TXO * kMaxOrbRhs) dots_kernel(const double2* __restrict__ Pm,
                                                          const double2* __restrict__ Tm, int n, long long G,
                                                          double2* __restrict__ partial) {
   extern __shared__ double2 rsm[];
   double2* tt = rsm;  // n x DCH
   const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
   const long long x0 = blockIdx.x * (long long)DCH;
-  for (int e = tid; e < n * DCH; e += TXO * NYO) {
+  for (int e = tid; e < n * DCH; e += TXO * blockDim.y) {
     const int i = e / DCH, k = e % DCH;
     const long long x = x0 + k;
     tt[e] = x < G ? Tm[(long long)i * G + x] : make_double2(0.0, 0.0);
   }
   __syncthreads();
   const int nn = n * n;
-  for (int j = ty; j < n; j += NYO) {
+  for (int j = ty; j < n; j += blockDim.y) {
     double2 pv[DCH / TXO];
 #pragma unroll
     for (int r = 0; r < DCH / TXO; ++r) {
@@ -148,7 +147,7 @@ __global__ void __launch_bounds__(128) dots_reduce_kernel(const double2* __restr
 }
 
 // out(x,i) = T(x,i) - sum_j P_j(x) D(j,i)
-__global__ void __launch_bounds__(TXO * NYO) project_kernel(const double2* __restrict__ Tm,
+__global__ void __launch_bounds__(TXO * kMaxOrbRhs) project_kernel(const double2* __restrict__ Tm,
                                                             const double2* __restrict__ Pm,
                                                             const double2* __restrict__ D, int n, long long G,
                                                             double2* __restrict__ out) {
@@ -156,13 +155,13 @@ __global__ void __launch_bounds__(TXO * NYO) project_kernel(const double2* __res
   double2* sd = rsm;            // n*n
   double2* sp = rsm + n * n;    // n x TXO
   const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
-  for (int e = tid; e < n * n; e += TXO * NYO) sd[e] = D[e];
+  for (int e = tid; e < n * n; e += TXO * blockDim.y) sd[e] = D[e];
   const long long x = blockIdx.x * (long long)TXO + lx;
   const bool ok = x < G;
-  for (int j = ty; j < n; j += NYO) sp[j * TXO + lx] = ok ? Pm[(long long)j * G + x] : make_double2(0.0, 0.0);
+  for (int j = ty; j < n; j += blockDim.y) sp[j * TXO + lx] = ok ? Pm[(long long)j * G + x] : make_double2(0.0, 0.0);
   __syncthreads();
   if (!ok) return;
-  for (int i = ty; i < n; i += NYO) {
+  for (int i = ty; i < n; i += blockDim.y) {
     double2 a = make_double2(0.0, 0.0);
     for (int j = 0; j < n; ++j) cfma(a, sp[j * TXO + lx], sd[j + n * i]);
     out[(long long)i * G + x] = csub(Tm[(long long)i * G + x], a);
@@ -171,7 +170,7 @@ __global__ void __launch_bounds__(TXO * NYO) project_kernel(const double2* __res
 
 // out(x,i) = T(x,i) - sum_j P_j(x) (M1(j,i) + M2(j,i)) - sum_j X_j(x) D2(j,i)
 // (the projector and projector-derivative terms of the orbital Jacobian)
-__global__ void __launch_bounds__(TXO * NYO) jac_combine_kernel(const double2* __restrict__ Tm,
+__global__ void __launch_bounds__(TXO * kMaxOrbRhs) jac_combine_kernel(const double2* __restrict__ Tm,
                                                                 const double2* __restrict__ Pm,
                                                                 const double2* __restrict__ M1,
                                                                 const double2* __restrict__ M2,
@@ -184,19 +183,19 @@ __global__ void __launch_bounds__(TXO * NYO) jac_combine_kernel(const double2* _
   double2* sp = sd + n * n;        // n x TXO
   double2* sx = sp + n * TXO;      // n x TXO
   const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
-  for (int e = tid; e < n * n; e += TXO * NYO) {
+  for (int e = tid; e < n * n; e += TXO * blockDim.y) {
     sm[e] = cadd(M1[e], M2[e]);
     sd[e] = D2[e];
   }
   const long long x = blockIdx.x * (long long)TXO + lx;
   const bool ok = x < G;
-  for (int j = ty; j < n; j += NYO) {
+  for (int j = ty; j < n; j += blockDim.y) {
     sp[j * TXO + lx] = ok ? Pm[(long long)j * G + x] : make_double2(0.0, 0.0);
     sx[j * TXO + lx] = ok ? Xm[(long long)j * G + x] : make_double2(0.0, 0.0);
   }
   __syncthreads();
   if (!ok) return;
-  for (int i = ty; i < n; i += NYO) {
+  for (int i = ty; i < n; i += blockDim.y) {
     double2 a = make_double2(0.0, 0.0);
     for (int j = 0; j < n; ++j) {
       cfma(a, sp[j * TXO + lx], sm[j + n * i]);
@@ -236,7 +235,9 @@ int rhs_attrs() {
   return SINCGPU_OK;
 }
 
-const dim3 kTile(TXO, NYO);
+// one warp per orbital (n <= 32): every warp of a block has the same share of
+// the per-orbital loops
+dim3 tile_for(int n) { return dim3(TXO, (unsigned)std::max(1, std::min(n, kMaxOrbRhs))); }
 
 size_t smem_mix(int n) { return sizeof(double2) * ((size_t)n * n + (size_t)n * TXO); }
 size_t smem_redpot(int n) { return sizeof(double2) * ((size_t)n * n + 2 * (size_t)n * TXO); }
@@ -245,7 +246,7 @@ size_t smem_jac(int n) { return sizeof(double2) * (2 * (size_t)n * n + 2 * (size
 
 int launch_dots(Ctx& c, const double2* P, const double2* T, double2* D, double2* part) {
   const int n = c.nspf, nb = ceil_div(c.G, DCH);
-  dots_kernel<<<nb, kTile, smem_dots(n), c.stream>>>(P, T, n, c.G, part);
+  dots_kernel<<<nb, tile_for(n), smem_dots(n), c.stream>>>(P, T, n, c.G, part);
   SG_LAUNCHED();
   dots_reduce_kernel<<<n * n, 128, 0, c.stream>>>(part, nb, n * n, D);
   SG_LAUNCHED();
@@ -266,7 +267,7 @@ int orbital_mix(Ctx& c, const double2* in, const double2* mat, double2* out) {
   const int n = c.nspf;
   SG_CHECK(n <= kMaxOrbRhs, SINCGPU_ERANGE, "at most %d orbitals", kMaxOrbRhs);
   SG_TRY(rhs_attrs());
-  mix_kernel<<<ceil_div(c.G, TXO), kTile, smem_mix(n), c.stream>>>(in, mat, n, c.G, out);
+  mix_kernel<<<ceil_div(c.G, TXO), tile_for(n), smem_mix(n), c.stream>>>(in, mat, n, c.G, out);
   SG_LAUNCHED();
   return SINCGPU_OK;
 }
@@ -276,7 +277,7 @@ int jac_combine(Ctx& c, const double2* T, const double2* P, const double2* M1, c
   const int n = c.nspf;
   SG_CHECK(n <= kMaxOrbRhs, SINCGPU_ERANGE, "at most %d orbitals", kMaxOrbRhs);
   SG_TRY(rhs_attrs());
-  jac_combine_kernel<<<ceil_div(c.G, TXO), kTile, smem_jac(n), c.stream>>>(T, P, M1, M2, X, D2, n, c.G, out);
+  jac_combine_kernel<<<ceil_div(c.G, TXO), tile_for(n), smem_jac(n), c.stream>>>(T, P, M1, M2, X, D2, n, c.G, out);
   SG_LAUNCHED();
   return SINCGPU_OK;
 }
@@ -294,7 +295,7 @@ int mult_reducedpot_range(Ctx& c, const double2* phi, const double2* redpot, int
   SG_CHECK(n <= kMaxOrbRhs, SINCGPU_ERANGE, "at most %d orbitals", kMaxOrbRhs);
   SG_TRY(rhs_attrs());
   ProfScope ps(c, ST_RHS_REDPOT);
-  redpot_kernel<<<ceil_div(c.G, TXO), kTile, smem_redpot(n), c.stream>>>(
+  redpot_kernel<<<ceil_div(c.G, TXO), tile_for(n), smem_redpot(n), c.stream>>>(
       phi, redpot, nullptr, nullptr, make_double2(1, 0), n, i0, ni, 0, c.G, out);
   SG_LAUNCHED();
   return SINCGPU_OK;
@@ -322,21 +323,21 @@ int actreduced(Ctx& c, const double2* phi, const double2* proj, const double2* d
   const int bt = ceil_div(G, TXO);
   {
     ProfScope ps(c, ST_RHS_MIX);
-    mix_kernel<<<bt, kTile, smem_mix(n), c.stream>>>(phi, denmat, n, G, Y);
+    mix_kernel<<<bt, tile_for(n), smem_mix(n), c.stream>>>(phi, denmat, n, G, Y);
     SG_LAUNCHED();
   }
   SG_TRY(mult_ke(c, Y, S, n, true, zfield));
   double2* dst = projflag == 1 ? T : out;
   {
     ProfScope ps(c, ST_RHS_REDPOT);
-    redpot_kernel<<<bt, kTile, smem_redpot(n), c.stream>>>(phi, redpot, S, invdenmat, timefac, n, 0, n,
+    redpot_kernel<<<bt, tile_for(n), smem_redpot(n), c.stream>>>(phi, redpot, S, invdenmat, timefac, n, 0, n,
                                                            dentimeflag ? 1 : 0, G, dst);
     SG_LAUNCHED();
   }
   if (projflag == 1) {
     ProfScope ps(c, ST_RHS_PROJ);
     SG_TRY(launch_dots(c, proj, T, D, part));
-    project_kernel<<<bt, kTile, smem_mix(n), c.stream>>>(T, proj, D, n, G, out);
+    project_kernel<<<bt, tile_for(n), smem_mix(n), c.stream>>>(T, proj, D, n, G, out);
     SG_LAUNCHED();
   }
   return SINCGPU_OK;
