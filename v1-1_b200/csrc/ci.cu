@@ -241,63 +241,85 @@ __global__ void __launch_bounds__(128) rdm_gather_kernel(const long long* __rest
   if (lane == 0) out[e] = acc;
 }
 
-// Fast path of the regularised inverse: Gauss-Jordan with partial pivoting (one
-// warp, lane r owns row r).  When every singular value is far above the
-// regularisation threshold the SVD formula is the plain inverse, and
-// sigma_min >= 1/||A^-1||_F certifies that; need_svd is set otherwise.
-__global__ void __launch_bounds__(32) inverse_gj_kernel(const double2* __restrict__ A_in, int n,
-                                                        double safe_sigma, double2* __restrict__ inv,
-                                                        int* __restrict__ need_svd) {
+// Fast path of the regularised inverse: Gauss-Jordan with partial pivoting on
+// [A | I] (n <= 32) by one CTA of 256 threads: warp 0 finds the pivot (largest
+// modulus, lowest row on ties), then the row swap, the pivot-row scaling and the
+// elimination are spread over all threads (one element each, n * 2n elements).
+// Same arithmetic per element as a one-row-per-lane elimination.  When every
+// singular value is far above the regularisation threshold the SVD formula is
+// the plain inverse, and sigma_min >= 1/||A^-1||_F certifies that; need_svd is
+// set otherwise.
+__global__ void __launch_bounds__(256) inverse_gj_kernel(const double2* __restrict__ A_in, int n,
+                                                         double safe_sigma, double2* __restrict__ inv,
+                                                         int* __restrict__ need_svd) {
   __shared__ double2 M[32][65];
-  const int r = threadIdx.x;
-  for (int j = 0; j < 2 * n; ++j)
-    if (r < n) M[r][j] = j < n ? A_in[r + n * j] : make_double2(j - n == r ? 1.0 : 0.0, 0.0);
-  __syncwarp();
-  bool singular = false;
+  __shared__ double2 fcol[32];
+  __shared__ int piv, sing;
+  __shared__ double fro_part[8];
+  const int tid = threadIdx.x, n2 = 2 * n;
+  for (int e = tid; e < n * n2; e += 256) {
+    const int r = e / n2, j = e - r * n2;
+    M[r][j] = j < n ? A_in[r + n * j] : make_double2(j - n == r ? 1.0 : 0.0, 0.0);
+  }
+  if (tid == 0) sing = 0;
+  __syncthreads();
   for (int k = 0; k < n; ++k) {
-    double mag = (r >= k && r < n) ? M[r][k].x * M[r][k].x + M[r][k].y * M[r][k].y : -1.0;
-    int arg = r;
-    for (int o = 16; o > 0; o >>= 1) {  // argmax, lowest row on ties
-      double m2 = __shfl_xor_sync(0xffffffffu, mag, o);
-      int a2 = __shfl_xor_sync(0xffffffffu, arg, o);
-      if (m2 > mag || (m2 == mag && a2 < arg)) {
-        mag = m2;
-        arg = a2;
+    if (tid < 32) {
+      const int r = tid;
+      double mag = (r >= k && r < n) ? M[r][k].x * M[r][k].x + M[r][k].y * M[r][k].y : -1.0;
+      int arg = r;
+      for (int o = 16; o > 0; o >>= 1) {  // argmax, lowest row on ties
+        const double m2 = __shfl_xor_sync(0xffffffffu, mag, o);
+        const int a2 = __shfl_xor_sync(0xffffffffu, arg, o);
+        if (m2 > mag || (m2 == mag && a2 < arg)) {
+          mag = m2;
+          arg = a2;
+        }
+      }
+      if (r == 0) {
+        piv = arg;
+        if (mag <= 0.0) sing = 1;
       }
     }
-    if (mag <= 0.0) {
-      singular = true;
-      break;
-    }
-    if (arg != k)  // arg is warp-uniform after the butterfly
-      for (int j = r; j < 2 * n; j += 32) {
-        double2 t = M[k][j];
+    __syncthreads();
+    if (sing) break;
+    const int arg = piv;
+    if (arg != k)
+      for (int j = tid; j < n2; j += 256) {
+        const double2 t = M[k][j];
         M[k][j] = M[arg][j];
         M[arg][j] = t;
       }
-    __syncwarp();
-    const double2 piv = M[k][k];
-    const double pm = piv.x * piv.x + piv.y * piv.y;
-    const double2 pinv = make_double2(piv.x / pm, -piv.y / pm);
-    __syncwarp();
-    if (r == k)
-      for (int j = 0; j < 2 * n; ++j) M[k][j] = cmul(M[k][j], pinv);
-    __syncwarp();
-    if (r < n && r != k) {
-      const double2 f = M[r][k];
-      for (int j = 0; j < 2 * n; ++j) M[r][j] = csub(M[r][j], cmul(f, M[k][j]));
+    __syncthreads();
+    const double2 pv = M[k][k];
+    const double pm = pv.x * pv.x + pv.y * pv.y;
+    const double2 pinv = make_double2(pv.x / pm, -pv.y / pm);
+    if (tid < n) fcol[tid] = M[tid][k];
+    __syncthreads();
+    for (int j = tid; j < n2; j += 256) M[k][j] = cmul(M[k][j], pinv);
+    __syncthreads();
+    for (int e = tid; e < n * n2; e += 256) {
+      const int r = e / n2, j = e - r * n2;
+      if (r != k) M[r][j] = csub(M[r][j], cmul(fcol[r], M[k][j]));
     }
-    __syncwarp();
+    __syncthreads();
   }
   double fro = 0.0;
-  if (r < n && !singular)
-    for (int j = 0; j < n; ++j) {
-      double2 v = M[r][n + j];
+  if (!sing)
+    for (int e = tid; e < n * n; e += 256) {
+      const int r = e % n, j = e / n;  // column-major output
+      const double2 v = M[r][n + j];
       fro += v.x * v.x + v.y * v.y;
       inv[r + n * j] = v;
     }
   for (int o = 16; o > 0; o >>= 1) fro += __shfl_xor_sync(0xffffffffu, fro, o);
-  if (r == 0) *need_svd = (singular || !(fro * safe_sigma * safe_sigma < 1.0)) ? 1 : 0;
+  if ((tid & 31) == 0) fro_part[tid >> 5] = fro;
+  __syncthreads();
+  if (tid == 0) {
+    double f = 0.0;
+    for (int w = 0; w < 8; ++w) f += fro_part[w];
+    *need_svd = (sing || !(f * safe_sigma * safe_sigma < 1.0)) ? 1 : 0;
+  }
 }
 
 // Regularised inverse of an n x n complex matrix by one-sided (Hestenes) Jacobi
@@ -340,7 +362,7 @@ int ci_denmat(Ctx& c, const double2* avec, double2* denmat, double2* invdenmat, 
     SG_TRY(c.ws_ci2.ensure(sizeof(double2) * n * n + 256));
     int* flag = (int*)((char*)c.ws_ci2.ptr + sizeof(double2) * n * n);
     // plain inverse is the SVD formula when sigma_min >= 1e-6 >> denreg
-    inverse_gj_kernel<<<1, 32, 0, c.stream>>>(denmat, n, std::max(1e-6, 1e4 * denreg), invdenmat, flag);
+    inverse_gj_kernel<<<1, 256, 0, c.stream>>>(denmat, n, std::max(1e-6, 1e4 * denreg), invdenmat, flag);
     SG_LAUNCHED();
     invmatsmooth_kernel<<<1, 32, 0, c.stream>>>(denmat, n, denreg, invdenmat, flag);
     SG_LAUNCHED();
