@@ -6,6 +6,7 @@
 #include <vector>
 #include <string>
 #include "context.hpp"
+#include "fft_lengths.h"
 #include "../../include/sincgpu.h"
 
 namespace sincgpu {
@@ -209,6 +210,7 @@ static int ctx_common(sincgpu_ctx* h, int numpoints, double spacing, int numspf,
   c.nspf = numspf;
   c.device = device;
   SG_CUDA(cudaSetDevice(device));
+  SG_TRY(upload_const_roots(device));
   SG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
   c.own_stream = true;
   c.bind_workspaces();

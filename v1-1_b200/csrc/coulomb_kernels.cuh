@@ -395,12 +395,6 @@ int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2*
   return SINCGPU_OK;
 }
 
-// Supported padded lengths (P, P1, P2); the plan picks the smallest P >= 2N-1.
-#define SINCGPU_FFT_LENGTHS(X) \
-  X(16, 4, 4) X(20, 5, 4) X(24, 6, 4) X(27, 9, 3) X(32, 8, 4) X(36, 6, 6) X(42, 7, 6) \
-  X(48, 8, 6) X(54, 9, 6) X(64, 8, 8) X(72, 9, 8) X(81, 9, 9) X(90, 10, 9) X(100, 10, 10) \
-  X(108, 12, 9) X(120, 12, 10) X(126, 14, 9) X(144, 12, 12) X(162, 18, 9) X(180, 15, 12) \
-  X(192, 16, 12) X(216, 18, 12) X(240, 16, 15) X(256, 16, 16)
 
 #define SINCGPU_DECLARE_LAUNCH(P, A, B)                                                             \
   extern template int coul_launch<A, B, double2>(Ctx&, const CoulArgs<double2>&, int, bool,         \

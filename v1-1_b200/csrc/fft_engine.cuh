@@ -28,9 +28,10 @@ struct FftPlan {
 };
 
 // roots[m] = exp(-2*pi*i*m/P), m in [0,P).  Inverse transforms use conj(roots).
-template <bool INV, class C>
-__device__ __forceinline__ C root(const C* roots, int m) {
-  C w = roots[m];
+// `roots` is a shared-memory table or a constant-memory accessor (fft_reg.cuh).
+template <bool INV, class RT>
+__device__ __forceinline__ auto root(const RT& roots, int m) {
+  auto w = roots[m];
   if (INV) w.y = -w.y;
   return w;
 }
@@ -54,7 +55,8 @@ struct Butterfly;
 
 template <bool INV, class C>
 struct Butterfly<2, INV, C> {
-  __device__ __forceinline__ static void run(C* a, const C*, int) {
+  template <class RT>
+  __device__ __forceinline__ static void run(C* a, const RT&, int) {
     C t0 = a[0], t1 = a[1];
     a[0] = cadd(t0, t1);
     a[1] = csub(t0, t1);
@@ -63,7 +65,8 @@ struct Butterfly<2, INV, C> {
 
 template <bool INV, class C>
 struct Butterfly<3, INV, C> {
-  __device__ __forceinline__ static void run(C* a, const C* roots, int P) {
+  template <class RT>
+  __device__ __forceinline__ static void run(C* a, const RT& roots, int P) {
     using Re = typename CplxTraits<C>::Real;
     // W_3 = exp(-+2 pi i/3) = (-1/2, s),  s = -+ sin(2 pi/3)
     const Re s = INV ? -roots[P / 3].y : roots[P / 3].y;
@@ -83,7 +86,8 @@ struct Butterfly<3, INV, C> {
 
 template <bool INV, class C>
 struct Butterfly<4, INV, C> {
-  __device__ __forceinline__ static void run(C* a, const C*, int) {
+  template <class RT>
+  __device__ __forceinline__ static void run(C* a, const RT&, int) {
     C s02 = cadd(a[0], a[2]), d02 = csub(a[0], a[2]);
     C s13 = cadd(a[1], a[3]), d13 = csub(a[1], a[3]);
     C rot = mul_mi<INV>(d13);
@@ -97,7 +101,8 @@ struct Butterfly<4, INV, C> {
 // odd prime radices: direct DFT with the symmetric pairing t <-> r-t
 template <int R, bool INV, class C>
 struct ButterflyOdd {
-  __device__ __forceinline__ static void run(C* a, const C* roots, int P) {
+  template <class RT>
+  __device__ __forceinline__ static void run(C* a, const RT& roots, int P) {
     const int step = P / R;
     C sp[(R - 1) / 2], sm[(R - 1) / 2];
 #pragma unroll

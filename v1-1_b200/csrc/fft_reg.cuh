@@ -12,9 +12,58 @@
 // roots[m] = exp(-2 pi i m / P) in shared memory.  The complex type C is double2
 // (the FP64 form) or float2 (the FP32 precision form).
 #pragma once
+#include <cmath>
+#include <vector>
 #include "fft_engine.cuh"
+#include "fft_lengths.h"
 
 namespace sincgpu {
+
+// Twiddle tables of every FFT length in constant memory (this translation unit's
+// copy): the sub-transforms' twiddles have compile-time indices, so they become
+// constant-bank operands instead of shared-memory loads.  The table holds the
+// same values as the contexts' shared-memory roots (long-double cos/sin rounded to
+// double; the FP32 table rounds those doubles).
+namespace {
+__constant__ double2 c_roots64[root_total()];
+__constant__ float2 c_roots32[root_total()];
+
+int upload_roots_here() {
+  std::vector<double2> h64(root_total());
+  std::vector<float2> h32(root_total());
+  for (int i = 0; i < kNumFftLens; ++i) {
+    const int P = kFftLens[i], o = root_offset(P);
+    for (int m = 0; m < P; ++m) {
+      const long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)P;
+      h64[o + m] = make_double2((double)cosl(ang), (double)sinl(ang));
+      h32[o + m] = make_float2((float)h64[o + m].x, (float)h64[o + m].y);
+    }
+  }
+  if (cudaMemcpyToSymbol(c_roots64, h64.data(), sizeof(double2) * h64.size()) != cudaSuccess) return 1;
+  if (cudaMemcpyToSymbol(c_roots32, h32.data(), sizeof(float2) * h32.size()) != cudaSuccess) return 1;
+  return 0;
+}
+const int c_roots_registered = register_const_roots(&upload_roots_here);
+
+template <class C>
+struct CRootTable;
+template <>
+struct CRootTable<double2> {
+  __device__ __forceinline__ static double2 at(int i) { return c_roots64[i]; }
+};
+template <>
+struct CRootTable<float2> {
+  __device__ __forceinline__ static float2 at(int i) { return c_roots32[i]; }
+};
+}  // namespace
+
+// roots of length P from constant memory: ConstRoots<P, C>{}[m] = exp(-2 pi i m / P)
+template <int P, class C>
+struct ConstRoots {
+  static constexpr int kOff = root_offset(P);
+  static_assert(kOff >= 0, "FFT length missing from the twiddle table");
+  __device__ __forceinline__ C operator[](int m) const { return CRootTable<C>::at(kOff + m); }
+};
 
 constexpr int first_radix(int m) {
   return m % 4 == 0 ? 4 : (m % 2 == 0 ? 2 : (m % 3 == 0 ? 3 : (m % 5 == 0 ? 5 : 7)));
@@ -24,7 +73,8 @@ constexpr int first_radix(int m) {
 template <int M, int L, bool INV, class C>
 struct RegFFT {
   static constexpr int R = first_radix(M / L);
-  __device__ __forceinline__ static void run(C (&a)[M], const C* roots, int P) {
+  template <class RT>
+  __device__ __forceinline__ static void run(C (&a)[M], const RT& roots, int P) {
     C b[M];
     const int rstep = P / M;
 #pragma unroll
@@ -48,7 +98,8 @@ struct RegFFT {
 };
 template <int M, bool INV, class C>
 struct RegFFT<M, M, INV, C> {
-  __device__ __forceinline__ static void run(C (&)[M], const C*, int) {}
+  template <class RT>
+  __device__ __forceinline__ static void run(C (&)[M], const RT&, int) {}
 };
 
 // ex: exchange buffer for TL lines.  Element e of line l sits at ex[e*TL + l]
@@ -67,7 +118,7 @@ __device__ __forceinline__ void dft_in_to_out(C (&a)[P1], C (&b)[P2], int s, int
                                               const C* roots) {
   constexpr int P = P1 * P2;
   if (s < P2) {
-    RegFFT<P1, 1, INV, C>::run(a, roots, P);
+    RegFFT<P1, 1, INV, C>::run(a, ConstRoots<P, C>{}, P);
 #pragma unroll
     for (int k1 = 0; k1 < P1; ++k1) {
       C v = a[k1];
@@ -79,7 +130,7 @@ __device__ __forceinline__ void dft_in_to_out(C (&a)[P1], C (&b)[P2], int s, int
   if (s < P1) {
 #pragma unroll
     for (int n2 = 0; n2 < P2; ++n2) b[n2] = ex[ex_at<P, ROW>(s * P2 + n2, l, TL)];
-    RegFFT<P2, 1, INV, C>::run(b, roots, P);
+    RegFFT<P2, 1, INV, C>::run(b, ConstRoots<P, C>{}, P);
   }
   __syncthreads();
 }
@@ -90,7 +141,7 @@ __device__ __forceinline__ void dft_out_to_in(C (&b)[P2], C (&a)[P1], int s, int
                                               const C* roots) {
   constexpr int P = P1 * P2;
   if (s < P1) {
-    RegFFT<P2, 1, INV, C>::run(b, roots, P);
+    RegFFT<P2, 1, INV, C>::run(b, ConstRoots<P, C>{}, P);
 #pragma unroll
     for (int m2 = 0; m2 < P2; ++m2) {
       C v = b[m2];
@@ -102,7 +153,7 @@ __device__ __forceinline__ void dft_out_to_in(C (&b)[P2], C (&a)[P1], int s, int
   if (s < P2) {
 #pragma unroll
     for (int k1 = 0; k1 < P1; ++k1) a[k1] = ex[ex_at<P, ROW>(s * P1 + k1, l, TL)];
-    RegFFT<P1, 1, INV, C>::run(a, roots, P);
+    RegFFT<P1, 1, INV, C>::run(a, ConstRoots<P, C>{}, P);
   }
   __syncthreads();
 }

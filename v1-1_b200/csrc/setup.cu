@@ -9,9 +9,34 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <mutex>
+#include <set>
 #include "context.hpp"
+#include "fft_lengths.h"
 
 namespace sincgpu {
+
+static std::vector<int (*)()>& root_uploaders() {
+  static std::vector<int (*)()> v;
+  return v;
+}
+
+int register_const_roots(int (*upload)()) {
+  root_uploaders().push_back(upload);
+  return 1;
+}
+
+int upload_const_roots(int device) {
+  static std::mutex mu;
+  static std::set<int> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count(device)) return SINCGPU_OK;
+  for (int (*f)() : root_uploaders())
+    SG_CHECK(f() == 0, SINCGPU_ECUDA, "upload of the constant twiddle tables failed");
+  done.insert(device);
+  return SINCGPU_OK;
+}
+
 
 static const double kPi = 3.14159265358979323846264338327950288;
 
