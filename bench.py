@@ -577,8 +577,8 @@ def secondary_rates(proj, torch, stream, flush, phi, den, inv, red, out, mat, av
 # in the running step the pass intermediates are L2 hits.
 TRAFFIC = {
     ("coul_fwd_x", 41, 10): 6629888, ("coul_fwd_y", 41, 10): 13083392, ("coul_z", 41, 10): 38650880,
-    ("coul_inv_y", 41, 10): 30139904, ("coul_inv_x", 41, 10): 15265024, ("twoe_gemm", 41, 10): 71862528,
-    ("rp_gemm", 41, 10): 164237056, ("rhs_redpot", 41, 10): 135516416, ("ke_xy", 41, 10): 12162048,
+    ("coul_inv_y", 41, 10): 30139904, ("coul_inv_x", 41, 10): 15265024, ("twoe_gemm", 41, 10): 71800000,
+    ("rp_gemm", 41, 10): 168300000, ("rhs_redpot", 41, 10): 135516416, ("ke_xy", 41, 10): 12162048,
     ("ke_z", 41, 10): 22084352,
 }
 
