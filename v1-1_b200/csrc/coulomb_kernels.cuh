@@ -83,7 +83,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
     a[n1] = cvt<C>(v);
   }
   __syncthreads();
-  dft_in_to_out<P1, P2, false, C, true>(a, b, s, l, TL, ex, roots);
+  dft_in_to_out<P1, P2, false, C, true, false>(a, b, s, l, TL, ex, roots);
   if (row && s < P1) {
     C* dst = ca.W1 + ((long long)p * N * N + f) * P;
 #pragma unroll
@@ -111,7 +111,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
     a[n1] = (col && s < P2 && y < N) ? src[(long long)y * P] : CplxTraits<C>::make(0.0, 0.0);
   }
   __syncthreads();
-  dft_in_to_out<P1, P2, false, C>(a, b, s, l, TL, ex, roots);
+  dft_in_to_out<P1, P2, false, C, false, false>(a, b, s, l, TL, ex, roots);
   if (col && s < P1) {
     C* dst = ca.W2 + ((long long)p * N + z) * P * P + kx;
 #pragma unroll
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_z<C>(P1 * P2))
 #pragma unroll
     for (int k2 = 0; k2 < P2; ++k2) b[k2] = cmul(b[k2], kh[(long long)(s + P1 * k2) * zs]);
   }
-  dft_out_to_in<P1, P2, true, C>(b, a, s, l, TL, ex, roots);
+  dft_out_to_in<P1, P2, true, C, false, false>(b, a, s, l, TL, ex, roots);
   if (col && s < P2) {
 #pragma unroll
     for (int m1 = 0; m1 < P1; ++m1) {
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_ztma<C>(P1 * P
 #pragma unroll
       for (int k2 = 0; k2 < P2; ++k2) bb[k2] = CplxTraits<C>::make(bb[k2].x * kh[k2], bb[k2].y * kh[k2]);
     }
-    dft_out_to_in<P1, P2, true, C>(bb, a, s, l, TL, ex, roots);
+    dft_out_to_in<P1, P2, true, C, false, false>(bb, a, s, l, TL, ex, roots);
     if (col && s < P2) {
       C* base = ca.W2 + (long long)p * N * zs + f;
 #pragma unroll
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   for (int n1 = 0; n1 < P1; ++n1)
     a[n1] = (col && s < P2) ? src[(long long)(s + P2 * n1) * P] : CplxTraits<C>::make(0.0, 0.0);
   __syncthreads();
-  dft_in_to_out<P1, P2, true, C>(a, b, s, l, TL, ex, roots);
+  dft_in_to_out<P1, P2, true, C, false, false>(a, b, s, l, TL, ex, roots);
   if (col && s < P1) {
     C* dst = ca.W1 + ((long long)p * N + z) * N * P + kx;
 #pragma unroll
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   for (int n1 = 0; n1 < P1; ++n1)
     a[n1] = (row && s < P2) ? src[s + P2 * n1] : CplxTraits<C>::make(0.0, 0.0);
   __syncthreads();
-  dft_in_to_out<P1, P2, true, C, true>(a, b, s, l, TL, ex, roots);
+  dft_in_to_out<P1, P2, true, C, true, false>(a, b, s, l, TL, ex, roots);
   if (!(row && s < P1)) return;
   const long long G = ca.G;
   const long long g0 = (long long)f * N;

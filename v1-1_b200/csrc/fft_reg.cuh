@@ -113,7 +113,9 @@ __device__ __forceinline__ int ex_at(int e, int l, int TL) {
   return ROW ? l * (P + 1) + e : e * TL + l;
 }
 
-template <int P1, int P2, bool INV, class C, bool ROW = false>
+// TRAIL = false drops the closing barrier where the caller never writes the
+// exchange buffer again (or passes another barrier first).
+template <int P1, int P2, bool INV, class C, bool ROW = false, bool TRAIL = true>
 __device__ __forceinline__ void dft_in_to_out(C (&a)[P1], C (&b)[P2], int s, int l, int TL, C* ex,
                                               const C* roots) {
   constexpr int P = P1 * P2;
@@ -132,11 +134,11 @@ __device__ __forceinline__ void dft_in_to_out(C (&a)[P1], C (&b)[P2], int s, int
     for (int n2 = 0; n2 < P2; ++n2) b[n2] = ex[ex_at<P, ROW>(s * P2 + n2, l, TL)];
     RegFFT<P2, 1, INV, C>::run(b, ConstRoots<P, C>{}, P);
   }
-  __syncthreads();
+  if (TRAIL) __syncthreads();
 }
 
 // On entry b[] holds D_out (valid for s < P1); on exit a[] holds D_in (valid for s < P2).
-template <int P1, int P2, bool INV, class C, bool ROW = false>
+template <int P1, int P2, bool INV, class C, bool ROW = false, bool TRAIL = true>
 __device__ __forceinline__ void dft_out_to_in(C (&b)[P2], C (&a)[P1], int s, int l, int TL, C* ex,
                                               const C* roots) {
   constexpr int P = P1 * P2;
@@ -155,7 +157,7 @@ __device__ __forceinline__ void dft_out_to_in(C (&b)[P2], C (&a)[P1], int s, int
     for (int k1 = 0; k1 < P1; ++k1) a[k1] = ex[ex_at<P, ROW>(s * P1 + k1, l, TL)];
     RegFFT<P1, 1, INV, C>::run(a, ConstRoots<P, C>{}, P);
   }
-  __syncthreads();
+  if (TRAIL) __syncthreads();
 }
 
 }  // namespace sincgpu
