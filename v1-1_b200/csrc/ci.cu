@@ -184,12 +184,10 @@ int ci_spin_project(Ctx& c, double2* a) {
   SG_CHECK(s.attached && s.spin, SINCGPU_ESTATE, "no spin projectors attached (build them with sincgpu_walks_spin)");
   const int zb = s.nspinelim > 0 ? std::min(ceil_div(s.nspinelim, 256), 64) : 0;
   if (s.nspinsets + zb == 0) return SINCGPU_OK;
-  static bool attr = false;
-  if (!attr) {
-    SG_CUDA(cudaFuncSetAttribute(spin_project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(sizeof(double2) * 4096)));
-    attr = true;
-  }
+  // process-wide attribute, one fixed value, set once (thread-safe static init)
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      spin_project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(double2) * 4096));
+  SG_CUDA(attr);
   spin_project_kernel<<<s.nspinsets + zb, 256, sizeof(double2) * std::max(1, s.maxspinset), c.stream>>>(
       s.sp_set_off, s.sp_sets, s.sp_proj_off, s.sp_proj, s.nspinsets, s.sp_elim, s.nspinelim, a);
   SG_LAUNCHED();

@@ -156,12 +156,14 @@ int mult_ke(Ctx& c, const double2* in, double2* out, int howmany, bool extra, do
   SG_CHECK(smem <= 227 * 1024, SINCGPU_ERANGE, "kinetic kernel needs %zu bytes of shared memory (N=%d)",
            smem, N);
   SG_CHECK(howmany <= 65535, SINCGPU_ERANGE, "howmany %d too large", howmany);
-  static bool attr = false;
-  if (!attr) {
-    SG_CUDA(cudaFuncSetAttribute(ke_xy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    SG_CUDA(cudaFuncSetAttribute(ke_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    attr = true;
-  }
+  // process-wide attributes, one fixed value, set once (thread-safe static init)
+  static const cudaError_t attr = [] {
+    cudaError_t e = cudaFuncSetAttribute(ke_xy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(ke_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    return e;
+  }();
+  SG_CUDA(attr);
   {
     ProfScope ps(c, ST_KE_XY);
     ke_xy_kernel<<<dim3(N, howmany), 256, smem, c.stream>>>(in, out, ka);

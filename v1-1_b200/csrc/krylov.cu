@@ -298,12 +298,10 @@ __global__ void cscale_kernel(const double2* __restrict__ in, double2 s, int nc,
 int pade_expm(Ctx& c, const double* Hm, int mh, int mx, double t, int col, double* exph, double* Efull,
               double* gscratch, int* d_ns) {
   SG_CHECK(mx >= 1 && mx <= kMaxPade, SINCGPU_ERANGE, "Pade order %d outside [1,%d]", mx, kMaxPade);
-  static bool attr = false;
-  if (!attr) {
-    SG_CUDA(cudaFuncSetAttribute(kry_padm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(sizeof(double) * 5 * 64 * 64)));
-    attr = true;
-  }
+  // process-wide attribute, one fixed value, set once (thread-safe static init)
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      kry_padm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(double) * 5 * 64 * 64));
+  SG_CUDA(attr);
   const bool smem = mx <= 64;
   SG_CHECK(smem || gscratch, SINCGPU_EINVAL, "Pade order %d needs global scratch", mx);
   const size_t psmem = smem ? sizeof(double) * 5 * (size_t)mx * mx : 0;

@@ -224,14 +224,15 @@ namespace {
 
 // the kernels' shared-memory limit: one fixed value (race-free across threads)
 int rhs_attrs() {
-  static bool done = false;
-  if (done) return SINCGPU_OK;
-  SG_CUDA(cudaFuncSetAttribute(mix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax));
-  SG_CUDA(cudaFuncSetAttribute(redpot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax));
-  SG_CUDA(cudaFuncSetAttribute(dots_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax));
-  SG_CUDA(cudaFuncSetAttribute(project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax));
-  SG_CUDA(cudaFuncSetAttribute(jac_combine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax));
-  done = true;
+  static const cudaError_t attr = [] {
+    for (const void* k : {(const void*)mix_kernel, (const void*)redpot_kernel, (const void*)dots_kernel,
+                          (const void*)project_kernel, (const void*)jac_combine_kernel}) {
+      const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }();
+  SG_CUDA(attr);
   return SINCGPU_OK;
 }
 
