@@ -44,13 +44,27 @@ __global__ void __launch_bounds__(256) ke_xy_kernel(const double2* __restrict__ 
   double* Xi = Xr + n8 * S;    // n8 x S
   const int z = blockIdx.x, orb = blockIdx.y;
   const double2* src = in + (long long)orb * ka.G + (long long)z * N * N;
-  for (int i = threadIdx.x; i < n8 * S; i += blockDim.x) {
-    Ks[i] = ka.ketile[i];
-    int y = i / S, x = i - y * S;
-    double2 v = make_double2(0.0, 0.0);
-    if (y < N && x < N) v = src[y * N + x];
-    Xr[i] = v.x;
-    Xi[i] = v.y;
+  // staged in batches of 8 elements per thread: all 8 loads are in flight before
+  // the first shared-memory store
+  for (int i0 = threadIdx.x; i0 < n8 * S; i0 += 8 * blockDim.x) {
+    double kv[8];
+    double2 xv[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = i0 + r * blockDim.x;
+      const int y = i / S, x = i - y * S;
+      kv[r] = i < n8 * S ? ka.ketile[i] : 0.0;
+      xv[r] = (i < n8 * S && y < N && x < N) ? src[y * N + x] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = i0 + r * blockDim.x;
+      if (i < n8 * S) {
+        Ks[i] = kv[r];
+        Xr[i] = xv[r].x;
+        Xi[i] = xv[r].y;
+      }
+    }
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -101,13 +115,25 @@ __global__ void __launch_bounds__(256) ke_z_kernel(const double2* __restrict__ i
   const int y = blockIdx.x, orb = blockIdx.y;
   const long long NN = (long long)N * N;
   const double2* src = in + (long long)orb * ka.G + (long long)y * N;
-  for (int i = threadIdx.x; i < n8 * S; i += blockDim.x) {
-    Ks[i] = ka.ketile[i];
-    int zz = i / S, x = i - zz * S;
-    double2 v = make_double2(0.0, 0.0);
-    if (zz < N && x < N) v = src[zz * NN + x];
-    Xr[i] = v.x;
-    Xi[i] = v.y;
+  for (int i0 = threadIdx.x; i0 < n8 * S; i0 += 8 * blockDim.x) {
+    double kv[8];
+    double2 xv[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = i0 + r * blockDim.x;
+      const int zz = i / S, x = i - zz * S;
+      kv[r] = i < n8 * S ? ka.ketile[i] : 0.0;
+      xv[r] = (i < n8 * S && zz < N && x < N) ? src[zz * NN + x] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = i0 + r * blockDim.x;
+      if (i < n8 * S) {
+        Ks[i] = kv[r];
+        Xr[i] = xv[r].x;
+        Xi[i] = xv[r].y;
+      }
+    }
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
