@@ -13,6 +13,10 @@ namespace sincgpu {
 // context's stream): growing it neither synchronises the device nor stalls the
 // other contexts' streams, which a plain cudaFree would.  Growth is refused while
 // the owner stream is being captured into a graph.
+// Device bytes of Coulomb pass intermediates (W1 + W2) per pair chunk when the
+// chunk size is automatic.
+constexpr long long kCoulChunkBudget = 2LL << 30;
+
 struct Workspace {
   void* ptr = nullptr;
   size_t bytes = 0;

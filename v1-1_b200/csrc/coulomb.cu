@@ -14,8 +14,11 @@
 //   CZ : DFT along z, * khat, inverse DFT (P^2 columns, only z<N kept)
 //   CYI: inverse DFT along y              (N*P columns, only y<N kept)
 //   CXI: inverse DFT along x              (N^2 rows, only x<N kept) -> R
-// Pruned inputs/outputs never touch memory.  Pairs are processed in chunks
-// sized so that the intermediates W1 (N*N*P) and W2 (N*P*P) stay L2 resident.
+// Pruned inputs/outputs never touch memory.  Pairs are processed in chunks whose
+// intermediates W1 (N*N*P) and W2 (N*P*P) fit a 2 GB budget: the passes are
+// bound by FP64 issue and latency, not by HBM, so few launches over many pairs
+// beat L2-sized chunks (measured on the 41^3 / 10-orbital workload: 0.89 ms per
+// evaluation with 48 MB chunks of 7 pairs, 0.75 ms with one chunk of all 55).
 // The passes run in FP64 (double2) or, with the context option coulomb_fp32,
 // in FP32 (float2) with FP64 inputs and outputs.
 #include <algorithm>
@@ -113,7 +116,7 @@ static int coul_run_t(Ctx& c, const double2* src1, const double2* src2, const in
   const long long per_pair = (long long)sizeof(C) * ((long long)N * N * P + (long long)N * P * P);
   int chunk = c.coul_chunk;
   if (chunk <= 0) {
-    const long long budget = 48LL << 20;
+    const long long budget = kCoulChunkBudget;
     chunk = (int)std::max(1LL, budget / per_pair);
   }
   chunk = std::min(chunk, npair);

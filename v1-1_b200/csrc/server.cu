@@ -79,7 +79,7 @@ long long estimate_bytes(const Req& r) {
   b += 16 * G * n * (2 + 25);                 // orbitals (2 slots) + Krylov basis and Jacobian state
   b += 16 * G * n * n * 3;                    // reducedpot (2 slots) + scratch
   b += 8 * 2 * npair * G;                     // planar reduced potentials
-  b += 48ll << 20;                            // Coulomb W1/W2 chunk
+  b += std::min(sincgpu::kCoulChunkBudget, npair * 16 * (r.N * r.N * P + r.N * P * P));  // Coulomb W1/W2 chunk
   b += 16 * P * P * P;                        // kernel spectrum
   b += 16 * G * n * 6;                        // RHS temporaries
   const long long walks = nc * (long long)(r.numelec * r.nspf + r.numelec * r.numelec * r.nspf * r.nspf / 2);
