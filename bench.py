@@ -572,14 +572,14 @@ def secondary_rates(proj, torch, stream, flush, phi, den, inv, red, out, mat, av
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
-# ncu capture of workload B (41^3 grid, 10 orbitals), keyed by (stage, N, nspf).
-# ncu flushes L2 before each captured launch, so these are cold-cache figures:
-# in the running step the pass intermediates are L2 hits.
+# ncu capture of workload B (41^3 grid, 10 orbitals; one Coulomb launch per pass
+# covers all 55 pairs), keyed by (stage, N, nspf).  ncu flushes L2 before each
+# captured launch, so these are cold-cache figures.
 TRAFFIC = {
-    ("coul_fwd_x", 41, 10): 6629888, ("coul_fwd_y", 41, 10): 13083392, ("coul_z", 41, 10): 38650880,
-    ("coul_inv_y", 41, 10): 30139904, ("coul_inv_x", 41, 10): 15265024, ("twoe_gemm", 41, 10): 71800000,
-    ("rp_gemm", 41, 10): 168300000, ("rhs_redpot", 41, 10): 135516416, ("ke_xy", 41, 10): 12162048,
-    ("ke_z", 41, 10): 22084352,
+    ("coul_fwd_x", 41, 10): 70590000, ("coul_fwd_y", 41, 10): 300490000, ("coul_z", 41, 10): 426130000,
+    ("coul_inv_y", 41, 10): 323310000, ("coul_inv_x", 41, 10): 143240000, ("twoe_gemm", 41, 10): 72050000,
+    ("rp_gemm", 41, 10): 169050000, ("rhs_redpot", 41, 10): 136340000, ("ke_xy", 41, 10): 12170000,
+    ("ke_z", 41, 10): 22090000,
 }
 
 _DGEMM = {}

@@ -76,7 +76,8 @@ int sincgpu_fft_length(sincgpu_ctx* ctx);
  * "coulomb_fp32" (1: the Coulomb passes in FP32, the precision form);
  * "contract_tf32" (1: the reducedpot contraction on the tensor cores as 3xTF32
  * with FP32 accumulation, the precision form); "coul_tma" (the Coulomb z pass
- * with TMA-staged slabs: 1 on, 0 off, -1 automatic = on for FFT lengths >= 128). */
+ * with TMA-staged slabs: 1 on, 0 off, -1 automatic = off: the plain pass was
+ * faster at every measured length once whole pair lists go in one launch). */
 int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
 
 /* C(M x N, row-major) = A(M x K, row-major) * B(N x K, row-major)^T on the

@@ -179,7 +179,7 @@ struct Ctx {
   int coul_chunk = 0;   // pairs per pass sequence (0 = automatic)
   int coul_fp32 = 0;    // 1: Coulomb passes in FP32 (precision form), 0: FP64
   int contract_tf32 = 0;  // 1: reducedpot contraction as 3xTF32 on the tensor cores
-  int coul_tma = -1;      // TMA-staged persistent z pass: 1 on, 0 off, -1 automatic
+  int coul_tma = -1;      // TMA-staged persistent z pass: 1 on, 0 off, -1 automatic (off)
   int rp_dmma = 1;        // 1: FP64 reducedpot GEMM on the FP64 tensor cores (DMMA), 0: DFMA tiles
   int twoe_dmma = 1;      // 1: FP64 twoematel GEMM on the FP64 tensor cores (DMMA), 0: DFMA tiles
   Prof prof;

@@ -139,12 +139,13 @@ static int coul_run_t(Ctx& c, const double2* src1, const double2* src2, const in
   ca.npair_total = npair;
   // TMA-staged z pass: one map over the chunk's W2 (the last, shorter chunk
   // only addresses its first pairs)
-  // automatic choice: measured faster for the long lines of P >= 128 (162: z pass
-  // 9.9 -> 8.1 ms FP64, 4.8 -> 4.1 ms FP32 per evaluation of the 81^3 / 16-orbital
-  // workload) and slower at P = 81 (0.23 -> 0.25 ms), where fewer resident warps
-  // per SM cost more than the staging saves
+  // automatic choice: the plain pass.  With chunks of a few pairs the staged pass
+  // was faster for P >= 128 (162: 9.9 -> 8.1 ms per evaluation); with the
+  // whole-pair-list chunks the plain pass wins at every measured length (162:
+  // 4.8 vs 5.4 ms FP64, 2.1 vs 2.5 ms FP32; 81: 0.16 vs 0.18 ms), its three
+  // resident CTAs per SM hiding the W2 latency better than two staged ones
   CUtensorMap zmap;
-  const bool want_tma = c.coul_tma > 0 || (c.coul_tma < 0 && P >= 128);
+  const bool want_tma = c.coul_tma > 0;
   const bool use_tma = want_tma && make_zmap<C>(c, ca.W2, chunk, &zmap);
   int* err = nullptr;
   if (use_tma) {
