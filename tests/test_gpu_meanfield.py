@@ -123,6 +123,22 @@ def test_coulomb_tma_z_pass_matches_plain(h2):
     assert gpu.kernel_timeouts() == [0, 0]
 
 
+def test_pair_chunking_is_exact(h2):
+    """Each pair's Coulomb solve is independent of the others, so the pair-chunk
+    size (automatic: the whole list within a 2 GB budget) changes nothing: chunks
+    of 3 pairs give bitwise the same reduced potentials and twoematel."""
+    sysm, gpu = h2
+    phi = orc.seeded_orbitals(sysm, 10, seed=31)
+    mat0, red0 = gpu.call_twoe_matel00(phi)
+    gpu.set_option("coul_chunk", 3)
+    try:
+        mat3, red3 = gpu.call_twoe_matel00(phi)
+    finally:
+        gpu.set_option("coul_chunk", 0)
+    assert np.array_equal(red0, red3)
+    assert np.array_equal(mat0, mat3)
+
+
 def test_mult_ke(he, h2):
     for sysm, gpu in ((he[0], he[1]), h2):
         rng = np.random.default_rng(5)

@@ -182,6 +182,7 @@ struct Ctx {
   int coul_tma = -1;      // TMA-staged persistent z pass: 1 on, 0 off, -1 automatic (off)
   int rp_dmma = 1;        // 1: FP64 reducedpot GEMM on the FP64 tensor cores (DMMA), 0: DFMA tiles
   int twoe_dmma = 1;      // 1: FP64 twoematel GEMM on the FP64 tensor cores (DMMA), 0: DFMA tiles
+  int twoe_tile = 0;      // twoematel tile edge 16R: 0 = least padding, 2..9 = that R
   Prof prof;
 
   ~Ctx();

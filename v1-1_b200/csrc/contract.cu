@@ -301,6 +301,7 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
   int R = 2;
   for (int r = 2; r <= 9; ++r)
     if (ceil_div(M, 16 * r) * 16 * r <= ceil_div(M, 16 * R) * 16 * R) R = r;
+  if (c.twoe_tile >= 2 && c.twoe_tile <= 9) R = c.twoe_tile;
   const int TT = 16 * R;
   const int ntm = ceil_div(M, TT), ntn = ntm;
   const int ntiles = ntm * (ntm + 1) / 2;  // upper triangle
