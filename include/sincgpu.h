@@ -77,7 +77,11 @@ int sincgpu_fft_length(sincgpu_ctx* ctx);
  * "contract_tf32" (1: the reducedpot contraction on the tensor cores as 3xTF32
  * with FP32 accumulation, the precision form); "coul_tma" (the Coulomb z pass
  * with TMA-staged slabs: 1 on, 0 off, -1 automatic = off: the plain pass was
- * faster at every measured length once whole pair lists go in one launch). */
+ * faster at every measured length once whole pair lists go in one launch);
+ * "twoe_tile" (twoematel tile edge 16R: 0 = least padding, 2..9 = R);
+ * "orth_fused" (1: the orbital Arnoldi orthogonalisation of one Krylov step in
+ * one cooperative launch with bounded grid barriers, 0: one launch per dot,
+ * projection and norm; the results are bitwise the same). */
 int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
 
 /* C(M x N, row-major) = A(M x K, row-major) * B(N x K, row-major)^T on the

@@ -99,6 +99,26 @@ def test_expospfprop_state_over_calls(system):
     assert np.abs(out - ref).max() < 1e-10 * np.abs(ref).max()
 
 
+def test_orthogonalisation_fused_is_bitwise(system):
+    """The one-launch Arnoldi orthogonalisation (bounded grid barriers) gives the
+    same bits, step counts and saved state as the dot / projection / norm launches."""
+    import torch
+    sysm, gpu, phi, slots, dslots = system
+    outs = []
+    try:
+        for fused in (1, 0):
+            gpu.set_option("orth_fused", fused)
+            gpu.orbprop_setup(5, 12, 1.2, 0.002)
+            d = dev(torch, phi)
+            iters = [gpu.expospfprop_dev(d, dslots[0], dslots[1], t, t + 0.08, t, t + 0.08, True, expotol=1e-9)
+                     for t in (0.0, 0.08)]
+            outs.append((host(d), iters, gpu.orbprop_state()))
+    finally:
+        gpu.set_option("orth_fused", 1)
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert outs[0][1] == outs[1][1] and outs[0][2] == outs[1][2]
+
+
 def test_expospfprop_rejects_bad_setup(system):
     from sincgpu import SincGpuError
     gpu = system[1]

@@ -299,6 +299,11 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
     h->c.coul_fp32 = (int)value;
     return SINCGPU_OK;
   }
+  if (!strcmp(name, "orth_fused")) {
+    SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "orth_fused must be 0 or 1");
+    h->c.orth_fused = (int)value;
+    return SINCGPU_OK;
+  }
   if (!strcmp(name, "twoe_tile")) {
     SG_CHECK(value == 0 || (value >= 2 && value <= 9), SINCGPU_EINVAL, "twoe_tile must be 0 or 2..9");
     h->c.twoe_tile = (int)value;

@@ -183,6 +183,7 @@ struct Ctx {
   int rp_dmma = 1;        // 1: FP64 reducedpot GEMM on the FP64 tensor cores (DMMA), 0: DFMA tiles
   int twoe_dmma = 1;      // 1: FP64 twoematel GEMM on the FP64 tensor cores (DMMA), 0: DFMA tiles
   int twoe_tile = 0;      // twoematel tile edge 16R: 0 = least padding, 2..9 = that R
+  int orth_fused = 1;     // 1: an orbital Arnoldi step's orthogonalisation in one cooperative launch
   Prof prof;
 
   ~Ctx();

@@ -39,6 +39,7 @@ struct OrbKryState {
   double avnorm;  // |J v_{m+1}|
   double hlast;   // last h(j+1,j) (the breakdown value when mbrk != 0)
   int mbrk;       // 0, or the breakdown dimension
+  int gfail;      // 1: a grid barrier of lv_arnoldi_orth_kernel gave up
 };
 
 __device__ __forceinline__ double lv_block_sum(double v, double* red) {
@@ -146,6 +147,136 @@ __global__ void __launch_bounds__(kLvThreads) lv_mgs_kernel(const double2* __res
   if (threadIdx.x == 0) part_out[blockIdx.x] = s;
 }
 
+// Grid-wide barrier of a cooperative launch (all CTAs resident): bar[0] counts
+// the arrivals of the current generation, bar[1] is the generation.  The last
+// CTA to arrive clears the count and advances the generation; the others poll
+// the generation at most kGridPolls times.  Returns false when the limit was
+// reached, after raising st->gfail (the caller's CTA then leaves the kernel and
+// the host reports SINCGPU_ETIMEOUT).
+constexpr unsigned kGridPolls = 1u << 22;
+
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, OrbKryState* st, int* ok) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vb = bar;
+    const unsigned gen = vb[1];
+    __threadfence();
+    int done = 1;
+    if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+      atomicExch(&bar[0], 0u);
+      __threadfence();
+      atomicAdd(&bar[1], 1u);
+    } else {
+      done = 0;
+      for (unsigned it = 0; it < kGridPolls; ++it)
+        if (vb[1] != gen) {
+          done = 1;
+          break;
+        }
+      if (!done) atomicExch(&st->gfail, 1);
+    }
+    __threadfence();
+    *ok = done;
+  }
+  __syncthreads();
+  return *ok != 0;
+}
+
+// lv_total over partials written earlier in the same launch (read through L2)
+__device__ __forceinline__ double lv_total_l2(const double* part, double* red) {
+  const double v = threadIdx.x < kLvBlocks ? __ldcg(part + threadIdx.x) : 0.0;
+  return lv_block_sum(v, red);
+}
+
+// The whole orthogonalisation of Arnoldi step j in one cooperative launch:
+// lv_dot_kernel (<v_0, p>), the j + 1 lv_mgs_kernel projections and
+// lv_arnoldi_norm_kernel, with the same grid, element assignment, partial sums
+// and fixed-order totals (so the same bits), p held in registers throughout and
+// a grid barrier where the separate launches had a kernel boundary.  p is read
+// once and written once; v_i comes from L2 the second time (it was v_{i+1} of
+// the projection before).  E elements per thread: nv <= E * kLvBlocks * kLvThreads.
+template <int E>
+__global__ void __launch_bounds__(kLvThreads, 2) lv_arnoldi_orth_kernel(const double2* __restrict__ V, double2* p,
+                                                                         long long nv, int j, double* part0,
+                                                                         double* part1, double* __restrict__ Hm,
+                                                                         int mh, double break_tol, OrbKryState* st,
+                                                                         unsigned* bar) {
+  __shared__ double red[33];
+  __shared__ int ok;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long k0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double2 x[E];
+  double s = 0.0;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const long long k = k0 + e * stride;
+    x[e] = make_double2(0.0, 0.0);
+    if (k < nv) {
+      x[e] = p[k];
+      const double2 a = V[k];
+      s = fma(a.x, x[e].x, s);
+      s = fma(a.y, x[e].y, s);
+    }
+  }
+  s = lv_block_sum(s, red);
+  if (threadIdx.x == 0) part0[blockIdx.x] = s;
+  if (!grid_barrier(bar, st, &ok)) return;
+  for (int i = 0; i <= j; ++i) {
+    const double* pin = (i & 1) ? part1 : part0;
+    double* pout = (i & 1) ? part0 : part1;
+    const double h = lv_total_l2(pin, red);
+    if (blockIdx.x == 0 && threadIdx.x == 0) Hm[(long long)j * mh + i] = h;
+    const double2* vi = V + (long long)i * nv;
+    const double2* vn = i < j ? V + (long long)(i + 1) * nv : nullptr;
+    s = 0.0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const long long k = k0 + e * stride;
+      if (k < nv) {
+        const double2 a = vi[k];
+        x[e].x = fma(-h, a.x, x[e].x);
+        x[e].y = fma(-h, a.y, x[e].y);
+        const double2 b = vn ? vn[k] : x[e];
+        s = fma(b.x, x[e].x, s);
+        s = fma(b.y, x[e].y, s);
+      }
+    }
+    s = lv_block_sum(s, red);
+    if (threadIdx.x == 0) pout[blockIdx.x] = s;
+    if (!grid_barrier(bar, st, &ok)) return;
+  }
+  const double h = sqrt(lv_total_l2(((j + 1) & 1) ? part1 : part0, red));
+  const bool brk = h <= break_tol;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->hlast = h;
+    if (brk) st->mbrk = j + 1;
+    else Hm[(long long)j * mh + j + 1] = h;
+  }
+  const double inv = 1.0 / h;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const long long k = k0 + e * stride;
+    if (k < nv) p[k] = brk ? x[e] : make_double2(x[e].x * inv, x[e].y * inv);
+  }
+}
+
+constexpr int kOrthE = 5;  // register-resident elements per thread of the one-launch orthogonalisation
+
+// whether all kLvBlocks CTAs of lv_arnoldi_orth_kernel fit on the device at once
+// (the cooperative launch needs it); evaluated once per process
+static bool orth_fits() {
+  static const bool fits = [] {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return false;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lv_arnoldi_orth_kernel<kOrthE>, kLvThreads, 0) !=
+        cudaSuccess)
+      return false;
+    return (long long)per_sm * sms >= kLvBlocks;
+  }();
+  return fits;
+}
+
 // h(j+1,j) = |p|; breakdown test; p /= h (expokit.f90 Arnoldi loop)
 __global__ void __launch_bounds__(kLvThreads) lv_arnoldi_norm_kernel(double2* __restrict__ p, long long nv, int j,
                                                                      const double* __restrict__ part,
@@ -245,6 +376,7 @@ struct OrbWork {
   double *part0, *part1, *Hm, *exph, *Efull, *pscratch, *err;
   OrbKryState* st;
   int* ns;
+  unsigned* gbar;  // lv_arnoldi_orth_kernel's grid barrier (count, generation)
 };
 
 size_t al256(size_t b) { return (b + 255) / 256 * 256; }
@@ -259,7 +391,7 @@ int orb_work(Ctx& c, int m, OrbWork& o) {
   size_t need = al256(vb) * ((size_t)m + 2 + 6) + al256(dpart) + 5 * al256(mat) +
                 2 * al256(sizeof(double) * kLvBlocks) + al256(sizeof(double) * mh * mh) +
                 al256(sizeof(double) * 130) + al256(sizeof(double) * kMaxPadeOrb * kMaxPadeOrb) +
-                al256(sizeof(double) * 5 * kMaxPadeOrb * kMaxPadeOrb) + 3 * 256;
+                al256(sizeof(double) * 5 * kMaxPadeOrb * kMaxPadeOrb) + 4 * 256;
   SG_TRY(c.ws_orb.ensure(need));
   char* p = (char*)c.ws_orb.ptr;
   auto take = [&](size_t b) {
@@ -289,6 +421,7 @@ int orb_work(Ctx& c, int m, OrbWork& o) {
   o.err = (double*)take(sizeof(double));
   o.st = (OrbKryState*)take(sizeof(OrbKryState));
   o.ns = (int*)take(sizeof(int));
+  o.gbar = (unsigned*)take(2 * sizeof(unsigned));
   return SINCGPU_OK;
 }
 
@@ -390,6 +523,9 @@ int expospfprop(Ctx& c, double2* phi, const MeanFieldSlot* slots, double tin, do
   bool w_zero = true;
   SG_CUDA(cudaMemsetAsync(o.w, 0, sizeof(double2) * nv, c.stream));
   const int lvg = kLvBlocks;
+  const bool orth_fused = c.orth_fused && nv <= (long long)kOrthE * lvg * kLvThreads && orth_fits();
+  SG_CUDA(cudaMemsetAsync(o.gbar, 0, 2 * sizeof(unsigned), c.stream));
+  SG_CUDA(cudaMemsetAsync(o.st, 0, sizeof(OrbKryState), c.stream));
   const int ub = std::min<long long>(ceil_div(nv, 256), 148 * 8);
   OrbKryState hst{};
   while (t_now < t_out) {
@@ -421,19 +557,35 @@ int expospfprop(Ctx& c, double2* phi, const MeanFieldSlot* slots, double tin, do
       ++nmult;
       double2* p = o.V + (size_t)(j + 1) * nv;
       SG_TRY(jacoperate(c, o, o.V + (size_t)j * nv, slots, facs, nslot, timefac, ez, p));
-      lv_dot_kernel<<<lvg, kLvThreads, 0, c.stream>>>(o.V, p, nv, o.part0);
-      SG_LAUNCHED();
-      double* pin = o.part0;
-      double* pout = o.part1;
-      for (int i = 0; i <= j; ++i) {
-        lv_mgs_kernel<<<lvg, kLvThreads, 0, c.stream>>>(o.V, p, nv, i, j, pin, pout, o.Hm, mh);
+      if (orth_fused) {
+        const double2* Vc = o.V;
+        double *P0 = o.part0, *P1 = o.part1, *H = o.Hm;
+        OrbKryState* S = o.st;
+        unsigned* B = o.gbar;
+        int jj = j, mhh = mh;
+        long long nvv = nv;
+        double bt = break_tol;
+        void* args[] = {(void*)&Vc, (void*)&p,   (void*)&nvv, (void*)&jj, (void*)&P0, (void*)&P1,
+                        (void*)&H,  (void*)&mhh, (void*)&bt,  (void*)&S,  (void*)&B};
+        SG_CUDA(cudaLaunchCooperativeKernel((const void*)lv_arnoldi_orth_kernel<kOrthE>, dim3(lvg),
+                                            dim3(kLvThreads), args, 0, c.stream));
+        count_launch();
+      } else {
+        lv_dot_kernel<<<lvg, kLvThreads, 0, c.stream>>>(o.V, p, nv, o.part0);
         SG_LAUNCHED();
-        std::swap(pin, pout);
+        double* pin = o.part0;
+        double* pout = o.part1;
+        for (int i = 0; i <= j; ++i) {
+          lv_mgs_kernel<<<lvg, kLvThreads, 0, c.stream>>>(o.V, p, nv, i, j, pin, pout, o.Hm, mh);
+          SG_LAUNCHED();
+          std::swap(pin, pout);
+        }
+        lv_arnoldi_norm_kernel<<<lvg, kLvThreads, 0, c.stream>>>(p, nv, j, pin, o.Hm, mh, break_tol, o.st);
+        SG_LAUNCHED();
       }
-      lv_arnoldi_norm_kernel<<<lvg, kLvThreads, 0, c.stream>>>(p, nv, j, pin, o.Hm, mh, break_tol, o.st);
-      SG_LAUNCHED();
       SG_CUDA(cudaMemcpyAsync(&hst, o.st, sizeof(OrbKryState), cudaMemcpyDeviceToHost, c.stream));
       SG_CUDA(cudaStreamSynchronize(c.stream));
+      SG_CHECK(!hst.gfail, SINCGPU_ETIMEOUT, "grid barrier of the Arnoldi orthogonalisation timed out");
       if (hst.mbrk) {  // happy breakdown
         k1 = 0;
         mbrkdwn = hst.mbrk;
