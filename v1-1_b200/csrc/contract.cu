@@ -32,6 +32,12 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool val
   int n = valid ? 8 : 0;
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
 }
+// 16-byte asynchronous global->shared copy (zero-fill when !valid)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
 // D (8 x 8, two values per lane) += A (8 x 4) B (4 x 8) on the FP64 tensor cores;
 // lane g * 4 + t holds A[g][t], B[t][g] and D[g][2t], D[g][2t + 1]
 __device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
@@ -215,6 +221,148 @@ __global__ void __launch_bounds__(DMMA ? 64 * R : 256, 1) twoe_gemm3_kernel(cons
   }
 }
 
+// twoematel GEMM on the FP64 tensor cores, software-pipelined: the same tiles,
+// warps and fragments as twoe_gemm3_kernel<R, true> (2R warps, warp w owns rows
+// 16 (w / 2) .. + 15 of the 16R x 16R tile and half of its columns), but the pair
+// products of stage t + 1 are formed between the MMAs of stage t (one product per
+// thread after each K = 4 step: 16R x TK products over 64R threads is exactly 4
+// per thread), the product tile is double-buffered and the raw orbital values and
+// Rpl rows triple-buffered, so one barrier per stage separates the stages and the
+// tensor pipe is not idle while the products are formed.
+template <int R>
+__global__ void __launch_bounds__(64 * R, 1) twoe_dmma_kernel(const double2* __restrict__ phi1,
+                                                              const double2* __restrict__ phi2,
+                                                              const int* __restrict__ pa, const int* __restrict__ pb,
+                                                              const double* __restrict__ Rpl, int npair, int nspf,
+                                                              long long G, int ntn, long long xper,
+                                                              double* __restrict__ part) {
+  constexpr int TT = 16 * R;
+  constexpr int TS = TK + 4;  // shared-memory row stride (doubles), 4 mod 16
+  constexpr int NTH = 64 * R;
+  static_assert(TT * TK == 4 * NTH, "four products per thread and stage");
+  extern __shared__ __align__(16) double dsm[];
+  double* As = dsm;                                             // [2][TT][TS]
+  double* Bs = As + 2 * TT * TS;                                // [3][TT][TS]
+  double2* fsm = reinterpret_cast<double2*>(Bs + 3 * TT * TS);  // [3][2][nspf][TK]
+  int* sa = reinterpret_cast<int*>(fsm + 6 * nspf * TK);
+  int* sb = sa + TT;
+  int* sc = sb + TT;
+  const int M = 2 * npair;
+  int tm = 0, rem = blockIdx.x;
+  while (rem >= ntn - tm) {
+    rem -= ntn - tm;
+    ++tm;
+  }
+  const int tn = tm + rem;
+  const int m0 = tm * TT, n0 = tn * TT;
+  const long long xb = blockIdx.y * xper;
+  const long long xe = min(G, xb + xper);
+  const int tid = threadIdx.x;
+  for (int i = tid; i < TT; i += NTH) {
+    const int m = m0 + i;
+    if (m < M) {
+      const int p = m % npair;
+      sa[i] = pa[p];
+      sb[i] = pb[p];
+      sc[i] = m / npair;
+    } else {
+      sa[i] = 0;
+      sb[i] = 0;
+      sc[i] = -1;
+    }
+  }
+  auto load = [&](int st, long long x0) {
+    double2* f = fsm + st * 2 * nspf * TK;
+    for (int i = tid; i < nspf * TK; i += NTH) {
+      const int o = i / TK, k = i % TK;
+      const long long x = x0 + k;
+      const bool ok = x < xe;
+      const double* g1 = reinterpret_cast<const double*>(ok ? phi1 + (long long)o * G + x : phi1);
+      const double* g2 = reinterpret_cast<const double*>(ok ? phi2 + (long long)o * G + x : phi2);
+      double* d1 = reinterpret_cast<double*>(f + o * TK + k);
+      double* d2 = reinterpret_cast<double*>(f + (nspf + o) * TK + k);
+      cp_async16(d1, g1, ok);
+      cp_async16(d2, g2, ok);
+    }
+    double* b = Bs + st * TT * TS;
+    for (int i = tid; i < TK * TT; i += NTH) {
+      const int nn = i / TK, k = i % TK;
+      const int n = n0 + nn;
+      const long long x = x0 + k;
+      const bool ok = n < M && x < xe;
+      cp_async8(&b[nn * TS + k], ok ? (const void*)(Rpl + (long long)n * G + x) : (const void*)Rpl, ok);
+    }
+    cp_async_commit();
+  };
+  // product q (0..3) of this thread for stage st into product buffer ab
+  auto product = [&](int st, int ab, int q) {
+    const int i = tid + q * NTH;
+    const int mm = i / TK, k = i % TK;
+    const double2* f = fsm + st * 2 * nspf * TK;
+    double v = 0.0;
+    const int comp = sc[mm];
+    if (comp >= 0) {
+      const double2 r = cmulc(f[sa[mm] * TK + k], f[(nspf + sb[mm]) * TK + k]);
+      v = comp == 0 ? r.x : r.y;
+    }
+    As[(ab * TT + mm) * TS + k] = v;
+  };
+  double dacc[2][R][2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < R; ++j) dacc[i][j][0] = dacc[i][j][1] = 0.0;
+  const int wrow = 16 * ((tid >> 5) >> 1), wcol = 8 * R * ((tid >> 5) & 1);
+  const int g8 = (tid & 31) >> 2, t4 = tid & 3;
+  const long long nk = (xe - xb + TK - 1) / TK;
+  __syncthreads();  // sa/sb/sc visible
+  if (nk > 0) {
+    load(0, xb);
+    if (nk > 1) {
+      load(1, xb + TK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) product(0, 0, q);
+  }
+  for (long long t = 0; t < nk; ++t) {
+    const int st = (int)(t % 3), ab = (int)(t & 1);
+    if (t + 1 < nk) cp_async_wait<0>();  // raw stage t + 1 (the only group in flight)
+    __syncthreads();  // products of t and raw t + 1 visible; stage t - 1 fully consumed
+    if (t + 2 < nk) load((int)((t + 2) % 3), xb + (t + 2) * TK);
+    const double* Ast = As + ab * TT * TS;
+    const double* Bst = Bs + st * TT * TS;
+    const bool next = t + 1 < nk;
+#pragma unroll
+    for (int k4 = 0; k4 < TK; k4 += 4) {
+      double a[2], b[R];
+#pragma unroll
+      for (int r = 0; r < 2; ++r) a[r] = Ast[(wrow + 8 * r + g8) * TS + k4 + t4];
+#pragma unroll
+      for (int j = 0; j < R; ++j) b[j] = Bst[(wcol + 8 * j + g8) * TS + k4 + t4];
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int j = 0; j < R; ++j) dmma_884(dacc[r][j], a[r], b[j]);
+      if (next) product((int)((t + 1) % 3), ab ^ 1, k4 / 4);
+    }
+  }
+  double* out = part + (long long)blockIdx.y * M * M;
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int m = m0 + wrow + 8 * r + g8;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const int n = n0 + wcol + 8 * j + 2 * t4;
+      if (m < M && n < M) out[(long long)m * M + n] = dacc[r][j][0];
+      if (m < M && n + 1 < M) out[(long long)m * M + n + 1] = dacc[r][j][1];
+    }
+  }
+}
+
 // C[m][n] = sum_s part[s][m][n] (deterministic): a CTA owns 32 consecutive
 // elements; its 8 warps sum interleaved eighths of the split range (warp g takes
 // splits g, g + 8, ...) in a fixed order and warp 0 adds the eight partial sums in
@@ -326,8 +474,20 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
     const size_t sbytes = sizeof(double) * 3 * (size_t)TT * TS + sizeof(double2) * 4 * (size_t)n * TK +
                           sizeof(int) * 3 * (size_t)TT;
     const dim3 grid(ntiles, nsplit);
+    // the pipelined kernel copies whole complex values (16 bytes)
+    const bool pipe = ((uintptr_t)phi1 % 16 == 0) && ((uintptr_t)phi2 % 16 == 0);
 #define SG_TWOE_LAUNCH(RR, DM)                                                                             \
-  {                                                                                                        \
+  if (DM && pipe) {                                                                                        \
+    static const cudaError_t attr = cudaFuncSetAttribute(                                                  \
+        twoe_dmma_kernel<RR>, cudaFuncAttributeMaxDynamicSharedMemorySize,                                 \
+        (int)(sizeof(double) * 5 * 16 * RR * (TK + 4) + sizeof(double2) * 6 * kMaxOrb * TK +                \
+              sizeof(int) * 3 * 16 * RR));                                                                 \
+    SG_CUDA(attr);                                                                                         \
+    const size_t pbytes = sizeof(double) * 5 * (size_t)TT * (TK + 4) + sizeof(double2) * 6 * (size_t)n * TK + \
+                          sizeof(int) * 3 * (size_t)TT;                                                    \
+    twoe_dmma_kernel<RR><<<grid, 64 * RR, pbytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl, npair, n, c.G, ntn, \
+                                                              xper, part);                                 \
+  } else {                                                                                                 \
     static const cudaError_t attr = cudaFuncSetAttribute(                                                  \
         twoe_gemm3_kernel<RR, DM>, cudaFuncAttributeMaxDynamicSharedMemorySize,                            \
         (int)(sizeof(double) * 3 * 16 * RR * (TK + 4) + sizeof(double2) * 4 * kMaxOrb * TK +                \
@@ -513,80 +673,81 @@ __global__ void __launch_bounds__(16 * CG) rp_gemm3_kernel(const double* __restr
 }
 
 // reducedpot GEMM on the FP64 tensor cores (mma.sync m8n8k4 f64, the FP64 tensor
-// path of sm_100a): CTA tile 128 (x) x 64 (columns), 8 warps of 32 x 32 (4 x 4
-// MMA tiles, 32 accumulators per thread), K in chunks of 8 with a three-stage
-// cp.async pipeline.  Shared-memory rows are padded to 4 (mod 16) doubles so that
+// path of sm_100a): CTA tile 64 (x) x 16 FN (columns), 8 warps (4 x 2) of
+// 16 x 8 FN (2 x FN MMA tiles, 4 FN accumulators per thread), K in chunks of 8
+// with a three-stage cp.async pipeline.  One column tile covers all n(n+1)
+// columns of the hermitian half for n <= 10 (FN = 7: 112 columns), so every Rpl
+// row is read once.  Shared-memory rows are padded to 4 (mod 16) doubles so that
 // the fragment loads (lane g + 4t reads row t, column g) are free of bank
-// conflicts.  The accumulator pair (2t, 2t+1) of a fragment is one complex
-// column pair (Re, Im) of reducedpot.
-constexpr int DM = 128, DN = 64, DK = 8, DST = 3;
-constexpr int DAS = DM + 4, DBS = DN + 4;
+// conflicts.  The accumulator pair (2t, 2t+1) of a fragment is one complex column
+// pair (Re, Im) of reducedpot.
+constexpr int DM = 64, DK = 8, DST = 3;
+constexpr int DAS = DM + 4;
 
 
-template <bool HALF>
-__global__ void __launch_bounds__(256, 3) rp_dmma_kernel(const double* __restrict__ Rpl, const double* __restrict__ Wm,
+template <bool HALF, int FN>
+__global__ void __launch_bounds__(256, 2) rp_dmma_kernel(const double* __restrict__ Rpl, const double* __restrict__ Wm,
                                                       int K, int NC, long long G, double2* __restrict__ out,
                                                       const int* __restrict__ tmap, int n) {
+  constexpr int DN = 16 * FN, DBS = DN + 4;
   __shared__ __align__(16) double As[DST][DK][DAS];
   __shared__ __align__(16) double Bs[DST][DK][DBS];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3;
-  const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
+  const int wm = (warp & 3) * 16, wn = (warp >> 2) * 8 * FN;
   const long long x0 = (long long)blockIdx.x * DM;
   const int c0 = blockIdx.y * DN;
   const int nk = (K + DK - 1) / DK;
+  // Wm rows hold NC (even) doubles, so column pairs start on 16-byte boundaries
   auto load = [&](int st, int k0) {
-    for (int i = tid; i < DK * DM; i += 256) {
+#pragma unroll
+    for (int q = 0; q < DK * DM / 256; ++q) {
+      const int i = tid + 256 * q;
       const int k = i / DM, xx = i % DM;
       const long long x = x0 + xx;
       const bool ok = (k0 + k < K) && x < G;
       cp_async8(&As[st][k][xx], ok ? (const void*)(Rpl + (long long)(k0 + k) * G + x) : (const void*)Rpl, ok);
     }
-    for (int i = tid; i < DK * DN; i += 256) {
-      const int k = i / DN, cc = i % DN;
+    for (int i = tid; i < DK * DN / 2; i += 256) {
+      const int k = i / (DN / 2), cc = 2 * (i % (DN / 2));
       const bool ok = (k0 + k < K) && (c0 + cc < NC);
-      cp_async8(&Bs[st][k][cc], ok ? (const void*)(Wm + (long long)(k0 + k) * NC + c0 + cc) : (const void*)Wm, ok);
+      cp_async16(&Bs[st][k][cc], ok ? (const void*)(Wm + (long long)(k0 + k) * NC + c0 + cc) : (const void*)Wm,
+                 ok);
     }
     cp_async_commit();
   };
-  double acc[4][4][2];
+  double acc[2][FN][2];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int j = 0; j < FN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   load(0, 0);
   if (nk > 1) load(1, DK);
   for (int kc = 0; kc < nk; ++kc) {
     const int st = kc % DST;
-    if (kc + 2 < nk) {
-      load((kc + 2) % DST, (kc + 2) * DK);
-      cp_async_wait<2>();
-    } else if (kc + 1 < nk) {
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncthreads();
+    if (kc + 1 < nk) cp_async_wait<1>();
+    else cp_async_wait<0>();
+    __syncthreads();  // chunk kc visible; every warp is done with chunk kc - 1
+    if (kc + 2 < nk) load((kc + 2) % DST, (kc + 2) * DK);
 #pragma unroll
     for (int k4 = 0; k4 < DK; k4 += 4) {
-      double a[4], b[4];
+      double a[2], b[FN];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[st][k4 + t][wm + 8 * i + g];
+      for (int i = 0; i < 2; ++i) a[i] = As[st][k4 + t][wm + 8 * i + g];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[st][k4 + t][wn + 8 * j + g];
+      for (int j = 0; j < FN; ++j) b[j] = Bs[st][k4 + t][wn + 8 * j + g];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) dmma_884(acc[i][j], a[i], b[j]);
+        for (int j = 0; j < FN; ++j) dmma_884(acc[i][j], a[i], b[j]);
     }
-    __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < 2; ++i) {
     const long long x = x0 + wm + 8 * i + g;
     if (x >= G) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < FN; ++j) {
       const int col = c0 + wn + 8 * j + 2 * t;
       if (col >= NC) continue;
       const double2 v = make_double2(acc[i][j][0], acc[i][j][1]);
@@ -599,6 +760,21 @@ __global__ void __launch_bounds__(256, 3) rp_dmma_kernel(const double* __restric
       }
     }
   }
+}
+
+// column fragments per warp (CTA width 16 FN) with the fewest padded columns of
+// NC, the widest on ties
+static int rp_dmma_fn(int NC) {
+  int best = 8;
+  long long waste = -1;
+  for (int fn : {8, 7, 6, 5, 4}) {
+    const long long w = (long long)ceil_div(NC, 16 * fn) * 16 * fn - NC;
+    if (waste < 0 || w < waste) {
+      waste = w;
+      best = fn;
+    }
+  }
+  return best;
 }
 
 static int reduced_pot_impl(Ctx& c, const double* Rpl, const int* h_pa, const int* h_pb, int npair,
@@ -647,11 +823,24 @@ static int reduced_pot_impl(Ctx& c, const double* Rpl, const int* h_pa, const in
   ProfScope ps(c, ST_RP_GEMM);
   if (c.contract_tf32) return rp_gemm_tf32(c, Rpl, Wm, K, NC, half ? d_tmap : nullptr, reducedpot);
   if (c.rp_dmma) {
-    const dim3 grid((unsigned)ceil_div(c.G, DM), (unsigned)ceil_div(NC, DN));
-    if (half)
-      rp_dmma_kernel<true><<<grid, 256, 0, c.stream>>>(Rpl, Wm, K, NC, c.G, reducedpot, d_tmap, n);
-    else
-      rp_dmma_kernel<false><<<grid, 256, 0, c.stream>>>(Rpl, Wm, K, NC, c.G, reducedpot, nullptr, n);
+    const int fn = rp_dmma_fn(NC);
+    const dim3 grid((unsigned)ceil_div(c.G, DM), (unsigned)ceil_div(NC, 16 * fn));
+#define SG_RP_DMMA(FN)                                                                                   \
+  case FN:                                                                                               \
+    if (half)                                                                                            \
+      rp_dmma_kernel<true, FN><<<grid, 256, 0, c.stream>>>(Rpl, Wm, K, NC, c.G, reducedpot, d_tmap, n);  \
+    else                                                                                                 \
+      rp_dmma_kernel<false, FN><<<grid, 256, 0, c.stream>>>(Rpl, Wm, K, NC, c.G, reducedpot, nullptr, n); \
+    break;
+    switch (fn) {
+      SG_RP_DMMA(4)
+      SG_RP_DMMA(5)
+      SG_RP_DMMA(6)
+      SG_RP_DMMA(7)
+      default:
+        SG_RP_DMMA(8)
+    }
+#undef SG_RP_DMMA
     SG_LAUNCHED();
     return SINCGPU_OK;
   }
