@@ -81,7 +81,10 @@ int sincgpu_fft_length(sincgpu_ctx* ctx);
  * "twoe_tile" (twoematel tile edge 16R: 0 = least padding, 2..9 = R);
  * "orth_fused" (1: the orbital Arnoldi orthogonalisation of one Krylov step in
  * one cooperative launch with bounded grid barriers, 0: one launch per dot,
- * projection and norm; the results are bitwise the same). */
+ * projection and norm; the results are bitwise the same); "rhs_overlap" (1: the
+ * A-vector orbital-RHS entry runs the RDMs, the density-matrix inverse and the
+ * kinetic contraction on a second stream of the context, beside the Coulomb
+ * passes and twoematel, joined by events; 0: one stream; bitwise the same). */
 int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
 
 /* C(M x N, row-major) = A(M x K, row-major) * B(N x K, row-major)^T on the

@@ -75,6 +75,19 @@ def test_orbital_rhs_avec_repeatable(li):
     assert np.array_equal(o1, o2)
 
 
+def test_orbital_rhs_avec_overlap_is_bitwise(li):
+    """The CI part and the kinetic contraction on the side stream (rhs_overlap = 1,
+    the default) change only when work runs, not what it computes."""
+    _, gpu, _, phi, a = li
+    o1 = gpu.orbital_rhs_avec(phi, a, ztdpot=0.02)
+    gpu.set_option("rhs_overlap", 0)
+    try:
+        o0 = gpu.orbital_rhs_avec(phi, a, ztdpot=0.02)
+    finally:
+        gpu.set_option("rhs_overlap", 1)
+    assert np.array_equal(o0, o1)
+
+
 def test_avec_reducedpot_mirror_equals_full(li):
     """The A-vector entry computes only the k <= i half of reducedpot and mirrors
     it (its 2-RDM comes from one A-vector); it equals the full product of the

@@ -113,6 +113,12 @@ Ctx::~Ctx() {
   if (rhs_exec) cudaGraphExecDestroy(rhs_exec);
   if (rhs_graph) cudaGraphDestroy(rhs_graph);
   ci.release(stream);
+  if (side) {
+    cudaStreamSynchronize(side);
+    cudaStreamDestroy(side);
+  }
+  for (cudaEvent_t e : {ev_fork, ev_ci, ev_join})
+    if (e) cudaEventDestroy(e);
   if (stream && own_stream) cudaStreamDestroy(stream);
 }
 
@@ -175,10 +181,11 @@ int twoe_core(Ctx& c, const double2* phi1, const double2* phi2, double2* twoemat
 // twoematel and reducedpot of one orbital set; tally_herm when the 2-RDM is the one
 // of a single A-vector (the library built it), which lets reducedpot be mirrored
 int mean_field(Ctx& c, const double2* phi, const double2* tally, double2* twoematel, double2* reducedpot,
-               bool tally_herm) {
+               bool tally_herm, cudaEvent_t tally_ready) {
   std::vector<int> pa, pb;
   bool herm;
   SG_TRY(twoe_core(c, phi, phi, twoematel, nullptr, pa, pb, herm));
+  if (tally_ready) SG_CUDA(cudaStreamWaitEvent(c.stream, tally_ready, 0));
   return reduced_pot(c, (const double*)c.ws_red.ptr, pa.data(), pb.data(), (int)pa.size(), herm, tally,
                      reducedpot, tally_herm);
 }
@@ -213,6 +220,9 @@ static int ctx_common(sincgpu_ctx* h, int numpoints, double spacing, int numspf,
   SG_TRY(upload_const_roots(device));
   SG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
   c.own_stream = true;
+  SG_CUDA(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&c.ev_fork, &c.ev_ci, &c.ev_join})
+    SG_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   c.bind_workspaces();
   // memory the contexts release stays cached in the device's stream-ordered pool
   // for the next allocations instead of going back to the driver
@@ -297,6 +307,11 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
     SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "coulomb_fp32 must be 0 or 1");
     if (value) SG_TRY(ensure_fp32_tables(h->c));
     h->c.coul_fp32 = (int)value;
+    return SINCGPU_OK;
+  }
+  if (!strcmp(name, "rhs_overlap")) {
+    SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "rhs_overlap must be 0 or 1");
+    h->c.rhs_overlap = (int)value;
     return SINCGPU_OK;
   }
   if (!strcmp(name, "orth_fused")) {

@@ -212,12 +212,45 @@ int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* h, const double* phi, const double
   SG_CHECK(phi && avector && denmat && invdenmat && tally && reducedpot && out, SINCGPU_EINVAL,
            "null argument");
   SG_CHECK(out != phi, SINCGPU_EINVAL, "out must not alias phi");
-  SG_TRY(sincgpu_getdenmat_dev(h, avector, denmat, invdenmat, 1e-10));
-  SG_TRY(sincgpu_get_tworeducedx_dev(h, avector, avector, tally));
-  // the 2-RDM of one A-vector: reducedpot(x,i,k) = conj reducedpot(x,k,i)
-  return orbital_rhs(h->c, (const double2*)phi, (const double2*)tally, (const double2*)denmat,
-                     (const double2*)invdenmat, make_double2(tre, tim), ztdpot, (double2*)twoematel,
-                     (double2*)reducedpot, (double2*)out, true);
+  Ctx& c = h->c;
+  const double2 *P = (const double2*)phi, *A = (const double2*)avector;
+  const double2 tf = make_double2(tre, tim);
+  if (!c.rhs_overlap) {
+    SG_TRY(sincgpu_getdenmat_dev(h, avector, denmat, invdenmat, 1e-10));
+    SG_TRY(sincgpu_get_tworeducedx_dev(h, avector, avector, tally));
+    // the 2-RDM of one A-vector: reducedpot(x,i,k) = conj reducedpot(x,k,i)
+    return orbital_rhs(c, P, (const double2*)tally, (const double2*)denmat, (const double2*)invdenmat, tf, ztdpot,
+                       (double2*)twoematel, (double2*)reducedpot, (double2*)out, true);
+  }
+  // The RDMs, the density-matrix inverse, the mix with denmat and the kinetic
+  // contraction depend on the A-vector or the orbitals alone: they run on the
+  // side stream while this stream runs the Coulomb passes and twoematel.  The
+  // side stream starts after everything issued so far (ev_fork); reducedpot waits
+  // for the tally (ev_ci) and the reduced-potential apply for the kinetic result
+  // (ev_join).  Workspaces grown meanwhile are ordered on the side stream (their
+  // owner is c.stream, swapped below).  The same fork and join hold under graph
+  // capture.
+  SG_CUDA(cudaEventRecord(c.ev_fork, c.stream));
+  SG_CUDA(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
+  const cudaStream_t main_stream = c.stream;
+  c.stream = c.side;
+  const int rc_side = [&]() -> int {
+    SG_TRY(ci_denmat(c, A, (double2*)denmat, (double2*)invdenmat, 1e-10));
+    SG_TRY(ci_tally(c, A, A, (double2*)tally));
+    SG_CUDA(cudaEventRecord(c.ev_ci, c.side));
+    return actreduced_pre(c, P, (const double2*)denmat, ztdpot);
+  }();
+  c.stream = main_stream;
+  SG_CUDA(cudaEventRecord(c.ev_join, c.side));
+  if (rc_side != SINCGPU_OK) {
+    cudaStreamWaitEvent(c.stream, c.ev_join, 0);
+    return rc_side;
+  }
+  const int rc = mean_field(c, P, (const double2*)tally, (double2*)twoematel, (double2*)reducedpot, true, c.ev_ci);
+  SG_CUDA(cudaStreamWaitEvent(c.stream, c.ev_join, 0));
+  if (rc != SINCGPU_OK) return rc;
+  return actreduced_post(c, P, P, (const double2*)invdenmat, (const double2*)reducedpot, tf, 1, 1,
+                         (double2*)out);
 }
 
 int sincgpu_expoavecprop_dev(sincgpu_ctx* h, const double* avec_in, double* avec_out, double t,

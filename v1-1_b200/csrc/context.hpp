@@ -184,6 +184,10 @@ struct Ctx {
   int twoe_dmma = 1;      // 1: FP64 twoematel GEMM on the FP64 tensor cores (DMMA), 0: DFMA tiles
   int twoe_tile = 0;      // twoematel tile edge 16R: 0 = least padding, 2..9 = that R
   int orth_fused = 1;     // 1: an orbital Arnoldi step's orthogonalisation in one cooperative launch
+  int rhs_overlap = 1;    // 1: the fused orbital-RHS entry runs its CI part and the mix + kinetic
+                          //    contraction on `side`, beside the Coulomb passes and twoematel
+  cudaStream_t side = nullptr;  // the second stream of the fused orbital-RHS entry (own, non-blocking)
+  cudaEvent_t ev_fork = nullptr, ev_ci = nullptr, ev_join = nullptr;
   Prof prof;
 
   ~Ctx();
@@ -265,8 +269,9 @@ int reduced_pot_full(Ctx& c, const double2* twoereduced, const double2* tally, d
 
 // capi.cu: twoematel + reducedpot of one orbital set, and that followed by
 // actreduced00 (tally_herm: see reduced_pot)
+// tally_ready: when set, reducedpot waits for it (the tally is written on another stream)
 int mean_field(Ctx& c, const double2* phi, const double2* tally, double2* twoematel, double2* reducedpot,
-               bool tally_herm);
+               bool tally_herm, cudaEvent_t tally_ready = nullptr);
 int orbital_rhs(Ctx& c, const double2* phi, const double2* tally, const double2* denmat, const double2* invdenmat,
                 double2 timefac, double ztdpot, double2* twoematel, double2* reducedpot, double2* out,
                 bool tally_herm);
@@ -303,6 +308,12 @@ int mult_reducedpot_range(Ctx& c, const double2* phi, const double2* redpot, int
 int actreduced(Ctx& c, const double2* phi, const double2* proj, const double2* denmat,
                const double2* invdenmat, const double2* redpot, double2 timefac,
                int dentimeflag, int projflag, double zfield, double2* out);
+// actreduced in two halves: the mix with denmat and the kinetic (+ potential and
+// field) contraction, which need no reduced potentials, then the reduced-potential
+// apply and the projection; the temporaries between them live in ws_rhs
+int actreduced_pre(Ctx& c, const double2* phi, const double2* denmat, double zfield);
+int actreduced_post(Ctx& c, const double2* phi, const double2* proj, const double2* invdenmat,
+                    const double2* redpot, double2 timefac, int dentimeflag, int projflag, double2* out);
 // D(j,i) = <P_j|T_i> over the grid (split-K, deterministic); part holds
 // orbital_dots_scratch(c) * nspf^2 partial sums
 int orbital_dots_scratch(const Ctx& c);

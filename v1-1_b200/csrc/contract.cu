@@ -674,19 +674,20 @@ __global__ void __launch_bounds__(16 * CG) rp_gemm3_kernel(const double* __restr
 
 // reducedpot GEMM on the FP64 tensor cores (mma.sync m8n8k4 f64, the FP64 tensor
 // path of sm_100a): CTA tile 64 (x) x 16 FN (columns), 8 warps (4 x 2) of
-// 16 x 8 FN (2 x FN MMA tiles, 4 FN accumulators per thread), K in chunks of 8
-// with a three-stage cp.async pipeline.  One column tile covers all n(n+1)
-// columns of the hermitian half for n <= 10 (FN = 7: 112 columns), so every Rpl
-// row is read once.  Shared-memory rows are padded to 4 (mod 16) doubles so that
+// 16 x 8 FN (2 x FN MMA tiles, 4 FN accumulators per thread), three CTAs per SM,
+// K in chunks of 16 with a two-stage cp.async pipeline (deeper chunks and the
+// third CTA measured faster than 8-deep chunks in three stages at two CTAs per
+// SM).  One column tile covers all n(n+1) columns of the hermitian half for
+// n <= 10 (FN = 7: 112 columns), so every Rpl row is read once.  Shared-memory rows are padded to 4 (mod 16) doubles so that
 // the fragment loads (lane g + 4t reads row t, column g) are free of bank
 // conflicts.  The accumulator pair (2t, 2t+1) of a fragment is one complex column
 // pair (Re, Im) of reducedpot.
-constexpr int DM = 64, DK = 8, DST = 3;
+constexpr int DM = 64, DK = 16, DST = 2;
 constexpr int DAS = DM + 4;
 
 
 template <bool HALF, int FN>
-__global__ void __launch_bounds__(256, 2) rp_dmma_kernel(const double* __restrict__ Rpl, const double* __restrict__ Wm,
+__global__ void __launch_bounds__(256, 3) rp_dmma_kernel(const double* __restrict__ Rpl, const double* __restrict__ Wm,
                                                       int K, int NC, long long G, double2* __restrict__ out,
                                                       const int* __restrict__ tmap, int n) {
   constexpr int DN = 16 * FN, DBS = DN + 4;
@@ -722,13 +723,11 @@ __global__ void __launch_bounds__(256, 2) rp_dmma_kernel(const double* __restric
 #pragma unroll
     for (int j = 0; j < FN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   load(0, 0);
-  if (nk > 1) load(1, DK);
   for (int kc = 0; kc < nk; ++kc) {
     const int st = kc % DST;
-    if (kc + 1 < nk) cp_async_wait<1>();
-    else cp_async_wait<0>();
+    cp_async_wait<0>();
     __syncthreads();  // chunk kc visible; every warp is done with chunk kc - 1
-    if (kc + 2 < nk) load((kc + 2) % DST, (kc + 2) * DK);
+    if (kc + 1 < nk) load((kc + 1) % DST, (kc + 1) * DK);
 #pragma unroll
     for (int k4 = 0; k4 < DK; k4 += 4) {
       double a[2], b[FN];
@@ -762,12 +761,12 @@ __global__ void __launch_bounds__(256, 2) rp_dmma_kernel(const double* __restric
   }
 }
 
-// column fragments per warp (CTA width 16 FN) with the fewest padded columns of
-// NC, the widest on ties
+// column fragments per warp (CTA width 16 FN, FN <= 7 for the static shared
+// memory) with the fewest padded columns of NC, the widest on ties
 static int rp_dmma_fn(int NC) {
-  int best = 8;
+  int best = 7;
   long long waste = -1;
-  for (int fn : {8, 7, 6, 5, 4}) {
+  for (int fn : {7, 6, 5, 4}) {
     const long long w = (long long)ceil_div(NC, 16 * fn) * 16 * fn - NC;
     if (waste < 0 || w < waste) {
       waste = w;
@@ -836,9 +835,8 @@ static int reduced_pot_impl(Ctx& c, const double* Rpl, const int* h_pa, const in
       SG_RP_DMMA(4)
       SG_RP_DMMA(5)
       SG_RP_DMMA(6)
-      SG_RP_DMMA(7)
       default:
-        SG_RP_DMMA(8)
+        SG_RP_DMMA(7)
     }
 #undef SG_RP_DMMA
     SG_LAUNCHED();

@@ -306,9 +306,12 @@ int mult_reducedpot(Ctx& c, const double2* phi, const double2* redpot, double2* 
   return mult_reducedpot_range(c, phi, redpot, 0, c.nspf, out);
 }
 
-int actreduced(Ctx& c, const double2* phi, const double2* proj, const double2* denmat,
-               const double2* invdenmat, const double2* redpot, double2 timefac, int dentimeflag,
-               int projflag, double zfield, double2* out) {
+namespace {
+// actreduced temporaries in ws_rhs: Y = phi denmat, S = KE(Y), T, split-K partials, D
+struct RhsTemps {
+  double2 *Y, *S, *T, *part, *D;
+};
+int rhs_temps(Ctx& c, RhsTemps& t) {
   const int n = c.nspf;
   SG_CHECK(n <= kMaxOrbRhs, SINCGPU_ERANGE, "at most %d orbitals", kMaxOrbRhs);
   SG_TRY(rhs_attrs());
@@ -316,18 +319,42 @@ int actreduced(Ctx& c, const double2* phi, const double2* proj, const double2* d
   const int nb = ceil_div(G, DCH);
   const size_t need = sizeof(double2) * (3 * (size_t)n * G + (size_t)nb * n * n + (size_t)n * n);
   SG_TRY(c.ws_rhs.ensure(need));
-  double2* Y = (double2*)c.ws_rhs.ptr;
-  double2* S = Y + (size_t)n * G;
-  double2* T = S + (size_t)n * G;
-  double2* part = T + (size_t)n * G;
-  double2* D = part + (size_t)nb * n * n;
-  const int bt = ceil_div(G, TXO);
+  t.Y = (double2*)c.ws_rhs.ptr;
+  t.S = t.Y + (size_t)n * G;
+  t.T = t.S + (size_t)n * G;
+  t.part = t.T + (size_t)n * G;
+  t.D = t.part + (size_t)nb * n * n;
+  return SINCGPU_OK;
+}
+}  // namespace
+
+int actreduced(Ctx& c, const double2* phi, const double2* proj, const double2* denmat,
+               const double2* invdenmat, const double2* redpot, double2 timefac, int dentimeflag,
+               int projflag, double zfield, double2* out) {
+  SG_TRY(actreduced_pre(c, phi, denmat, zfield));
+  return actreduced_post(c, phi, proj, invdenmat, redpot, timefac, dentimeflag, projflag, out);
+}
+
+int actreduced_pre(Ctx& c, const double2* phi, const double2* denmat, double zfield) {
+  RhsTemps t;
+  SG_TRY(rhs_temps(c, t));
+  const int n = c.nspf;
   {
     ProfScope ps(c, ST_RHS_MIX);
-    mix_kernel<<<bt, tile_for(n), smem_mix(n), c.stream>>>(phi, denmat, n, G, Y);
+    mix_kernel<<<ceil_div(c.G, TXO), tile_for(n), smem_mix(n), c.stream>>>(phi, denmat, n, c.G, t.Y);
     SG_LAUNCHED();
   }
-  SG_TRY(mult_ke(c, Y, S, n, true, zfield));
+  return mult_ke(c, t.Y, t.S, n, true, zfield);
+}
+
+int actreduced_post(Ctx& c, const double2* phi, const double2* proj, const double2* invdenmat,
+                    const double2* redpot, double2 timefac, int dentimeflag, int projflag, double2* out) {
+  RhsTemps t;
+  SG_TRY(rhs_temps(c, t));
+  const int n = c.nspf;
+  const long long G = c.G;
+  const int bt = ceil_div(G, TXO);
+  double2 *S = t.S, *T = t.T, *part = t.part, *D = t.D;
   double2* dst = projflag == 1 ? T : out;
   {
     ProfScope ps(c, ST_RHS_REDPOT);
