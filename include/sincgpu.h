@@ -83,8 +83,9 @@ int sincgpu_fft_length(sincgpu_ctx* ctx);
  * one cooperative launch with bounded grid barriers, 0: one launch per dot,
  * projection and norm; the results are bitwise the same); "rhs_overlap" (1: the
  * A-vector orbital-RHS entry runs the RDMs, the density-matrix inverse and the
- * kinetic contraction on a second stream of the context, beside the Coulomb
- * passes and twoematel, joined by events; 0: one stream; bitwise the same). */
+ * kinetic contraction on a second stream of the context beside the Coulomb
+ * passes, then twoematel there beside reducedpot and the apply, joined by
+ * events; 0: one stream; bitwise the same). */
 int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
 
 /* C(M x N, row-major) = A(M x K, row-major) * B(N x K, row-major)^T on the

@@ -82,7 +82,7 @@ int dupload(Ctx& c, void** dst, const void* src, size_t bytes) {
 }
 
 void Ctx::bind_workspaces() {
-  for (Workspace* w : {&ws_fft, &ws_pairs, &ws_gemm, &ws_rhs, &ws_io, &ws_red, &ws_conv, &ws_state, &ws_ci,
+  for (Workspace* w : {&ws_fft, &ws_pairs, &ws_gemm, &ws_twoe, &ws_rhs, &ws_io, &ws_red, &ws_conv, &ws_state, &ws_ci,
                        &ws_ci2, &ws_kry, &ws_orb, &ws_tcerr, &cmf.ws})
     w->owner = &stream;
 }
@@ -90,6 +90,7 @@ void Ctx::bind_workspaces() {
 Ctx::~Ctx() {
   // stream-ordered frees below follow the context's own work; work that a batch
   // graph ran on another stream is waited for here
+  if (side) cudaStreamSynchronize(side);
   if (stream) cudaStreamSynchronize(stream);
   if (rhs_graph) cudaDeviceSynchronize();
   for (void* p : {(void*)d_kevect, (void*)d_ketile, (void*)d_pot, (void*)d_zdip, (void*)d_tcoul, (void*)d_khat,
@@ -98,6 +99,7 @@ Ctx::~Ctx() {
   ws_fft.release();
   ws_pairs.release();
   ws_gemm.release();
+  ws_twoe.release();
   ws_rhs.release();
   ws_io.release();
   ws_red.release();
@@ -113,11 +115,8 @@ Ctx::~Ctx() {
   if (rhs_exec) cudaGraphExecDestroy(rhs_exec);
   if (rhs_graph) cudaGraphDestroy(rhs_graph);
   ci.release(stream);
-  if (side) {
-    cudaStreamSynchronize(side);
-    cudaStreamDestroy(side);
-  }
-  for (cudaEvent_t e : {ev_fork, ev_ci, ev_join})
+  if (side) cudaStreamDestroy(side);
+  for (cudaEvent_t e : {ev_fork, ev_ci, ev_join, ev_coul, ev_twoe})
     if (e) cudaEventDestroy(e);
   if (stream && own_stream) cudaStreamDestroy(stream);
 }
@@ -181,10 +180,31 @@ int twoe_core(Ctx& c, const double2* phi1, const double2* phi2, double2* twoemat
 // twoematel and reducedpot of one orbital set; tally_herm when the 2-RDM is the one
 // of a single A-vector (the library built it), which lets reducedpot be mirrored
 int mean_field(Ctx& c, const double2* phi, const double2* tally, double2* twoematel, double2* reducedpot,
-               bool tally_herm, cudaEvent_t tally_ready) {
+               bool tally_herm, cudaEvent_t tally_ready, cudaStream_t side) {
   std::vector<int> pa, pb;
   bool herm;
-  SG_TRY(twoe_core(c, phi, phi, twoematel, nullptr, pa, pb, herm));
+  if (side && twoematel) {
+    // twoematel feeds nothing below, so it runs on `side` beside reducedpot and the
+    // apply; the pair tables both read are uploaded here first (on this stream)
+    SG_TRY(twoe_core(c, phi, phi, nullptr, nullptr, pa, pb, herm));
+    const int* d;
+    SG_TRY(cached_ints(c, IC_PA, pa.data(), pa.size(), &d));
+    SG_TRY(cached_ints(c, IC_PB, pb.data(), pb.size(), &d));
+    SG_CUDA(cudaEventRecord(c.ev_coul, c.stream));
+    SG_CUDA(cudaStreamWaitEvent(side, c.ev_coul, 0));
+    const cudaStream_t main_stream = c.stream;
+    c.stream = side;
+    const int rc = twoe_matel(c, phi, phi, pa.data(), pb.data(), (int)pa.size(), (const double*)c.ws_red.ptr, herm,
+                              twoematel);
+    c.stream = main_stream;
+    SG_CUDA(cudaEventRecord(c.ev_twoe, side));
+    if (rc != SINCGPU_OK) {
+      cudaStreamWaitEvent(c.stream, c.ev_twoe, 0);
+      return rc;
+    }
+  } else {
+    SG_TRY(twoe_core(c, phi, phi, twoematel, nullptr, pa, pb, herm));
+  }
   if (tally_ready) SG_CUDA(cudaStreamWaitEvent(c.stream, tally_ready, 0));
   return reduced_pot(c, (const double*)c.ws_red.ptr, pa.data(), pb.data(), (int)pa.size(), herm, tally,
                      reducedpot, tally_herm);
@@ -221,7 +241,7 @@ static int ctx_common(sincgpu_ctx* h, int numpoints, double spacing, int numspf,
   SG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
   c.own_stream = true;
   SG_CUDA(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
-  for (cudaEvent_t* e : {&c.ev_fork, &c.ev_ci, &c.ev_join})
+  for (cudaEvent_t* e : {&c.ev_fork, &c.ev_ci, &c.ev_join, &c.ev_coul, &c.ev_twoe})
     SG_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   c.bind_workspaces();
   // memory the contexts release stays cached in the device's stream-ordered pool

@@ -224,10 +224,11 @@ int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* h, const double* phi, const double
   }
   // The RDMs, the density-matrix inverse, the mix with denmat and the kinetic
   // contraction depend on the A-vector or the orbitals alone: they run on the
-  // side stream while this stream runs the Coulomb passes and twoematel.  The
-  // side stream starts after everything issued so far (ev_fork); reducedpot waits
-  // for the tally (ev_ci) and the reduced-potential apply for the kinetic result
-  // (ev_join).  Workspaces grown meanwhile are ordered on the side stream (their
+  // side stream while this stream runs the Coulomb passes.  The side stream starts
+  // after everything issued so far (ev_fork); reducedpot waits for the tally
+  // (ev_ci) and the reduced-potential apply for the kinetic result (ev_join).
+  // twoematel, which nothing here reads, then runs on the side stream beside
+  // reducedpot, the apply and the projection (mean_field), and joins last.  Workspaces grown meanwhile are ordered on the side stream (their
   // owner is c.stream, swapped below).  The same fork and join hold under graph
   // capture.
   SG_CUDA(cudaEventRecord(c.ev_fork, c.stream));
@@ -246,11 +247,15 @@ int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* h, const double* phi, const double
     cudaStreamWaitEvent(c.stream, c.ev_join, 0);
     return rc_side;
   }
-  const int rc = mean_field(c, P, (const double2*)tally, (double2*)twoematel, (double2*)reducedpot, true, c.ev_ci);
+  const int rc = mean_field(c, P, (const double2*)tally, (double2*)twoematel, (double2*)reducedpot, true, c.ev_ci,
+                            twoematel ? c.side : nullptr);
   SG_CUDA(cudaStreamWaitEvent(c.stream, c.ev_join, 0));
-  if (rc != SINCGPU_OK) return rc;
-  return actreduced_post(c, P, P, (const double2*)invdenmat, (const double2*)reducedpot, tf, 1, 1,
-                         (double2*)out);
+  const int rc2 = rc == SINCGPU_OK ? actreduced_post(c, P, P, (const double2*)invdenmat,
+                                                     (const double2*)reducedpot, tf, 1, 1, (double2*)out)
+                                   : rc;
+  // twoematel (side stream) joins last
+  if (twoematel) SG_CUDA(cudaStreamWaitEvent(c.stream, c.ev_twoe, 0));
+  return rc2;
 }
 
 int sincgpu_expoavecprop_dev(sincgpu_ctx* h, const double* avec_in, double* avec_out, double t,

@@ -160,7 +160,8 @@ struct Ctx {
   // ---- scratch --------------------------------------------------------------
   Workspace ws_fft;     // W1 + W2 of the Coulomb passes
   Workspace ws_pairs;   // pair lists
-  Workspace ws_gemm;    // split-K partials, W matrix
+  Workspace ws_gemm;    // reducedpot W matrix
+  Workspace ws_twoe;    // twoematel split-K partials (may run beside reducedpot)
   Workspace ws_rhs;     // RHS temporaries
   Workspace ws_io;      // staging for host-pointer entry points
   Workspace ws_red;     // planar reduced potentials of the last build
@@ -187,7 +188,7 @@ struct Ctx {
   int rhs_overlap = 1;    // 1: the fused orbital-RHS entry runs its CI part and the mix + kinetic
                           //    contraction on `side`, beside the Coulomb passes and twoematel
   cudaStream_t side = nullptr;  // the second stream of the fused orbital-RHS entry (own, non-blocking)
-  cudaEvent_t ev_fork = nullptr, ev_ci = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_ci = nullptr, ev_join = nullptr, ev_coul = nullptr, ev_twoe = nullptr;
   Prof prof;
 
   ~Ctx();
@@ -269,9 +270,11 @@ int reduced_pot_full(Ctx& c, const double2* twoereduced, const double2* tally, d
 
 // capi.cu: twoematel + reducedpot of one orbital set, and that followed by
 // actreduced00 (tally_herm: see reduced_pot)
-// tally_ready: when set, reducedpot waits for it (the tally is written on another stream)
+// tally_ready: when set, reducedpot waits for it (the tally is written on another
+// stream); side: when set, twoematel runs on that stream after the Coulomb passes
+// and c.ev_twoe marks its end (the caller joins it)
 int mean_field(Ctx& c, const double2* phi, const double2* tally, double2* twoematel, double2* reducedpot,
-               bool tally_herm, cudaEvent_t tally_ready = nullptr);
+               bool tally_herm, cudaEvent_t tally_ready = nullptr, cudaStream_t side = nullptr);
 int orbital_rhs(Ctx& c, const double2* phi, const double2* tally, const double2* denmat, const double2* invdenmat,
                 double2 timefac, double ztdpot, double2* twoematel, double2* reducedpot, double2* out,
                 bool tally_herm);

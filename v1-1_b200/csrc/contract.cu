@@ -459,8 +459,8 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
   nsplit = ceil_div(c.G, xper);
   const long long MM = (long long)M * M;
   size_t need = sizeof(double) * (MM * nsplit + MM);
-  SG_TRY(c.ws_gemm.ensure(need));
-  double* part = (double*)c.ws_gemm.ptr;
+  SG_TRY(c.ws_twoe.ensure(need));
+  double* part = (double*)c.ws_twoe.ptr;
   double* C = part + MM * nsplit;
   const int *d_pa, *d_pb, *d_lut;
   std::vector<int> lut;
