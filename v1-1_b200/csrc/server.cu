@@ -128,6 +128,9 @@ void sincgpu_server::run(Req& r, Res& out) {
   const int nc = walks ? walks->w.numconfig : 0;
   if (rc == SINCGPU_OK && r.fp32) rc = sincgpu_set_option(ctx, "coulomb_fp32", 1);
   if (rc == SINCGPU_OK && r.fp32) rc = sincgpu_set_option(ctx, "contract_tf32", 1);
+  // requests share the GPU: a cooperative launch waits until all of its CTAs fit
+  // at once, which would hold every other request's kernels back
+  if (rc == SINCGPU_OK) rc = sincgpu_set_option(ctx, "orth_fused", 0);
   if (rc == SINCGPU_OK)
     rc = sincgpu_cmf_setup(ctx, r.dt, 1, 1e-8, 1e-9, 30, 100, 10, 100, 1.2, 1e-10, 0.0, -1.0);
   if (rc == SINCGPU_OK)
