@@ -180,7 +180,7 @@ int twoe_core(Ctx& c, const double2* phi1, const double2* phi2, double2* twoemat
 // twoematel and reducedpot of one orbital set; tally_herm when the 2-RDM is the one
 // of a single A-vector (the library built it), which lets reducedpot be mirrored
 int mean_field(Ctx& c, const double2* phi, const double2* tally, double2* twoematel, double2* reducedpot,
-               bool tally_herm, cudaEvent_t tally_ready, cudaStream_t side) {
+               bool tally_herm, cudaEvent_t tally_ready, cudaStream_t side, RpApply* apply) {
   std::vector<int> pa, pb;
   bool herm;
   if (side && twoematel) {
@@ -207,7 +207,7 @@ int mean_field(Ctx& c, const double2* phi, const double2* tally, double2* twoema
   }
   if (tally_ready) SG_CUDA(cudaStreamWaitEvent(c.stream, tally_ready, 0));
   return reduced_pot(c, (const double*)c.ws_red.ptr, pa.data(), pb.data(), (int)pa.size(), herm, tally,
-                     reducedpot, tally_herm);
+                     reducedpot, tally_herm, apply);
 }
 
 int orbital_rhs(Ctx& c, const double2* phi, const double2* tally, const double2* denmat, const double2* invdenmat,

@@ -54,6 +54,13 @@ void count_launch();
 __host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+#ifdef __CUDACC__
+// acc += v*m with explicit FMAs (one rounding order wherever it is used)
+__device__ __forceinline__ void cfma(double2& acc, double2 v, double2 m) {
+  acc.x = fma(v.x, m.x, fma(-v.y, m.y, acc.x));
+  acc.y = fma(v.x, m.y, fma(v.y, m.x, acc.y));
+}
+#endif
 __host__ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a*conj(b)
   return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }

@@ -264,8 +264,22 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
 // tally_herm: the 2-RDM has Gamma(c,d,k,i) = conj Gamma(d,c,i,k) (one A-vector);
 // with a hermitian pair list only the k <= i half of reducedpot is computed and
 // the rest mirrored
+// The reduced-potential apply of actreduced00 folded into the reducedpot GEMM's
+// epilogue: T = timefac (S + sum_k reducedpot(.,k,.) phi_k) inv, when reducedpot
+// is a hermitian half whose columns fit one CTA tile (n <= 10) on the FP64 tensor
+// path; `done` reports whether it was (else the caller applies reducedpot itself).
+struct RpApply {
+  const double2* phi;
+  const double2* S;
+  const double2* inv;
+  double2 timefac;
+  double2* T;
+  cudaEvent_t ready;  // S and inv are written on another stream (or nullptr)
+  bool done;
+};
 int reduced_pot(Ctx& c, const double* Rpl, const int* h_pa, const int* h_pb, int npair,
-                bool herm, const double2* tally, double2* reducedpot, bool tally_herm = false);
+                bool herm, const double2* tally, double2* reducedpot, bool tally_herm = false,
+                RpApply* apply = nullptr);
 int reduced_pot_full(Ctx& c, const double2* twoereduced, const double2* tally, double2* reducedpot);
 
 // capi.cu: twoematel + reducedpot of one orbital set, and that followed by
@@ -274,7 +288,8 @@ int reduced_pot_full(Ctx& c, const double2* twoereduced, const double2* tally, d
 // stream); side: when set, twoematel runs on that stream after the Coulomb passes
 // and c.ev_twoe marks its end (the caller joins it)
 int mean_field(Ctx& c, const double2* phi, const double2* tally, double2* twoematel, double2* reducedpot,
-               bool tally_herm, cudaEvent_t tally_ready = nullptr, cudaStream_t side = nullptr);
+               bool tally_herm, cudaEvent_t tally_ready = nullptr, cudaStream_t side = nullptr,
+               RpApply* apply = nullptr);
 int orbital_rhs(Ctx& c, const double2* phi, const double2* tally, const double2* denmat, const double2* invdenmat,
                 double2 timefac, double ztdpot, double2* twoematel, double2* reducedpot, double2* out,
                 bool tally_herm);
@@ -314,9 +329,13 @@ int actreduced(Ctx& c, const double2* phi, const double2* proj, const double2* d
 // actreduced in two halves: the mix with denmat and the kinetic (+ potential and
 // field) contraction, which need no reduced potentials, then the reduced-potential
 // apply and the projection; the temporaries between them live in ws_rhs
+// (t_ready: T, the apply's result before the projection, is already in ws_rhs)
 int actreduced_pre(Ctx& c, const double2* phi, const double2* denmat, double zfield);
 int actreduced_post(Ctx& c, const double2* phi, const double2* proj, const double2* invdenmat,
-                    const double2* redpot, double2 timefac, int dentimeflag, int projflag, double2* out);
+                    const double2* redpot, double2 timefac, int dentimeflag, int projflag, double2* out,
+                    bool t_ready = false);
+// the kinetic result S of actreduced_pre and the apply target T in ws_rhs
+int actreduced_temps(Ctx& c, double2** S, double2** T);
 // D(j,i) = <P_j|T_i> over the grid (split-K, deterministic); part holds
 // orbital_dots_scratch(c) * nspf^2 partial sums
 int orbital_dots_scratch(const Ctx& c);

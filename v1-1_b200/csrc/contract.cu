@@ -686,18 +686,16 @@ constexpr int DM = 64, DK = 16, DST = 2;
 constexpr int DAS = DM + 4;
 
 
-template <bool HALF, int FN>
-__global__ void __launch_bounds__(256, 3) rp_dmma_kernel(const double* __restrict__ Rpl, const double* __restrict__ Wm,
-                                                      int K, int NC, long long G, double2* __restrict__ out,
-                                                      const int* __restrict__ tmap, int n) {
-  constexpr int DN = 16 * FN, DBS = DN + 4;
-  __shared__ __align__(16) double As[DST][DK][DAS];
-  __shared__ __align__(16) double Bs[DST][DK][DBS];
+// the K loop of rp_dmma_kernel: acc (2 x FN fragments per warp) of the CTA's 64-point tile
+template <int FN>
+__device__ __forceinline__ void rp_dmma_mainloop(double (*As)[DK][DAS], double (*Bs)[DK][16 * FN + 4],
+                                                 const double* __restrict__ Rpl, const double* __restrict__ Wm,
+                                                 int K, int NC, long long G, long long x0, int c0,
+                                                 double (&acc)[2][FN][2]) {
+  constexpr int DN = 16 * FN;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3;
   const int wm = (warp & 3) * 16, wn = (warp >> 2) * 8 * FN;
-  const long long x0 = (long long)blockIdx.x * DM;
-  const int c0 = blockIdx.y * DN;
   const int nk = (K + DK - 1) / DK;
   // Wm rows hold NC (even) doubles, so column pairs start on 16-byte boundaries
   auto load = [&](int st, int k0) {
@@ -717,7 +715,6 @@ __global__ void __launch_bounds__(256, 3) rp_dmma_kernel(const double* __restric
     }
     cp_async_commit();
   };
-  double acc[2][FN][2];
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -741,6 +738,17 @@ __global__ void __launch_bounds__(256, 3) rp_dmma_kernel(const double* __restric
         for (int j = 0; j < FN; ++j) dmma_884(acc[i][j], a[i], b[j]);
     }
   }
+}
+
+// reducedpot from the accumulators: column 2 tt + re/im; with HALF the pair
+// tt = (kk <= ii) of tmap and its mirror (ii, kk) = conj
+template <bool HALF, int FN>
+__device__ __forceinline__ void rp_dmma_store(const double (&acc)[2][FN][2], long long G, long long x0, int c0,
+                                              int NC, const int* __restrict__ tmap, int n,
+                                              double2* __restrict__ out) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 3) * 16, wn = (warp >> 2) * 8 * FN;
 #pragma unroll
   for (int i = 0; i < 2; ++i) {
     const long long x = x0 + wm + 8 * i + g;
@@ -761,6 +769,91 @@ __global__ void __launch_bounds__(256, 3) rp_dmma_kernel(const double* __restric
   }
 }
 
+template <bool HALF, int FN>
+__global__ void __launch_bounds__(256, 3) rp_dmma_kernel(const double* __restrict__ Rpl, const double* __restrict__ Wm,
+                                                      int K, int NC, long long G, double2* __restrict__ out,
+                                                      const int* __restrict__ tmap, int n) {
+  __shared__ __align__(16) double As[DST][DK][DAS];
+  __shared__ __align__(16) double Bs[DST][DK][16 * FN + 4];
+  const long long x0 = (long long)blockIdx.x * DM;
+  const int c0 = blockIdx.y * 16 * FN;
+  double acc[2][FN][2];
+  rp_dmma_mainloop<FN>(As, Bs, Rpl, Wm, K, NC, G, x0, c0, acc);
+  rp_dmma_store<HALF, FN>(acc, G, x0, c0, NC, tmap, n, out);
+}
+
+// rp_dmma_kernel<true, FN> with the reduced-potential apply of actreduced00 in its
+// epilogue (all n(n+1) half columns in the CTA's one column tile, n(n+1) <= 16 FN):
+// after writing reducedpot the CTA keeps its 64 x n(n+1) tile in shared memory and
+// forms, per point and orbital i, s_i = S_i + sum_k reducedpot(x,k,i) phi_k(x)
+// (k ascending; the k > i terms from the mirrored pair) and then
+// T_i = timefac sum_j s_j inv(j,i): redpot_kernel's arithmetic in its order, so
+// the same bits, without reading the reducedpot it has just written back from
+// HBM.  Dynamic shared memory: the K loop's stages, then the epilogue's tile.
+constexpr int RPV = DM + 2;  // tile row stride (doubles): conflict-free accumulator stores
+template <int FN>
+__global__ void __launch_bounds__(256, 3) rp_apply_kernel(const double* __restrict__ Rpl, const double* __restrict__ Wm,
+                                                       int K, int NC, long long G, double2* __restrict__ out,
+                                                       const int* __restrict__ tmap, int n,
+                                                       const double2* __restrict__ phi,
+                                                       const double2* __restrict__ S,
+                                                       const double2* __restrict__ inv, double2 timefac,
+                                                       double2* __restrict__ T) {
+  extern __shared__ __align__(16) double rp_sm[];
+  auto As = reinterpret_cast<double (*)[DK][DAS]>(rp_sm);
+  auto Bs = reinterpret_cast<double (*)[DK][16 * FN + 4]>(rp_sm + DST * DK * DAS);
+  const long long x0 = (long long)blockIdx.x * DM;
+  double acc[2][FN][2];
+  rp_dmma_mainloop<FN>(As, Bs, Rpl, Wm, K, NC, G, x0, 0, acc);
+  rp_dmma_store<true, FN>(acc, G, x0, 0, NC, tmap, n, out);
+  __syncthreads();  // every warp is done with the stages
+  double* Vt = rp_sm;                                           // [NC][RPV]
+  double2* ss = reinterpret_cast<double2*>(Vt + NC * RPV);      // [n][DM]
+  double2* sinv = ss + n * DM;                                  // n*n
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 3) * 16, wn = (warp >> 2) * 8 * FN;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < FN; ++j) {
+      const int col = wn + 8 * j + 2 * t, xx = wm + 8 * i + g;
+      if (col < NC) {
+        Vt[col * RPV + xx] = acc[i][j][0];
+        Vt[(col + 1) * RPV + xx] = acc[i][j][1];
+      }
+    }
+  for (int e = tid; e < n * n; e += 256) sinv[e] = inv[e];
+  __syncthreads();
+  for (int it = tid; it < n * DM; it += 256) {
+    const int i = it / DM, xx = it % DM;
+    const long long x = x0 + xx;
+    if (x >= G) continue;
+    double2 a = S[(long long)i * G + x];
+    for (int k = 0; k < n; ++k) {
+      const int tt = k <= i ? i * (i + 1) / 2 + k : k * (k + 1) / 2 + i;
+      const double re = Vt[2 * tt * RPV + xx], im = Vt[(2 * tt + 1) * RPV + xx];
+      cfma(a, make_double2(re, k <= i ? im : -im), phi[(long long)k * G + x]);
+    }
+    ss[i * DM + xx] = a;
+  }
+  __syncthreads();
+  for (int it = tid; it < n * DM; it += 256) {
+    const int i = it / DM, xx = it % DM;
+    const long long x = x0 + xx;
+    if (x >= G) continue;
+    double2 a = make_double2(0.0, 0.0);
+    for (int j = 0; j < n; ++j) cfma(a, ss[j * DM + xx], sinv[j + n * i]);
+    T[(long long)i * G + x] = cmul(timefac, a);
+  }
+}
+
+static size_t rp_apply_smem(int n, int NC, int FN) {
+  const size_t stages = sizeof(double) * DST * DK * ((size_t)DAS + 16 * FN + 4);
+  const size_t epi = sizeof(double) * (size_t)NC * RPV + sizeof(double2) * ((size_t)n * DM + (size_t)n * n);
+  return std::max(stages, epi);
+}
+
 // column fragments per warp (CTA width 16 FN, FN <= 7 for the static shared
 // memory) with the fewest padded columns of NC, the widest on ties
 static int rp_dmma_fn(int NC) {
@@ -777,7 +870,8 @@ static int rp_dmma_fn(int NC) {
 }
 
 static int reduced_pot_impl(Ctx& c, const double* Rpl, const int* h_pa, const int* h_pb, int npair,
-                            bool herm, const double2* tally, double2* reducedpot, bool half) {
+                            bool herm, const double2* tally, double2* reducedpot, bool half, RpApply* apply) {
+  if (apply) apply->done = false;
   const int n = c.nspf;
   half = half && herm;
   const int nt = n * (n + 1) / 2;
@@ -824,6 +918,38 @@ static int reduced_pot_impl(Ctx& c, const double* Rpl, const int* h_pa, const in
   if (c.rp_dmma) {
     const int fn = rp_dmma_fn(NC);
     const dim3 grid((unsigned)ceil_div(c.G, DM), (unsigned)ceil_div(NC, 16 * fn));
+    if (apply && half && grid.y == 1) {
+      // process-wide attributes, one fixed value each (thread-safe static initialisation)
+      static const cudaError_t attr = [] {
+        const void* ks[] = {(const void*)rp_apply_kernel<4>, (const void*)rp_apply_kernel<5>,
+                            (const void*)rp_apply_kernel<6>, (const void*)rp_apply_kernel<7>};
+        for (const void* k : ks) {
+          const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)rp_apply_smem(10, 112, 7));
+          if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+      }();
+      SG_CUDA(attr);
+      if (apply->ready) SG_CUDA(cudaStreamWaitEvent(c.stream, apply->ready, 0));
+      const size_t sm = rp_apply_smem(n, NC, fn);
+#define SG_RP_APPLY(FN)                                                                                  \
+  case FN:                                                                                               \
+    rp_apply_kernel<FN><<<grid, 256, sm, c.stream>>>(Rpl, Wm, K, NC, c.G, reducedpot, d_tmap, n, apply->phi, \
+                                                     apply->S, apply->inv, apply->timefac, apply->T);    \
+    break;
+      switch (fn) {
+        SG_RP_APPLY(4)
+        SG_RP_APPLY(5)
+        SG_RP_APPLY(6)
+        default:
+          SG_RP_APPLY(7)
+      }
+#undef SG_RP_APPLY
+      SG_LAUNCHED();
+      apply->done = true;
+      return SINCGPU_OK;
+    }
 #define SG_RP_DMMA(FN)                                                                                   \
   case FN:                                                                                               \
     if (half)                                                                                            \
@@ -863,8 +989,8 @@ static int reduced_pot_impl(Ctx& c, const double* Rpl, const int* h_pa, const in
 }
 
 int reduced_pot(Ctx& c, const double* Rpl, const int* h_pa, const int* h_pb, int npair, bool herm,
-                const double2* tally, double2* reducedpot, bool tally_herm) {
-  return reduced_pot_impl(c, Rpl, h_pa, h_pb, npair, herm, tally, reducedpot, tally_herm);
+                const double2* tally, double2* reducedpot, bool tally_herm, RpApply* apply) {
+  return reduced_pot_impl(c, Rpl, h_pa, h_pb, npair, herm, tally, reducedpot, tally_herm, apply);
 }
 
 // twoereduced(G, n^2) interleaved -> planar rows for all ordered pairs
@@ -891,7 +1017,7 @@ int reduced_pot_full(Ctx& c, const double2* twoereduced, const double2* tally, d
   double* Rpl = (double*)c.ws_conv.ptr;
   to_planar_kernel<<<ceil_div(total, 256), 256, 0, c.stream>>>(twoereduced, total, total, Rpl);
   SG_LAUNCHED();
-  return reduced_pot_impl(c, Rpl, pa.data(), pb.data(), npair, false, tally, reducedpot, false);
+  return reduced_pot_impl(c, Rpl, pa.data(), pb.data(), npair, false, tally, reducedpot, false, nullptr);
 }
 
 }  // namespace sincgpu

@@ -23,11 +23,6 @@ constexpr int TXO = 32;          // grid points per tile (lanes)
 constexpr int kMaxOrbRhs = 32;   // largest orbital count of these kernels
 constexpr int kRhsSmemMax = 64 * 1024;
 
-__device__ __forceinline__ void cfma(double2& acc, double2 v, double2 m) {  // acc += v*m
-  acc.x = fma(v.x, m.x, fma(-v.y, m.y, acc.x));
-  acc.y = fma(v.x, m.y, fma(v.y, m.x, acc.y));
-}
-
 // out(x,i) = sum_j in(x,j) mat(j,i)   (column-major n x n complex mat)
 __global__ void __launch_bounds__(TXO * kMaxOrbRhs) mix_kernel(const double2* __restrict__ in,
                                                         const double2* __restrict__ mat, int n, long long G,
@@ -347,8 +342,17 @@ int actreduced_pre(Ctx& c, const double2* phi, const double2* denmat, double zfi
   return mult_ke(c, t.Y, t.S, n, true, zfield);
 }
 
+int actreduced_temps(Ctx& c, double2** S, double2** T) {
+  RhsTemps t;
+  SG_TRY(rhs_temps(c, t));
+  *S = t.S;
+  *T = t.T;
+  return SINCGPU_OK;
+}
+
 int actreduced_post(Ctx& c, const double2* phi, const double2* proj, const double2* invdenmat,
-                    const double2* redpot, double2 timefac, int dentimeflag, int projflag, double2* out) {
+                    const double2* redpot, double2 timefac, int dentimeflag, int projflag, double2* out,
+                    bool t_ready) {
   RhsTemps t;
   SG_TRY(rhs_temps(c, t));
   const int n = c.nspf;
@@ -356,7 +360,7 @@ int actreduced_post(Ctx& c, const double2* phi, const double2* proj, const doubl
   const int bt = ceil_div(G, TXO);
   double2 *S = t.S, *T = t.T, *part = t.part, *D = t.D;
   double2* dst = projflag == 1 ? T : out;
-  {
+  if (!t_ready) {
     ProfScope ps(c, ST_RHS_REDPOT);
     redpot_kernel<<<bt, tile_for(n), smem_redpot(n), c.stream>>>(phi, redpot, S, invdenmat, timefac, n, 0, n,
                                                            dentimeflag ? 1 : 0, G, dst);
