@@ -229,7 +229,11 @@ __global__ void __launch_bounds__(DMMA ? 64 * R : 256, 1) twoe_gemm3_kernel(cons
 // per thread), the product tile is double-buffered and the raw orbital values and
 // Rpl rows triple-buffered, so one barrier per stage separates the stages and the
 // tensor pipe is not idle while the products are formed.
-template <int R>
+// SYM (one tile holds all 2U rows and columns): C is symmetric, so only the 8 x 8
+// blocks on and below the diagonal are computed, R (2R + 1) of the (2R)^2; each
+// off-diagonal block is also stored transposed in place of its mirror.  Row blocks p and 2R - 1 - p form a pair
+// with 2R + 1 blocks; warp 2p takes the first R + 1 of them, warp 2p + 1 the rest.
+template <int R, bool SYM>
 __global__ void __launch_bounds__(64 * R, 1) twoe_dmma_kernel(const double2* __restrict__ phi1,
                                                               const double2* __restrict__ phi2,
                                                               const int* __restrict__ pa, const int* __restrict__ pb,
@@ -314,6 +318,20 @@ __global__ void __launch_bounds__(64 * R, 1) twoe_dmma_kernel(const double2* __r
     for (int j = 0; j < R; ++j) dacc[i][j][0] = dacc[i][j][1] = 0.0;
   const int wrow = 16 * ((tid >> 5) >> 1), wcol = 8 * R * ((tid >> 5) & 1);
   const int g8 = (tid & 31) >> 2, t4 = tid & 3;
+  // SYM: this warp's blocks (row block sr[j] in {rA, rB}, column block sb8[j])
+  constexpr int NS = SYM ? R + 1 : 1;
+  const int pr = (tid >> 5) >> 1, rA = pr, rB = 2 * R - 1 - pr;
+  bool sok[NS], sisA[NS];
+  int sb8[NS];
+  double sacc[NS][2];
+#pragma unroll
+  for (int j = 0; j < NS; ++j) {
+    const int s = ((tid >> 5) & 1) * (R + 1) + j;  // slot within the pair's 2R + 1 blocks
+    sok[j] = s <= 2 * R;
+    sisA[j] = s <= pr;
+    sb8[j] = s <= pr ? s : s - pr - 1;
+    sacc[j][0] = sacc[j][1] = 0.0;
+  }
   const long long nk = (xe - xb + TK - 1) / TK;
   __syncthreads();  // sa/sb/sc visible
   if (nk > 0) {
@@ -338,19 +356,41 @@ __global__ void __launch_bounds__(64 * R, 1) twoe_dmma_kernel(const double2* __r
     const bool next = t + 1 < nk;
 #pragma unroll
     for (int k4 = 0; k4 < TK; k4 += 4) {
-      double a[2], b[R];
+      if constexpr (SYM) {
+        const double aA = Ast[(8 * rA + g8) * TS + k4 + t4], aB = Ast[(8 * rB + g8) * TS + k4 + t4];
 #pragma unroll
-      for (int r = 0; r < 2; ++r) a[r] = Ast[(wrow + 8 * r + g8) * TS + k4 + t4];
+        for (int j = 0; j < NS; ++j)
+          if (sok[j]) dmma_884(sacc[j], sisA[j] ? aA : aB, Bst[(8 * sb8[j] + g8) * TS + k4 + t4]);
+      } else {
+        double a[2], b[R];
 #pragma unroll
-      for (int j = 0; j < R; ++j) b[j] = Bst[(wcol + 8 * j + g8) * TS + k4 + t4];
+        for (int r = 0; r < 2; ++r) a[r] = Ast[(wrow + 8 * r + g8) * TS + k4 + t4];
 #pragma unroll
-      for (int r = 0; r < 2; ++r)
+        for (int j = 0; j < R; ++j) b[j] = Bst[(wcol + 8 * j + g8) * TS + k4 + t4];
 #pragma unroll
-        for (int j = 0; j < R; ++j) dmma_884(dacc[r][j], a[r], b[j]);
+        for (int r = 0; r < 2; ++r)
+#pragma unroll
+          for (int j = 0; j < R; ++j) dmma_884(dacc[r][j], a[r], b[j]);
+      }
       if (next) product((int)((t + 1) % 3), ab ^ 1, k4 / 4);
     }
   }
   double* out = part + (long long)blockIdx.y * M * M;
+  if constexpr (SYM) {
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+      if (!sok[j]) continue;
+      const int rb = sisA[j] ? rA : rB;
+      const int m = m0 + 8 * rb + g8, n = n0 + 8 * sb8[j] + 2 * t4;
+      if (m < M && n < M) out[(long long)m * M + n] = sacc[j][0];
+      if (m < M && n + 1 < M) out[(long long)m * M + n + 1] = sacc[j][1];
+      if (sb8[j] != rb) {  // the transposed block above the diagonal (never computed)
+        if (m < M && n < M) out[(long long)n * M + m] = sacc[j][0];
+        if (m < M && n + 1 < M) out[(long long)(n + 1) * M + m] = sacc[j][1];
+      }
+    }
+    return;
+  }
 #pragma unroll
   for (int r = 0; r < 2; ++r) {
     const int m = m0 + wrow + 8 * r + g8;
@@ -468,6 +508,7 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
   SG_TRY(cached_ints(c, IC_PA, h_pa, npair, &d_pa));
   SG_TRY(cached_ints(c, IC_PB, h_pb, npair, &d_pb));
   SG_TRY(cached_ints(c, IC_LUT, lut.data(), (size_t)n * n, &d_lut));
+  bool sym = false;
   {
     ProfScope ps(c, ST_TWOE_GEMM);
     const int TS = c.twoe_dmma ? TK + 4 : TK + 1;
@@ -476,17 +517,28 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
     const dim3 grid(ntiles, nsplit);
     // the pipelined kernel copies whole complex values (16 bytes)
     const bool pipe = ((uintptr_t)phi1 % 16 == 0) && ((uintptr_t)phi2 % 16 == 0);
+    // one symmetric tile (hermitian pairs): the blocks below its diagonal only
+    sym = pipe && herm && c.twoe_dmma && ntm == 1;
 #define SG_TWOE_LAUNCH(RR, DM)                                                                             \
   if (DM && pipe) {                                                                                        \
     static const cudaError_t attr = cudaFuncSetAttribute(                                                  \
-        twoe_dmma_kernel<RR>, cudaFuncAttributeMaxDynamicSharedMemorySize,                                 \
+        twoe_dmma_kernel<RR, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,                          \
         (int)(sizeof(double) * 5 * 16 * RR * (TK + 4) + sizeof(double2) * 6 * kMaxOrb * TK +                \
               sizeof(int) * 3 * 16 * RR));                                                                 \
     SG_CUDA(attr);                                                                                         \
     const size_t pbytes = sizeof(double) * 5 * (size_t)TT * (TK + 4) + sizeof(double2) * 6 * (size_t)n * TK + \
                           sizeof(int) * 3 * (size_t)TT;                                                    \
-    twoe_dmma_kernel<RR><<<grid, 64 * RR, pbytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl, npair, n, c.G, ntn, \
-                                                              xper, part);                                 \
+    static const cudaError_t attr2 = cudaFuncSetAttribute(                                                 \
+        twoe_dmma_kernel<RR, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,                           \
+        (int)(sizeof(double) * 5 * 16 * RR * (TK + 4) + sizeof(double2) * 6 * kMaxOrb * TK +                \
+              sizeof(int) * 3 * 16 * RR));                                                                 \
+    SG_CUDA(attr2);                                                                                        \
+    if (sym)                                                                                               \
+      twoe_dmma_kernel<RR, true><<<grid, 64 * RR, pbytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl, npair, n, c.G, \
+                                                                      ntn, xper, part);                    \
+    else                                                                                                   \
+      twoe_dmma_kernel<RR, false><<<grid, 64 * RR, pbytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl, npair, n,  \
+                                                                       c.G, ntn, xper, part);              \
   } else {                                                                                                 \
     static const cudaError_t attr = cudaFuncSetAttribute(                                                  \
         twoe_gemm3_kernel<RR, DM>, cudaFuncAttributeMaxDynamicSharedMemorySize,                            \
