@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(DMMA ? 64 * R : 256, 1) twoe_gemm3_kernel(cons
 // blocks on and below the diagonal are computed, R (2R + 1) of the (2R)^2; each
 // off-diagonal block is also stored transposed in place of its mirror.  Row blocks p and 2R - 1 - p form a pair
 // with 2R + 1 blocks; warp 2p takes the first R + 1 of them, warp 2p + 1 the rest.
-template <int R, bool SYM>
+template <int R, bool SYM, int KT>
 __global__ void __launch_bounds__(64 * R, 1) twoe_dmma_kernel(const double2* __restrict__ phi1,
                                                               const double2* __restrict__ phi2,
                                                               const int* __restrict__ pa, const int* __restrict__ pb,
@@ -241,14 +241,14 @@ __global__ void __launch_bounds__(64 * R, 1) twoe_dmma_kernel(const double2* __r
                                                               long long G, int ntn, long long xper,
                                                               double* __restrict__ part) {
   constexpr int TT = 16 * R;
-  constexpr int TS = TK + 4;  // shared-memory row stride (doubles), 4 mod 16
+  constexpr int TS = KT + 4;  // shared-memory row stride (doubles), 4 mod 16
   constexpr int NTH = 64 * R;
-  static_assert(TT * TK == 4 * NTH, "four products per thread and stage");
+  static_assert(TT * KT == (KT / 4) * NTH, "one product per thread and K = 4 step");
   extern __shared__ __align__(16) double dsm[];
   double* As = dsm;                                             // [2][TT][TS]
   double* Bs = As + 2 * TT * TS;                                // [3][TT][TS]
-  double2* fsm = reinterpret_cast<double2*>(Bs + 3 * TT * TS);  // [3][2][nspf][TK]
-  int* sa = reinterpret_cast<int*>(fsm + 6 * nspf * TK);
+  double2* fsm = reinterpret_cast<double2*>(Bs + 3 * TT * TS);  // [3][2][nspf][KT]
+  int* sa = reinterpret_cast<int*>(fsm + 6 * nspf * KT);
   int* sb = sa + TT;
   int* sc = sb + TT;
   const int M = 2 * npair;
@@ -276,21 +276,21 @@ __global__ void __launch_bounds__(64 * R, 1) twoe_dmma_kernel(const double2* __r
     }
   }
   auto load = [&](int st, long long x0) {
-    double2* f = fsm + st * 2 * nspf * TK;
-    for (int i = tid; i < nspf * TK; i += NTH) {
-      const int o = i / TK, k = i % TK;
+    double2* f = fsm + st * 2 * nspf * KT;
+    for (int i = tid; i < nspf * KT; i += NTH) {
+      const int o = i / KT, k = i % KT;
       const long long x = x0 + k;
       const bool ok = x < xe;
       const double* g1 = reinterpret_cast<const double*>(ok ? phi1 + (long long)o * G + x : phi1);
       const double* g2 = reinterpret_cast<const double*>(ok ? phi2 + (long long)o * G + x : phi2);
-      double* d1 = reinterpret_cast<double*>(f + o * TK + k);
-      double* d2 = reinterpret_cast<double*>(f + (nspf + o) * TK + k);
+      double* d1 = reinterpret_cast<double*>(f + o * KT + k);
+      double* d2 = reinterpret_cast<double*>(f + (nspf + o) * KT + k);
       cp_async16(d1, g1, ok);
       cp_async16(d2, g2, ok);
     }
     double* b = Bs + st * TT * TS;
-    for (int i = tid; i < TK * TT; i += NTH) {
-      const int nn = i / TK, k = i % TK;
+    for (int i = tid; i < KT * TT; i += NTH) {
+      const int nn = i / KT, k = i % KT;
       const int n = n0 + nn;
       const long long x = x0 + k;
       const bool ok = n < M && x < xe;
@@ -301,12 +301,12 @@ __global__ void __launch_bounds__(64 * R, 1) twoe_dmma_kernel(const double2* __r
   // product q (0..3) of this thread for stage st into product buffer ab
   auto product = [&](int st, int ab, int q) {
     const int i = tid + q * NTH;
-    const int mm = i / TK, k = i % TK;
-    const double2* f = fsm + st * 2 * nspf * TK;
+    const int mm = i / KT, k = i % KT;
+    const double2* f = fsm + st * 2 * nspf * KT;
     double v = 0.0;
     const int comp = sc[mm];
     if (comp >= 0) {
-      const double2 r = cmulc(f[sa[mm] * TK + k], f[(nspf + sb[mm]) * TK + k]);
+      const double2 r = cmulc(f[sa[mm] * KT + k], f[(nspf + sb[mm]) * KT + k]);
       v = comp == 0 ? r.x : r.y;
     }
     As[(ab * TT + mm) * TS + k] = v;
@@ -332,30 +332,30 @@ __global__ void __launch_bounds__(64 * R, 1) twoe_dmma_kernel(const double2* __r
     sb8[j] = s <= pr ? s : s - pr - 1;
     sacc[j][0] = sacc[j][1] = 0.0;
   }
-  const long long nk = (xe - xb + TK - 1) / TK;
+  const long long nk = (xe - xb + KT - 1) / KT;
   __syncthreads();  // sa/sb/sc visible
   if (nk > 0) {
     load(0, xb);
     if (nk > 1) {
-      load(1, xb + TK);
+      load(1, xb + KT);
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 4; ++q) product(0, 0, q);
+    for (int q = 0; q < KT / 4; ++q) product(0, 0, q);
   }
   for (long long t = 0; t < nk; ++t) {
     const int st = (int)(t % 3), ab = (int)(t & 1);
     if (t + 1 < nk) cp_async_wait<0>();  // raw stage t + 1 (the only group in flight)
     __syncthreads();  // products of t and raw t + 1 visible; stage t - 1 fully consumed
-    if (t + 2 < nk) load((int)((t + 2) % 3), xb + (t + 2) * TK);
+    if (t + 2 < nk) load((int)((t + 2) % 3), xb + (t + 2) * KT);
     const double* Ast = As + ab * TT * TS;
     const double* Bst = Bs + st * TT * TS;
     const bool next = t + 1 < nk;
 #pragma unroll
-    for (int k4 = 0; k4 < TK; k4 += 4) {
+    for (int k4 = 0; k4 < KT; k4 += 4) {
       if constexpr (SYM) {
         const double aA = Ast[(8 * rA + g8) * TS + k4 + t4], aB = Ast[(8 * rB + g8) * TS + k4 + t4];
 #pragma unroll
@@ -467,6 +467,42 @@ __global__ void twoe_assemble_kernel(const double* __restrict__ C, const int* __
   out[idx] = r;
 }
 
+// shared memory of twoe_dmma_kernel<R, *, KT>: product tiles, Rpl stages, raw
+// orbital stages, the pair tables
+static size_t twoe_pipe_smem(int R, int KT, int n) {
+  return sizeof(double) * 5 * (size_t)(16 * R) * (KT + 4) + sizeof(double2) * 6 * (size_t)n * KT +
+         sizeof(int) * 3 * (size_t)(16 * R);
+}
+constexpr int kTwoeSmemMax = 227 * 1024;
+
+template <int RR, bool SYM, int KT>
+static int launch_twoe_pipe_t(Ctx& c, dim3 grid, size_t bytes, const double2* phi1, const double2* phi2,
+                              const int* d_pa, const int* d_pb, const double* Rpl, int npair, int ntn,
+                              long long xper, double* part) {
+  // process-wide attribute, one fixed value (thread-safe static initialisation)
+  static const cudaError_t attr = cudaFuncSetAttribute(twoe_dmma_kernel<RR, SYM, KT>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kTwoeSmemMax);
+  SG_CUDA(attr);
+  twoe_dmma_kernel<RR, SYM, KT><<<grid, 64 * RR, bytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl, npair, c.nspf,
+                                                                     c.G, ntn, xper, part);
+  return SINCGPU_OK;
+}
+
+// K stages of 32 points where the shared memory allows (half the stages and
+// barriers of 16-point stages; the same bits), else 16
+template <int RR>
+static int launch_twoe_pipe(Ctx& c, dim3 grid, bool sym, const double2* phi1, const double2* phi2,
+                            const int* d_pa, const int* d_pb, const double* Rpl, int npair, int ntn,
+                            long long xper, double* part) {
+  const size_t b32 = twoe_pipe_smem(RR, 32, c.nspf), b16 = twoe_pipe_smem(RR, 16, c.nspf);
+  if (b32 <= (size_t)kTwoeSmemMax)
+    return sym ? launch_twoe_pipe_t<RR, true, 32>(c, grid, b32, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper, part)
+               : launch_twoe_pipe_t<RR, false, 32>(c, grid, b32, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper,
+                                                   part);
+  return sym ? launch_twoe_pipe_t<RR, true, 16>(c, grid, b16, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper, part)
+             : launch_twoe_pipe_t<RR, false, 16>(c, grid, b16, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper, part);
+}
+
 static void pair_lut(int n, const int* pa, const int* pb, int npair, bool herm, std::vector<int>& lut) {
   lut.assign((size_t)n * n, 0);
   for (int p = 0; p < npair; ++p) {
@@ -521,24 +557,7 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
     sym = pipe && herm && c.twoe_dmma && ntm == 1;
 #define SG_TWOE_LAUNCH(RR, DM)                                                                             \
   if (DM && pipe) {                                                                                        \
-    static const cudaError_t attr = cudaFuncSetAttribute(                                                  \
-        twoe_dmma_kernel<RR, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,                          \
-        (int)(sizeof(double) * 5 * 16 * RR * (TK + 4) + sizeof(double2) * 6 * kMaxOrb * TK +                \
-              sizeof(int) * 3 * 16 * RR));                                                                 \
-    SG_CUDA(attr);                                                                                         \
-    const size_t pbytes = sizeof(double) * 5 * (size_t)TT * (TK + 4) + sizeof(double2) * 6 * (size_t)n * TK + \
-                          sizeof(int) * 3 * (size_t)TT;                                                    \
-    static const cudaError_t attr2 = cudaFuncSetAttribute(                                                 \
-        twoe_dmma_kernel<RR, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,                           \
-        (int)(sizeof(double) * 5 * 16 * RR * (TK + 4) + sizeof(double2) * 6 * kMaxOrb * TK +                \
-              sizeof(int) * 3 * 16 * RR));                                                                 \
-    SG_CUDA(attr2);                                                                                        \
-    if (sym)                                                                                               \
-      twoe_dmma_kernel<RR, true><<<grid, 64 * RR, pbytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl, npair, n, c.G, \
-                                                                      ntn, xper, part);                    \
-    else                                                                                                   \
-      twoe_dmma_kernel<RR, false><<<grid, 64 * RR, pbytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl, npair, n,  \
-                                                                       c.G, ntn, xper, part);              \
+    SG_TRY(launch_twoe_pipe<RR>(c, grid, sym, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper, part));        \
   } else {                                                                                                 \
     static const cudaError_t attr = cudaFuncSetAttribute(                                                  \
         twoe_gemm3_kernel<RR, DM>, cudaFuncAttributeMaxDynamicSharedMemorySize,                            \
