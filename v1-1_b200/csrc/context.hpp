@@ -336,6 +336,12 @@ int actreduced_post(Ctx& c, const double2* phi, const double2* proj, const doubl
                     bool t_ready = false);
 // the kinetic result S of actreduced_pre and the apply target T in ws_rhs
 int actreduced_temps(Ctx& c, double2** S, double2** T);
+// actreduced_pre for several density matrices of one phi: the kinetic, potential
+// and field operators act on each orbital alike and so commute with the orbital
+// mixing, KE(phi denmat) = KE(phi) denmat; actreduced_ke forms KE(phi) once (ws_rhs
+// Y), actreduced_mix_ke then S = Y denmat for each denmat before actreduced_post
+int actreduced_ke(Ctx& c, const double2* phi, double zfield);
+int actreduced_mix_ke(Ctx& c, const double2* denmat);
 // D(j,i) = <P_j|T_i> over the grid (split-K, deterministic); part holds
 // orbital_dots_scratch(c) * nspf^2 partial sums
 int orbital_dots_scratch(const Ctx& c);

@@ -429,9 +429,15 @@ int orb_work(Ctx& c, int m, OrbWork& o) {
 int blend_actreduced(Ctx& c, const double2* x, const double2* proj, const MeanFieldSlot* slots,
                      const double* facs, int nslot, double2 timefac, double ez, double2* tmp, double2* out) {
   const long long len = c.G * c.nspf;
+  if (nslot > 1) SG_TRY(actreduced_ke(c, x, ez));  // KE(x) once for all slots
   for (int s = 0; s < nslot; ++s) {
-    SG_TRY(actreduced(c, x, proj, slots[s].denmat, slots[s].invdenmat, slots[s].reducedpot, timefac, 1,
-                      proj ? 1 : 0, ez, tmp));
+    if (nslot > 1) {
+      SG_TRY(actreduced_mix_ke(c, slots[s].denmat));
+      SG_TRY(actreduced_post(c, x, proj, slots[s].invdenmat, slots[s].reducedpot, timefac, 1, proj ? 1 : 0, tmp));
+    } else {
+      SG_TRY(actreduced(c, x, proj, slots[s].denmat, slots[s].invdenmat, slots[s].reducedpot, timefac, 1,
+                        proj ? 1 : 0, ez, tmp));
+    }
     SG_TRY(axpby(c, out, tmp, 1.0, facs[s], len, s == 0));
   }
   return SINCGPU_OK;

@@ -342,6 +342,22 @@ int actreduced_pre(Ctx& c, const double2* phi, const double2* denmat, double zfi
   return mult_ke(c, t.Y, t.S, n, true, zfield);
 }
 
+int actreduced_ke(Ctx& c, const double2* phi, double zfield) {
+  RhsTemps t;
+  SG_TRY(rhs_temps(c, t));
+  return mult_ke(c, phi, t.Y, c.nspf, true, zfield);
+}
+
+int actreduced_mix_ke(Ctx& c, const double2* denmat) {
+  RhsTemps t;
+  SG_TRY(rhs_temps(c, t));
+  const int n = c.nspf;
+  ProfScope ps(c, ST_RHS_MIX);
+  mix_kernel<<<ceil_div(c.G, TXO), tile_for(n), smem_mix(n), c.stream>>>(t.Y, denmat, n, c.G, t.S);
+  SG_LAUNCHED();
+  return SINCGPU_OK;
+}
+
 int actreduced_temps(Ctx& c, double2** S, double2** T) {
   RhsTemps t;
   SG_TRY(rhs_temps(c, t));
