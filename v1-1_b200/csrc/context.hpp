@@ -341,6 +341,12 @@ int actreduced_temps(Ctx& c, double2** S, double2** T);
 // mixing, KE(phi denmat) = KE(phi) denmat; actreduced_ke forms KE(phi) once (ws_rhs
 // Y), actreduced_mix_ke then S = Y denmat for each denmat before actreduced_post
 int actreduced_ke(Ctx& c, const double2* phi, double zfield);
+// out = facs[0] A_0 + facs[1] A_1, A_s = actreduced without projection for slot s
+// (denmat[s], invdenmat[s], redpot[s]), in one pass after one kinetic contraction
+bool actreduced_blend2_fits(int n);  // its shared memory (n <= 20)
+int actreduced_blend2(Ctx& c, const double2* x, const double2* const* denmat, const double2* const* invdenmat,
+                      const double2* const* redpot, const double* facs, double2 timefac, double zfield,
+                      double2* out);
 int actreduced_mix_ke(Ctx& c, const double2* denmat);
 // D(j,i) = <P_j|T_i> over the grid (split-K, deterministic); part holds
 // orbital_dots_scratch(c) * nspf^2 partial sums

@@ -429,6 +429,12 @@ int orb_work(Ctx& c, int m, OrbWork& o) {
 int blend_actreduced(Ctx& c, const double2* x, const double2* proj, const MeanFieldSlot* slots,
                      const double* facs, int nslot, double2 timefac, double ez, double2* tmp, double2* out) {
   const long long len = c.G * c.nspf;
+  if (nslot == 2 && !proj && actreduced_blend2_fits(c.nspf)) {
+    const double2* den[2] = {slots[0].denmat, slots[1].denmat};
+    const double2* inv[2] = {slots[0].invdenmat, slots[1].invdenmat};
+    const double2* rp[2] = {slots[0].reducedpot, slots[1].reducedpot};
+    return actreduced_blend2(c, x, den, inv, rp, facs, timefac, ez, out);
+  }
   if (nslot > 1) SG_TRY(actreduced_ke(c, x, ez));  // KE(x) once for all slots
   for (int s = 0; s < nslot; ++s) {
     if (nslot > 1) {

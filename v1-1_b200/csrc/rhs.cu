@@ -84,6 +84,60 @@ __global__ void __launch_bounds__(TXO * kMaxOrbRhs) redpot_kernel(const double2*
   }
 }
 
+// actreduced blended over two mean-field slots without projection (the orbital
+// Jacobian): out = f0 A_0 + f1 A_1 with A_s = timefac ((Y D_s + V_s . x) I_s) and
+// Y = KE(x) (+ potential and field), per point in one pass: mix_kernel,
+// redpot_kernel (dentime) and axpby_kernel's arithmetic in their order, so the
+// same bits as those launches, without the per-slot temporaries.
+__global__ void __launch_bounds__(TXO * kMaxOrbRhs) blend2_kernel(
+    const double2* __restrict__ xin, const double2* __restrict__ Y, const double2* __restrict__ V0,
+    const double2* __restrict__ V1, const double2* __restrict__ D0, const double2* __restrict__ D1,
+    const double2* __restrict__ I0, const double2* __restrict__ I1, double2 timefac, double f0, double f1, int n,
+    long long G, double2* __restrict__ out) {
+  extern __shared__ double2 rsm[];
+  double2* sD = rsm;            // [2][n*n]
+  double2* sI = sD + 2 * n * n;  // [2][n*n]
+  double2* sx = sI + 2 * n * n;  // n x TXO
+  double2* sy = sx + n * TXO;    // n x TXO
+  double2* ss = sy + n * TXO;    // n x TXO
+  const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
+  for (int e = tid; e < n * n; e += TXO * blockDim.y) {
+    sD[e] = D0[e];
+    sD[n * n + e] = D1[e];
+    sI[e] = I0[e];
+    sI[n * n + e] = I1[e];
+  }
+  const long long x = blockIdx.x * (long long)TXO + lx;
+  const bool ok = x < G;
+  for (int j = ty; j < n; j += blockDim.y) {
+    sx[j * TXO + lx] = ok ? xin[(long long)j * G + x] : make_double2(0.0, 0.0);
+    sy[j * TXO + lx] = ok ? Y[(long long)j * G + x] : make_double2(0.0, 0.0);
+  }
+  const int ii = ty;  // one warp per orbital
+  double2 res = make_double2(0.0, 0.0);
+  for (int s = 0; s < 2; ++s) {
+    __syncthreads();  // tiles loaded (s = 0); the previous slot's ss reads done (s = 1)
+    if (ok) {
+      const double2* Ds = sD + s * n * n;
+      double2 a = make_double2(0.0, 0.0);
+      for (int j = 0; j < n; ++j) cfma(a, sy[j * TXO + lx], Ds[j + n * ii]);
+      const double2* Vi = (s ? V1 : V0) + (long long)n * ii * G + x;
+#pragma unroll 4
+      for (int k = 0; k < n; ++k) cfma(a, Vi[(long long)k * G], sx[k * TXO + lx]);
+      ss[ii * TXO + lx] = a;
+    }
+    __syncthreads();
+    if (ok) {
+      const double2* Is = sI + s * n * n;
+      double2 t = make_double2(0.0, 0.0);
+      for (int j = 0; j < n; ++j) cfma(t, ss[j * TXO + lx], Is[j + n * ii]);
+      t = cmul(timefac, t);
+      res = s == 0 ? make_double2(f0 * t.x, f0 * t.y) : make_double2(fma(f1, t.x, 1.0 * res.x), fma(f1, t.y, 1.0 * res.y));
+    }
+  }
+  if (ok) out[(long long)ii * G + x] = res;
+}
+
 // partial[blk][j + n*i] = sum_{x in blk} conj(P_j(x)) T_i(x); block blk covers
 // DCH consecutive points, warp w the rows j = w, w + (warps per block), ...
 constexpr int DCH = 128;
@@ -221,7 +275,8 @@ namespace {
 int rhs_attrs() {
   static const cudaError_t attr = [] {
     for (const void* k : {(const void*)mix_kernel, (const void*)redpot_kernel, (const void*)dots_kernel,
-                          (const void*)project_kernel, (const void*)jac_combine_kernel}) {
+                          (const void*)project_kernel, (const void*)jac_combine_kernel,
+                          (const void*)blend2_kernel}) {
       const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax);
       if (e != cudaSuccess) return e;
     }
@@ -354,6 +409,26 @@ int actreduced_mix_ke(Ctx& c, const double2* denmat) {
   const int n = c.nspf;
   ProfScope ps(c, ST_RHS_MIX);
   mix_kernel<<<ceil_div(c.G, TXO), tile_for(n), smem_mix(n), c.stream>>>(t.Y, denmat, n, c.G, t.S);
+  SG_LAUNCHED();
+  return SINCGPU_OK;
+}
+
+bool actreduced_blend2_fits(int n) {
+  return n <= kMaxOrbRhs && sizeof(double2) * (4 * (size_t)n * n + 3 * (size_t)n * TXO) <= (size_t)kRhsSmemMax;
+}
+
+int actreduced_blend2(Ctx& c, const double2* x, const double2* const* denmat, const double2* const* invdenmat,
+                      const double2* const* redpot, const double* facs, double2 timefac, double zfield,
+                      double2* out) {
+  RhsTemps t;
+  SG_TRY(rhs_temps(c, t));
+  const int n = c.nspf;
+  SG_TRY(mult_ke(c, x, t.Y, n, true, zfield));
+  ProfScope ps(c, ST_RHS_REDPOT);
+  const size_t sm = sizeof(double2) * (4 * (size_t)n * n + 3 * (size_t)n * TXO);
+  blend2_kernel<<<ceil_div(c.G, TXO), tile_for(n), sm, c.stream>>>(x, t.Y, redpot[0], redpot[1], denmat[0],
+                                                                    denmat[1], invdenmat[0], invdenmat[1], timefac,
+                                                                    facs[0], facs[1], n, c.G, out);
   SG_LAUNCHED();
   return SINCGPU_OK;
 }
