@@ -116,7 +116,7 @@ Ctx::~Ctx() {
   if (rhs_graph) cudaGraphDestroy(rhs_graph);
   ci.release(stream);
   if (side) cudaStreamDestroy(side);
-  for (cudaEvent_t e : {ev_fork, ev_ci, ev_join, ev_coul, ev_twoe})
+  for (cudaEvent_t e : {ev_fork, ev_ci, ev_join, ev_coul, ev_twoe, ev_avec})
     if (e) cudaEventDestroy(e);
   if (stream && own_stream) cudaStreamDestroy(stream);
 }
@@ -241,7 +241,7 @@ static int ctx_common(sincgpu_ctx* h, int numpoints, double spacing, int numspf,
   SG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
   c.own_stream = true;
   SG_CUDA(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
-  for (cudaEvent_t* e : {&c.ev_fork, &c.ev_ci, &c.ev_join, &c.ev_coul, &c.ev_twoe})
+  for (cudaEvent_t* e : {&c.ev_fork, &c.ev_ci, &c.ev_join, &c.ev_coul, &c.ev_twoe, &c.ev_avec})
     SG_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   c.bind_workspaces();
   // memory the contexts release stays cached in the device's stream-ordered pool

@@ -205,10 +205,13 @@ int sincgpu_sparseconfigmult_dev(sincgpu_ctx* h, const double* in, double* out, 
   return ci_sigma(h->c, (const double2*)in, (double2*)out, h->c.nucrepulsion, ezfield, nucdip_z(h->c));
 }
 
-int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* h, const double* phi, const double* avector, double tre,
-                                 double tim, double ztdpot, double* denmat, double* invdenmat, double* tally,
-                                 double* twoematel, double* reducedpot, double* out) {
-  CTX_CHECK(h);
+namespace {
+// avec_ready (or nullptr): the A-vector reached the device before the orbitals (the
+// host-array entry), so the side stream's RDMs start on it while the orbitals are
+// still being copied; the mix and kinetic contraction wait for the orbitals
+int orbital_rhs_avec_impl(sincgpu_ctx* h, const double* phi, const double* avector, double tre, double tim,
+                          double ztdpot, double* denmat, double* invdenmat, double* tally, double* twoematel,
+                          double* reducedpot, double* out, cudaEvent_t avec_ready) {
   SG_CHECK(phi && avector && denmat && invdenmat && tally && reducedpot && out, SINCGPU_EINVAL,
            "null argument");
   SG_CHECK(out != phi, SINCGPU_EINVAL, "out must not alias phi");
@@ -232,13 +235,14 @@ int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* h, const double* phi, const double
   // owner is c.stream, swapped below).  The same fork and join hold under graph
   // capture.
   SG_CUDA(cudaEventRecord(c.ev_fork, c.stream));
-  SG_CUDA(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
+  SG_CUDA(cudaStreamWaitEvent(c.side, avec_ready ? avec_ready : c.ev_fork, 0));
   const cudaStream_t main_stream = c.stream;
   c.stream = c.side;
   const int rc_side = [&]() -> int {
     SG_TRY(ci_denmat(c, A, (double2*)denmat, (double2*)invdenmat, 1e-10));
     SG_TRY(ci_tally(c, A, A, (double2*)tally));
     SG_CUDA(cudaEventRecord(c.ev_ci, c.side));
+    if (avec_ready) SG_CUDA(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
     return actreduced_pre(c, P, (const double2*)denmat, ztdpot);
   }();
   c.stream = main_stream;
@@ -262,6 +266,15 @@ int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* h, const double* phi, const double
   // twoematel (side stream) joins last
   if (twoematel) SG_CUDA(cudaStreamWaitEvent(c.stream, c.ev_twoe, 0));
   return rc2;
+}
+}  // namespace
+
+int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* h, const double* phi, const double* avector, double tre,
+                                 double tim, double ztdpot, double* denmat, double* invdenmat, double* tally,
+                                 double* twoematel, double* reducedpot, double* out) {
+  CTX_CHECK(h);
+  return orbital_rhs_avec_impl(h, phi, avector, tre, tim, ztdpot, denmat, invdenmat, tally, twoematel, reducedpot,
+                               out, nullptr);
 }
 
 int sincgpu_expoavecprop_dev(sincgpu_ctx* h, const double* avec_in, double* avec_out, double t,
@@ -320,10 +333,12 @@ int sincgpu_orbital_rhs_avec(sincgpu_ctx* h, const double* phi, const double* av
   double* dtal = (double*)p;
   p += pad(b4);
   double* dmat = (double*)p;
-  SG_TRY(up(c, dphi, phi, bphi));
+  // the A-vector first: the RDMs start on it while the orbitals are copied
   SG_TRY(up(c, da, avector, ba));
-  SG_TRY(sincgpu_orbital_rhs_avec_dev(h, dphi, da, tre, tim, ztdpot, dden, dinv, dtal, dmat,
-                                      (double*)c.ws_state.ptr, dout));
+  SG_CUDA(cudaEventRecord(c.ev_avec, c.stream));
+  SG_TRY(up(c, dphi, phi, bphi));
+  SG_TRY(orbital_rhs_avec_impl(h, dphi, da, tre, tim, ztdpot, dden, dinv, dtal, dmat, (double*)c.ws_state.ptr,
+                               dout, c.rhs_overlap ? c.ev_avec : nullptr));
   SG_TRY(down(c, outspfs, dout, bphi));
   SG_CUDA(cudaStreamSynchronize(c.stream));
   return SINCGPU_OK;

@@ -189,6 +189,7 @@ struct Ctx {
                           //    contraction on `side`, beside the Coulomb passes and twoematel
   cudaStream_t side = nullptr;  // the second stream of the fused orbital-RHS entry (own, non-blocking)
   cudaEvent_t ev_fork = nullptr, ev_ci = nullptr, ev_join = nullptr, ev_coul = nullptr, ev_twoe = nullptr;
+  cudaEvent_t ev_avec = nullptr;  // host-array entry: the A-vector is on the device
   Prof prof;
 
   ~Ctx();
