@@ -253,15 +253,16 @@ int orbital_rhs_avec_impl(sincgpu_ctx* h, const double* phi, const double* avect
   }
   // reducedpot applies itself to the orbitals in its epilogue where it can
   // (after the kinetic result: ev_join); otherwise actreduced_post applies it
-  double2 *S = nullptr, *T = nullptr;
-  int rc = actreduced_temps(c, &S, &T);
-  RpApply ap{P, S, (const double2*)invdenmat, tf, T, c.ev_join, false};
+  double2 *S = nullptr, *T = nullptr, *part = nullptr;
+  int rc = actreduced_temps(c, &S, &T, &part);
+  RpApply ap{P, S, (const double2*)invdenmat, tf, T, c.ev_join, false, P, part};
   if (rc == SINCGPU_OK)
     rc = mean_field(c, P, (const double2*)tally, (double2*)twoematel, (double2*)reducedpot, true, c.ev_ci,
                     twoematel ? c.side : nullptr, &ap);
   SG_CUDA(cudaStreamWaitEvent(c.stream, c.ev_join, 0));
   const int rc2 = rc == SINCGPU_OK ? actreduced_post(c, P, P, (const double2*)invdenmat,
-                                                     (const double2*)reducedpot, tf, 1, 1, (double2*)out, ap.done)
+                                                     (const double2*)reducedpot, tf, 1, 1, (double2*)out, ap.done,
+                                                     ap.done)
                                    : rc;
   // twoematel (side stream) joins last
   if (twoematel) SG_CUDA(cudaStreamWaitEvent(c.stream, c.ev_twoe, 0));

@@ -277,6 +277,10 @@ struct RpApply {
   double2* T;
   cudaEvent_t ready;  // S and inv are written on another stream (or nullptr)
   bool done;
+  // when set: also the projector-dot partials part[b][j + n i] = sum over the 64
+  // points of tile b of conj(proj_j) T_i, as dots_kernel forms them (same bits)
+  const double2* proj;
+  double2* part;
 };
 int reduced_pot(Ctx& c, const double* Rpl, const int* h_pa, const int* h_pb, int npair,
                 bool herm, const double2* tally, double2* reducedpot, bool tally_herm = false,
@@ -334,9 +338,10 @@ int actreduced(Ctx& c, const double2* phi, const double2* proj, const double2* d
 int actreduced_pre(Ctx& c, const double2* phi, const double2* denmat, double zfield);
 int actreduced_post(Ctx& c, const double2* phi, const double2* proj, const double2* invdenmat,
                     const double2* redpot, double2 timefac, int dentimeflag, int projflag, double2* out,
-                    bool t_ready = false);
-// the kinetic result S of actreduced_pre and the apply target T in ws_rhs
-int actreduced_temps(Ctx& c, double2** S, double2** T);
+                    bool t_ready = false, bool dots_ready = false);
+// the kinetic result S of actreduced_pre, the apply target T and the projector-dot
+// partials (orbital_dots_scratch(c) blocks of 64 points) in ws_rhs
+int actreduced_temps(Ctx& c, double2** S, double2** T, double2** part = nullptr);
 // actreduced_pre for several density matrices of one phi: the kinetic, potential
 // and field operators act on each orbital alike and so commute with the orbital
 // mixing, KE(phi denmat) = KE(phi) denmat; actreduced_ke forms KE(phi) once (ws_rhs

@@ -869,7 +869,8 @@ __global__ void __launch_bounds__(256, 3) rp_apply_kernel(const double* __restri
                                                        const double2* __restrict__ phi,
                                                        const double2* __restrict__ S,
                                                        const double2* __restrict__ inv, double2 timefac,
-                                                       double2* __restrict__ T) {
+                                                       double2* __restrict__ T, const double2* __restrict__ proj,
+                                                       double2* __restrict__ part) {
   extern __shared__ __align__(16) double rp_sm[];
   auto As = reinterpret_cast<double (*)[DK][DAS]>(rp_sm);
   auto Bs = reinterpret_cast<double (*)[DK][16 * FN + 4]>(rp_sm + DST * DK * DAS);
@@ -908,14 +909,48 @@ __global__ void __launch_bounds__(256, 3) rp_apply_kernel(const double* __restri
     }
     ss[i * DM + xx] = a;
   }
-  __syncthreads();
+  __syncthreads();  // the s values complete; every read of the reducedpot tile done
+  // T of the tile, kept for the projector dots over the spent reducedpot tile
+  double2* Tt = reinterpret_cast<double2*>(rp_sm);  // [n][DM]
   for (int it = tid; it < n * DM; it += 256) {
     const int i = it / DM, xx = it % DM;
     const long long x = x0 + xx;
-    if (x >= G) continue;
+    if (x >= G) {
+      if (part) Tt[i * DM + xx] = make_double2(0.0, 0.0);
+      continue;
+    }
     double2 a = make_double2(0.0, 0.0);
     for (int j = 0; j < n; ++j) cfma(a, ss[j * DM + xx], sinv[j + n * i]);
-    T[(long long)i * G + x] = cmul(timefac, a);
+    a = cmul(timefac, a);
+    T[(long long)i * G + x] = a;
+    if (part) Tt[i * DM + xx] = a;
+  }
+  if (!part) return;
+  // projector-dot partials of this 64-point tile with dots_kernel's lane
+  // assignment (two 32-point halves per lane), FMA order and shuffle tree
+  __syncthreads();
+  const int nn = n * n;
+  for (int j = warp; j < n; j += 8) {
+    double2 pv[DM / 32];
+#pragma unroll
+    for (int r = 0; r < DM / 32; ++r) {
+      const long long x = x0 + r * 32 + lane;
+      pv[r] = x < G ? proj[(long long)j * G + x] : make_double2(0.0, 0.0);
+    }
+    for (int i = 0; i < n; ++i) {
+      double2 a = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int r = 0; r < DM / 32; ++r) {  // conj(p) t
+        const double2 p = pv[r], tv = Tt[i * DM + r * 32 + lane];
+        a.x = fma(p.x, tv.x, fma(p.y, tv.y, a.x));
+        a.y = fma(p.x, tv.y, fma(-p.y, tv.x, a.y));
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        a.x += __shfl_down_sync(0xffffffffu, a.x, o);
+        a.y += __shfl_down_sync(0xffffffffu, a.y, o);
+      }
+      if (lane == 0) part[(long long)blockIdx.x * nn + j + n * i] = a;
+    }
   }
 }
 
@@ -1007,7 +1042,8 @@ static int reduced_pot_impl(Ctx& c, const double* Rpl, const int* h_pa, const in
 #define SG_RP_APPLY(FN)                                                                                  \
   case FN:                                                                                               \
     rp_apply_kernel<FN><<<grid, 256, sm, c.stream>>>(Rpl, Wm, K, NC, c.G, reducedpot, d_tmap, n, apply->phi, \
-                                                     apply->S, apply->inv, apply->timefac, apply->T);    \
+                                                     apply->S, apply->inv, apply->timefac, apply->T,     \
+                                                     apply->proj, apply->part);                          \
     break;
       switch (fn) {
         SG_RP_APPLY(4)

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(TXO * kMaxOrbRhs) blend2_kernel(
 
 // partial[blk][j + n*i] = sum_{x in blk} conj(P_j(x)) T_i(x); block blk covers
 // DCH consecutive points, warp w the rows j = w, w + (warps per block), ...
-constexpr int DCH = 128;
+constexpr int DCH = 64;  // the reducedpot GEMM's 64-point tile, whose epilogue can form these partials
 __global__ void __launch_bounds__(TXO * kMaxOrbRhs) dots_kernel(const double2* __restrict__ Pm,
                                                          const double2* __restrict__ Tm, int n, long long G,
                                                          double2* __restrict__ partial) {
@@ -433,17 +433,18 @@ int actreduced_blend2(Ctx& c, const double2* x, const double2* const* denmat, co
   return SINCGPU_OK;
 }
 
-int actreduced_temps(Ctx& c, double2** S, double2** T) {
+int actreduced_temps(Ctx& c, double2** S, double2** T, double2** part) {
   RhsTemps t;
   SG_TRY(rhs_temps(c, t));
   *S = t.S;
   *T = t.T;
+  if (part) *part = t.part;
   return SINCGPU_OK;
 }
 
 int actreduced_post(Ctx& c, const double2* phi, const double2* proj, const double2* invdenmat,
                     const double2* redpot, double2 timefac, int dentimeflag, int projflag, double2* out,
-                    bool t_ready) {
+                    bool t_ready, bool dots_ready) {
   RhsTemps t;
   SG_TRY(rhs_temps(c, t));
   const int n = c.nspf;
@@ -459,7 +460,12 @@ int actreduced_post(Ctx& c, const double2* phi, const double2* proj, const doubl
   }
   if (projflag == 1) {
     ProfScope ps(c, ST_RHS_PROJ);
-    SG_TRY(launch_dots(c, proj, T, D, part));
+    if (dots_ready) {
+      dots_reduce_kernel<<<n * n, 128, 0, c.stream>>>(part, ceil_div(G, DCH), n * n, D);
+      SG_LAUNCHED();
+    } else {
+      SG_TRY(launch_dots(c, proj, T, D, part));
+    }
     project_kernel<<<bt, tile_for(n), smem_mix(n), c.stream>>>(T, proj, D, n, G, out);
     SG_LAUNCHED();
   }
