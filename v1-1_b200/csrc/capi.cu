@@ -179,6 +179,19 @@ int twoe_core(Ctx& c, const double2* phi1, const double2* phi2, double2* twoemat
 
 // twoematel and reducedpot of one orbital set; tally_herm when the 2-RDM is the one
 // of a single A-vector (the library built it), which lets reducedpot be mirrored
+int side_stream(Ctx& c) {
+  if (c.side) return SINCGPU_OK;
+  int cur = 0;
+  SG_CUDA(cudaGetDevice(&cur));
+  if (cur != c.device) SG_CUDA(cudaSetDevice(c.device));
+  cudaError_t e = cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking);
+  for (cudaEvent_t* ev : {&c.ev_fork, &c.ev_ci, &c.ev_join, &c.ev_coul, &c.ev_twoe, &c.ev_avec})
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+  if (cur != c.device) cudaSetDevice(cur);
+  SG_CUDA(e);
+  return SINCGPU_OK;
+}
+
 int mean_field(Ctx& c, const double2* phi, const double2* tally, double2* twoematel, double2* reducedpot,
                bool tally_herm, cudaEvent_t tally_ready, cudaStream_t side, RpApply* apply) {
   std::vector<int> pa, pb;
@@ -240,9 +253,6 @@ static int ctx_common(sincgpu_ctx* h, int numpoints, double spacing, int numspf,
   SG_TRY(upload_const_roots(device));
   SG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
   c.own_stream = true;
-  SG_CUDA(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
-  for (cudaEvent_t* e : {&c.ev_fork, &c.ev_ci, &c.ev_join, &c.ev_coul, &c.ev_twoe, &c.ev_avec})
-    SG_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   c.bind_workspaces();
   // memory the contexts release stays cached in the device's stream-ordered pool
   // for the next allocations instead of going back to the driver

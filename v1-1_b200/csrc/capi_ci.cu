@@ -234,6 +234,7 @@ int orbital_rhs_avec_impl(sincgpu_ctx* h, const double* phi, const double* avect
   // reducedpot, the apply and the projection (mean_field), and joins last.  Workspaces grown meanwhile are ordered on the side stream (their
   // owner is c.stream, swapped below).  The same fork and join hold under graph
   // capture.
+  SG_TRY(side_stream(c));
   SG_CUDA(cudaEventRecord(c.ev_fork, c.stream));
   SG_CUDA(cudaStreamWaitEvent(c.side, avec_ready ? avec_ready : c.ev_fork, 0));
   const cudaStream_t main_stream = c.stream;
@@ -335,8 +336,9 @@ int sincgpu_orbital_rhs_avec(sincgpu_ctx* h, const double* phi, const double* av
   p += pad(b4);
   double* dmat = (double*)p;
   // the A-vector first: the RDMs start on it while the orbitals are copied
+  if (c.rhs_overlap) SG_TRY(side_stream(c));
   SG_TRY(up(c, da, avector, ba));
-  SG_CUDA(cudaEventRecord(c.ev_avec, c.stream));
+  if (c.rhs_overlap) SG_CUDA(cudaEventRecord(c.ev_avec, c.stream));
   SG_TRY(up(c, dphi, phi, bphi));
   SG_TRY(orbital_rhs_avec_impl(h, dphi, da, tre, tim, ztdpot, dden, dinv, dtal, dmat, (double*)c.ws_state.ptr,
                                dout, c.rhs_overlap ? c.ev_avec : nullptr));

@@ -187,7 +187,8 @@ struct Ctx {
   int orth_fused = 1;     // 1: an orbital Arnoldi step's orthogonalisation in one cooperative launch
   int rhs_overlap = 1;    // 1: the fused orbital-RHS entry runs its CI part and the mix + kinetic
                           //    contraction on `side`, beside the Coulomb passes and twoematel
-  cudaStream_t side = nullptr;  // the second stream of the fused orbital-RHS entry (own, non-blocking)
+  cudaStream_t side = nullptr;  // the second stream of the fused orbital-RHS entry (own, non-blocking;
+                                //   made with its events on first use, side_stream)
   cudaEvent_t ev_fork = nullptr, ev_ci = nullptr, ev_join = nullptr, ev_coul = nullptr, ev_twoe = nullptr;
   cudaEvent_t ev_avec = nullptr;  // host-array entry: the A-vector is on the device
   Prof prof;
@@ -289,6 +290,8 @@ int reduced_pot_full(Ctx& c, const double2* twoereduced, const double2* tally, d
 
 // capi.cu: twoematel + reducedpot of one orbital set, and that followed by
 // actreduced00 (tally_herm: see reduced_pot)
+// creates c.side and the fork/join events on the context's device if not yet made
+int side_stream(Ctx& c);
 // tally_ready: when set, reducedpot waits for it (the tally is written on another
 // stream); side: when set, twoematel runs on that stream after the Coulomb passes
 // and c.ev_twoe marks its end (the caller joins it)
