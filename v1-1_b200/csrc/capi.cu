@@ -116,7 +116,8 @@ Ctx::~Ctx() {
   if (rhs_graph) cudaGraphDestroy(rhs_graph);
   ci.release(stream);
   if (side) cudaStreamDestroy(side);
-  for (cudaEvent_t e : {ev_fork, ev_ci, ev_join, ev_coul, ev_twoe, ev_avec})
+  if (orb_state_h) cudaFreeHost(orb_state_h);
+  for (cudaEvent_t e : {ev_fork, ev_ci, ev_join, ev_coul, ev_twoe, ev_avec, ev_orb_state})
     if (e) cudaEventDestroy(e);
   if (stream && own_stream) cudaStreamDestroy(stream);
 }

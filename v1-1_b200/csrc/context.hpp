@@ -191,6 +191,8 @@ struct Ctx {
                                 //   made with its events on first use, side_stream)
   cudaEvent_t ev_fork = nullptr, ev_ci = nullptr, ev_join = nullptr, ev_coul = nullptr, ev_twoe = nullptr;
   cudaEvent_t ev_avec = nullptr;  // host-array entry: the A-vector is on the device
+  void* orb_state_h = nullptr;    // page-locked copy of the orbital Krylov state (orbprop.cu)
+  cudaEvent_t ev_orb_state = nullptr;
   Prof prof;
 
   ~Ctx();

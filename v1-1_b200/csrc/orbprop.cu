@@ -425,6 +425,16 @@ int orb_work(Ctx& c, int m, OrbWork& o) {
   return SINCGPU_OK;
 }
 
+// page-locked host copy of OrbKryState and its event, made once per context
+int orb_state_host(Ctx& c, OrbKryState** h) {
+  if (!c.orb_state_h) {
+    SG_CUDA(cudaMallocHost(&c.orb_state_h, sizeof(OrbKryState)));
+    SG_CUDA(cudaEventCreateWithFlags(&c.ev_orb_state, cudaEventDisableTiming));
+  }
+  *h = static_cast<OrbKryState*>(c.orb_state_h);
+  return SINCGPU_OK;
+}
+
 // blended unprojected (proj == nullptr) or projected actreduced00 over the slots
 int blend_actreduced(Ctx& c, const double2* x, const double2* proj, const MeanFieldSlot* slots,
                      const double* facs, int nslot, double2 timefac, double ez, double2* tmp, double2* out) {
@@ -565,10 +575,17 @@ int expospfprop(Ctx& c, double2* phi, const MeanFieldSlot* slots, double tin, do
     t_last = t_step;
     t_step = std::min(t_out - t_now, t_new);
     int k1 = 3, mbrkdwn = m;
+    // The product J v_{j+1} is issued before step j's breakdown test is read back,
+    // so the device does not idle during the host round trip; after a breakdown it
+    // is dropped (it writes only v_{j+2} and the product's scratch, which the rest
+    // of the step does not read) and not counted.
+    OrbKryState* hst_pin = nullptr;
+    SG_TRY(orb_state_host(c, &hst_pin));
+    bool have_next = false;  // p = V[j + 1] already holds J V[j]
     for (int j = 0; j < m; ++j) {
       ++nmult;
       double2* p = o.V + (size_t)(j + 1) * nv;
-      SG_TRY(jacoperate(c, o, o.V + (size_t)j * nv, slots, facs, nslot, timefac, ez, p));
+      if (!have_next) SG_TRY(jacoperate(c, o, o.V + (size_t)j * nv, slots, facs, nslot, timefac, ez, p));
       if (orth_fused) {
         const double2* Vc = o.V;
         double *P0 = o.part0, *P1 = o.part1, *H = o.Hm;
@@ -595,8 +612,12 @@ int expospfprop(Ctx& c, double2* phi, const MeanFieldSlot* slots, double tin, do
         lv_arnoldi_norm_kernel<<<lvg, kLvThreads, 0, c.stream>>>(p, nv, j, pin, o.Hm, mh, break_tol, o.st);
         SG_LAUNCHED();
       }
-      SG_CUDA(cudaMemcpyAsync(&hst, o.st, sizeof(OrbKryState), cudaMemcpyDeviceToHost, c.stream));
-      SG_CUDA(cudaStreamSynchronize(c.stream));
+      SG_CUDA(cudaMemcpyAsync(hst_pin, o.st, sizeof(OrbKryState), cudaMemcpyDeviceToHost, c.stream));
+      SG_CUDA(cudaEventRecord(c.ev_orb_state, c.stream));
+      SG_TRY(jacoperate(c, o, p, slots, facs, nslot, timefac, ez, o.V + (size_t)(j + 2) * nv));
+      have_next = true;
+      SG_CUDA(cudaEventSynchronize(c.ev_orb_state));
+      hst = *hst_pin;
       SG_CHECK(!hst.gfail, SINCGPU_ETIMEOUT, "grid barrier of the Arnoldi orthogonalisation timed out");
       if (hst.mbrk) {  // happy breakdown
         k1 = 0;
@@ -608,7 +629,7 @@ int expospfprop(Ctx& c, double2* phi, const MeanFieldSlot* slots, double tin, do
     if (k1 != 0) {
       ++nmult;
       double2* p = o.V + (size_t)(m + 1) * nv;
-      SG_TRY(jacoperate(c, o, o.V + (size_t)m * nv, slots, facs, nslot, timefac, ez, p));
+      if (!have_next) SG_TRY(jacoperate(c, o, o.V + (size_t)m * nv, slots, facs, nslot, timefac, ez, p));
       lv_dot_kernel<<<lvg, kLvThreads, 0, c.stream>>>(p, p, nv, o.part0);
       SG_LAUNCHED();
       lv_avnorm_kernel<<<1, kLvThreads, 0, c.stream>>>(o.part0, o.st);
