@@ -583,7 +583,7 @@ def secondary_rates(proj, torch, stream, flush, phi, den, inv, red, out, mat, av
 # captured launch, so these are cold-cache figures.
 TRAFFIC = {
     ("coul_fwd_x", 41, 10): 70590000, ("coul_fwd_y", 41, 10): 300490000, ("coul_z", 41, 10): 426130000,
-    ("coul_inv_y", 41, 10): 323310000, ("coul_inv_x", 41, 10): 143240000, ("twoe_gemm", 41, 10): 72050000,
+    ("coul_inv_y", 41, 10): 323310000, ("coul_inv_x", 41, 10): 143240000, ("twoe_gemm", 41, 10): 72000000,
     ("rp_gemm", 41, 10): 169050000, ("rhs_redpot", 41, 10): 136340000, ("ke_xy", 41, 10): 12170000,
     ("ke_z", 41, 10): 22090000,
 }
