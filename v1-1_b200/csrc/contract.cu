@@ -896,16 +896,29 @@ __global__ void __launch_bounds__(256, 3) rp_apply_kernel(const double* __restri
       }
     }
   for (int e = tid; e < n * n; e += 256) sinv[e] = inv[e];
+  // this thread's point is the same for all its items (256 threads over 64 points):
+  // its orbital values once, all loads in flight together (n <= kApplyOrb)
+  static_assert(256 % DM == 0, "one point per thread");
+  constexpr int kApplyOrb = 10;  // n(n+1) <= 16 FN <= 112
+  const int pxx = tid % DM;
+  const long long px = x0 + pxx;
+  double2 ph[kApplyOrb];
+#pragma unroll
+  for (int k = 0; k < kApplyOrb; ++k)
+    ph[k] = (k < n && px < G) ? phi[(long long)k * G + px] : make_double2(0.0, 0.0);
   __syncthreads();
   for (int it = tid; it < n * DM; it += 256) {
-    const int i = it / DM, xx = it % DM;
+    const int i = it / DM, xx = it % DM;  // xx == pxx
     const long long x = x0 + xx;
     if (x >= G) continue;
     double2 a = S[(long long)i * G + x];
-    for (int k = 0; k < n; ++k) {
-      const int tt = k <= i ? i * (i + 1) / 2 + k : k * (k + 1) / 2 + i;
-      const double re = Vt[2 * tt * RPV + xx], im = Vt[(2 * tt + 1) * RPV + xx];
-      cfma(a, make_double2(re, k <= i ? im : -im), phi[(long long)k * G + x]);
+#pragma unroll
+    for (int k = 0; k < kApplyOrb; ++k) {
+      if (k < n) {
+        const int tt = k <= i ? i * (i + 1) / 2 + k : k * (k + 1) / 2 + i;
+        const double re = Vt[2 * tt * RPV + xx], im = Vt[(2 * tt + 1) * RPV + xx];
+        cfma(a, make_double2(re, k <= i ? im : -im), ph[k]);
+      }
     }
     ss[i * DM + xx] = a;
   }
