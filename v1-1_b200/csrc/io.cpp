@@ -16,7 +16,7 @@
 //               avector(numr) complex*16
 // Loading an A-vector (easy_load_avectors, configload.f90:801-847) reorders
 // each stored determinant to the canonical order, multiplies by the phase of
-// that reordering and places it at its index in this build's configuration
+// that reordering and places it at its index in the walk tables' configuration
 // list; determinants not in the list are an error.
 #include <algorithm>
 #include <cstdint>
