@@ -88,6 +88,17 @@ def test_orbital_rhs_avec_overlap_is_bitwise(li):
     assert np.array_equal(o0, o1)
 
 
+def test_scheduling_options_reject_bad_values(li):
+    from sincgpu import SincGpuError
+    gpu = li[1]
+    for name, bad in (("rhs_overlap", 2), ("orth_fused", -1), ("twoe_tile", 1), ("twoe_tile", 10)):
+        with pytest.raises(SincGpuError):
+            gpu.set_option(name, bad)
+    gpu.set_option("rhs_overlap", 1)
+    gpu.set_option("orth_fused", 1)
+    gpu.set_option("twoe_tile", 0)
+
+
 def test_avec_reducedpot_mirror_equals_full(li):
     """The A-vector entry computes only the k <= i half of reducedpot and mirrors
     it (its 2-RDM comes from one A-vector); it equals the full product of the
