@@ -140,33 +140,37 @@ __global__ void __launch_bounds__(TXO * kMaxOrbRhs) blend2_kernel(
 
 // partial[blk][j + n*i] = sum_{x in blk} conj(P_j(x)) T_i(x); block blk covers
 // DCH consecutive points, warp w the rows j = w, w + (warps per block), ...
-constexpr int DCH = 64;  // the reducedpot GEMM's 64-point tile, whose epilogue can form these partials
+// BL points per block: 64 (DCH) where the reducedpot GEMM's epilogue forms the same
+// partials for its 64-point tiles, 256 for the orbital Jacobian's dots (eight terms
+// per lane before the shuffle tree, a quarter of the partials to reduce)
+constexpr int DCH = 64;
+template <int BL>
 __global__ void __launch_bounds__(TXO * kMaxOrbRhs) dots_kernel(const double2* __restrict__ Pm,
                                                          const double2* __restrict__ Tm, int n, long long G,
                                                          double2* __restrict__ partial) {
   extern __shared__ double2 rsm[];
-  double2* tt = rsm;  // n x DCH
+  double2* tt = rsm;  // n x BL
   const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
-  const long long x0 = blockIdx.x * (long long)DCH;
-  for (int e = tid; e < n * DCH; e += TXO * blockDim.y) {
-    const int i = e / DCH, k = e % DCH;
+  const long long x0 = blockIdx.x * (long long)BL;
+  for (int e = tid; e < n * BL; e += TXO * blockDim.y) {
+    const int i = e / BL, k = e % BL;
     const long long x = x0 + k;
     tt[e] = x < G ? Tm[(long long)i * G + x] : make_double2(0.0, 0.0);
   }
   __syncthreads();
   const int nn = n * n;
   for (int j = ty; j < n; j += blockDim.y) {
-    double2 pv[DCH / TXO];
+    double2 pv[BL / TXO];
 #pragma unroll
-    for (int r = 0; r < DCH / TXO; ++r) {
+    for (int r = 0; r < BL / TXO; ++r) {
       const long long x = x0 + r * TXO + lx;
       pv[r] = x < G ? Pm[(long long)j * G + x] : make_double2(0.0, 0.0);
     }
     for (int i = 0; i < n; ++i) {
       double2 a = make_double2(0.0, 0.0);
 #pragma unroll
-      for (int r = 0; r < DCH / TXO; ++r) {  // conj(p) t
-        const double2 p = pv[r], t = tt[i * DCH + r * TXO + lx];
+      for (int r = 0; r < BL / TXO; ++r) {  // conj(p) t
+        const double2 p = pv[r], t = tt[i * BL + r * TXO + lx];
         a.x = fma(p.x, t.x, fma(p.y, t.y, a.x));
         a.y = fma(p.x, t.y, fma(-p.y, t.x, a.y));
       }
@@ -274,7 +278,8 @@ namespace {
 // the kernels' shared-memory limit: one fixed value (race-free across threads)
 int rhs_attrs() {
   static const cudaError_t attr = [] {
-    for (const void* k : {(const void*)mix_kernel, (const void*)redpot_kernel, (const void*)dots_kernel,
+    for (const void* k : {(const void*)mix_kernel, (const void*)redpot_kernel, (const void*)dots_kernel<DCH>,
+                          (const void*)dots_kernel<4 * DCH>,
                           (const void*)project_kernel, (const void*)jac_combine_kernel,
                           (const void*)blend2_kernel}) {
       const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax);
@@ -292,12 +297,17 @@ dim3 tile_for(int n) { return dim3(TXO, (unsigned)std::max(1, std::min(n, kMaxOr
 
 size_t smem_mix(int n) { return sizeof(double2) * ((size_t)n * n + (size_t)n * TXO); }
 size_t smem_redpot(int n) { return sizeof(double2) * ((size_t)n * n + 2 * (size_t)n * TXO); }
-size_t smem_dots(int n) { return sizeof(double2) * (size_t)n * DCH; }
+size_t smem_dots(int n, int bl = DCH) { return sizeof(double2) * (size_t)n * bl; }
 size_t smem_jac(int n) { return sizeof(double2) * (2 * (size_t)n * n + 2 * (size_t)n * TXO); }
 
-int launch_dots(Ctx& c, const double2* P, const double2* T, double2* D, double2* part) {
-  const int n = c.nspf, nb = ceil_div(c.G, DCH);
-  dots_kernel<<<nb, tile_for(n), smem_dots(n), c.stream>>>(P, T, n, c.G, part);
+int launch_dots(Ctx& c, const double2* P, const double2* T, double2* D, double2* part, bool wide = false) {
+  const int n = c.nspf;
+  wide = wide && smem_dots(n, 4 * DCH) <= (size_t)kRhsSmemMax;
+  const int nb = ceil_div(c.G, wide ? 4 * DCH : DCH);
+  if (wide)
+    dots_kernel<4 * DCH><<<nb, tile_for(n), smem_dots(n, 4 * DCH), c.stream>>>(P, T, n, c.G, part);
+  else
+    dots_kernel<DCH><<<nb, tile_for(n), smem_dots(n), c.stream>>>(P, T, n, c.G, part);
   SG_LAUNCHED();
   dots_reduce_kernel<<<n * n, 128, 0, c.stream>>>(part, nb, n * n, D);
   SG_LAUNCHED();
@@ -311,7 +321,7 @@ int orbital_dots_scratch(const Ctx& c) { return ceil_div(c.G, DCH); }
 int orbital_dots(Ctx& c, const double2* P, const double2* T, double2* D, double2* part) {
   SG_CHECK(c.nspf <= kMaxOrbRhs, SINCGPU_ERANGE, "at most %d orbitals", kMaxOrbRhs);
   SG_TRY(rhs_attrs());
-  return launch_dots(c, P, T, D, part);
+  return launch_dots(c, P, T, D, part, true);
 }
 
 int orbital_mix(Ctx& c, const double2* in, const double2* mat, double2* out) {
