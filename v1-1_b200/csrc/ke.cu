@@ -142,23 +142,30 @@ __global__ void __launch_bounds__(256) ke_z_kernel(const double2* __restrict__ i
   double2* dst = out + (long long)orb * ka.G + (long long)y * N;
   for (int job = warp; job < T * T; job += blockDim.x >> 5) {
     const int z0 = (job / T) * 8, x0 = (job % T) * 8;
+    const int zz = z0 + g;
+    // the pass-1 values this lane adds to, loaded before the MMA chain so that
+    // their latency overlaps it
+    double2 prev[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int x = x0 + 2 * t + h;
+      prev[h] = (zz < N && x < N) ? dst[zz * NN + x] : make_double2(0.0, 0.0);
+    }
     double r0 = 0, r1 = 0, i0 = 0, i1 = 0;
     for (int k = 0; k < ka.k4; k += 4) {
       double aK = Ks[(z0 + g) * S + k + t];
       dmma884(r0, r1, aK, Xr[(k + t) * S + x0 + g]);
       dmma884(i0, i1, aK, Xi[(k + t) * S + x0 + g]);
     }
-    const int zz = z0 + g;
     if (zz < N) {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int x = x0 + 2 * t + h;
         if (x < N) {
-          double2* o = dst + zz * NN + x;
-          double2 v = *o;
+          double2 v = prev[h];
           v.x += h ? r1 : r0;
           v.y += h ? i1 : i0;
-          *o = v;
+          dst[zz * NN + x] = v;
         }
       }
     }
