@@ -152,10 +152,22 @@ __global__ void __launch_bounds__(TXO * kMaxOrbRhs) dots_kernel(const double2* _
   double2* tt = rsm;  // n x BL
   const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
   const long long x0 = blockIdx.x * (long long)BL;
-  for (int e = tid; e < n * BL; e += TXO * blockDim.y) {
-    const int i = e / BL, k = e % BL;
-    const long long x = x0 + k;
-    tt[e] = x < G ? Tm[(long long)i * G + x] : make_double2(0.0, 0.0);
+  const int nth = TXO * blockDim.y;
+  // staged in batches of 8 elements per thread: the 8 loads are in flight together
+  for (int e0 = tid; e0 < n * BL; e0 += 8 * nth) {
+    double2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int e = e0 + r * nth;
+      const int i = e / BL, k = e % BL;
+      const long long x = x0 + k;
+      v[r] = (e < n * BL && x < G) ? Tm[(long long)i * G + x] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int e = e0 + r * nth;
+      if (e < n * BL) tt[e] = v[r];
+    }
   }
   __syncthreads();
   const int nn = n * n;
