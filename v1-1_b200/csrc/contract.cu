@@ -1037,7 +1037,8 @@ static int reduced_pot_impl(Ctx& c, const double* Rpl, const int* h_pa, const in
   if (c.rp_dmma) {
     const int fn = rp_dmma_fn(NC);
     const dim3 grid((unsigned)ceil_div(c.G, DM), (unsigned)ceil_div(NC, 16 * fn));
-    if (apply && half && grid.y == 1) {
+    // one column tile (n(n+1) <= 112, so n <= 10: the epilogue's per-thread orbital registers)
+    if (apply && half && grid.y == 1 && n <= 10) {
       // process-wide attributes, one fixed value each (thread-safe static initialisation)
       static const cudaError_t attr = [] {
         const void* ks[] = {(const void*)rp_apply_kernel<4>, (const void*)rp_apply_kernel<5>,
