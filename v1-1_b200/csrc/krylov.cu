@@ -91,6 +91,65 @@ __global__ void __launch_bounds__(kKryThreads) kry_mgs_kernel(double* __restrict
   for (long long k = threadIdx.x; k < n; k += blockDim.x) p[k] *= inv;
 }
 
+// kry_mgs_kernel with p held in registers (the same elements per thread,
+// k = threadIdx.x + e blockDim.x, and the same sums in the same order: the same
+// bits) and v_{i+1} loaded while v_i's projection is being reduced, so that no
+// global access sits inside the sequential loop.  n <= E * kKryThreads.
+template <int E>
+__global__ void __launch_bounds__(kKryThreads) kry_mgs_reg_kernel(double* __restrict__ V, long long n, int j,
+                                                                  double* __restrict__ Hm, int mh,
+                                                                  double break_tol, KryState* st) {
+  __shared__ double red[33];
+  if (st->mbrk) return;
+  double* p = V + (long long)(j + 1) * n;
+  double x[E], a[E], an[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const long long k = threadIdx.x + (long long)e * blockDim.x;
+    x[e] = k < n ? p[k] : 0.0;
+    a[e] = k < n ? V[k] : 0.0;
+    an[e] = 0.0;
+  }
+  for (int i = 0; i <= j; ++i) {
+    if (i < j) {
+      const double* vn = V + (long long)(i + 1) * n;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const long long k = threadIdx.x + (long long)e * blockDim.x;
+        an[e] = k < n ? vn[k] : 0.0;
+      }
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      if (threadIdx.x + (long long)e * blockDim.x < n) s += a[e] * x[e];
+    const double hij = block_sum(s, red);
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      if (threadIdx.x + (long long)e * blockDim.x < n) x[e] -= hij * a[e];
+    if (threadIdx.x == 0) Hm[(long long)j * mh + i] = hij;
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < E; ++e) a[e] = an[e];
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int e = 0; e < E; ++e)
+    if (threadIdx.x + (long long)e * blockDim.x < n) s += x[e] * x[e];
+  const double h = sqrt(block_sum(s, red));
+  const bool brk = h <= break_tol;
+  if (threadIdx.x == 0) {
+    if (brk) st->mbrk = j + 1;
+    else Hm[(long long)j * mh + j + 1] = h;
+  }
+  const double inv = 1.0 / h;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const long long k = threadIdx.x + (long long)e * blockDim.x;
+    if (k < n) p[k] = brk ? x[e] : x[e] * inv;
+  }
+}
+
 __global__ void __launch_bounds__(kKryThreads) kry_avnorm_kernel(const double* __restrict__ p, long long n,
                                                                  KryState* st) {
   __shared__ double red[33];
@@ -365,7 +424,14 @@ int expv_avector(Ctx& c, const double2* v, double2* w, double t, double2 timefac
       SG_TRY(ci_sigma(c, (const double2*)(V + (size_t)j * n), tmp, c.nucrepulsion, ez, nucdipz));
       cscale_kernel<<<cb, 256, 0, c.stream>>>(tmp, timefac, nc, (double2*)(V + (size_t)(j + 1) * n), dst);
       SG_LAUNCHED();
-      kry_mgs_kernel<<<1, kKryThreads, 0, c.stream>>>(V, n, j, Hm, mh, break_tol, dst);
+      if (n <= kKryThreads)
+        kry_mgs_reg_kernel<1><<<1, kKryThreads, 0, c.stream>>>(V, n, j, Hm, mh, break_tol, dst);
+      else if (n <= 2 * kKryThreads)
+        kry_mgs_reg_kernel<2><<<1, kKryThreads, 0, c.stream>>>(V, n, j, Hm, mh, break_tol, dst);
+      else if (n <= 4 * kKryThreads)
+        kry_mgs_reg_kernel<4><<<1, kKryThreads, 0, c.stream>>>(V, n, j, Hm, mh, break_tol, dst);
+      else
+        kry_mgs_kernel<<<1, kKryThreads, 0, c.stream>>>(V, n, j, Hm, mh, break_tol, dst);
       SG_LAUNCHED();
     }
     ++nmult;
