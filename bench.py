@@ -44,7 +44,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="B")
+    ap.add_argument("--config", default="C", choices=["A", "B", "C"])
+    ap.add_argument("--no-workload-b", action="store_true",
+                    help="skip the 41^3 / 10-orbital workload measured beside the headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
@@ -132,32 +134,114 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU reference (oracle restatement), used for --impl reference and cpu_baseline
 # ---------------------------------------------------------------------------
-def seeded_avector(nc, seed):
-    rng = np.random.default_rng(seed)
-    a = rng.standard_normal(nc) + 1j * rng.standard_normal(nc)
-    return a / np.linalg.norm(a)
+def oracle_walks(w):
+    """The oracle's CI object for workload `w`.  Up to a few hundred determinants
+    the oracle builds its own walk tables; above that (the 14400-determinant
+    workload, where its pure-Python builder needs minutes) the tables come from
+    the library's host builder, which equals the oracle's bit for bit
+    (tests/test_walks.py, frozen digests of the 4-electron / 16-orbital tables),
+    and the oracle's numpy RDM routines run on them.  Set-up, not timed."""
+    from oracle.walks_oracle import CIWalks
+    from sincgpu import WalkTables
+    from sincgpu.inputs import ci_size
+    if ci_size(w.numelec, w.nspf) <= 1000:
+        return CIWalks(w.numelec, w.nspf, 0), "oracle"
+    wt = WalkTables(w.numelec, w.nspf, 0)
+    ow = object.__new__(CIWalks)
+    ow.numelec = ow.numpart = w.numelec
+    ow.nspf, ow.restrictms, ow.numconfig = w.nspf, 0, wt.numconfig
+    for name in ("configlist", "numsinglewalks", "numdoublewalks", "singlewalk", "singlewalkdirphase",
+                 "singlewalkopspf", "doublewalk", "doublewalkdirphase", "doublewalkdirspf"):
+        setattr(ow, name, wt.table(name))
+    ow.scol = np.concatenate([[0], np.cumsum(ow.numsinglewalks)]).astype(np.int64)
+    ow.dcol = np.concatenate([[0], np.cumsum(ow.numdoublewalks)]).astype(np.int64)
+    wt.close()
+    return ow, "library host builder (bit-identical to the oracle's)"
 
 
-def cpu_reference_eval(w, threads):
+def cpu_reference_eval(w, threads, want_outputs=False):
     """Seconds for one orbital-RHS evaluation with the CPU restatement of the
-    reference: 1-RDM + regularised inverse + 2-RDM from the A-vector, pair
-    Coulomb solves and twoematel, reducedpot, actreduced00."""
+    reference (1-RDM + regularised inverse + 2-RDM from the A-vector, pair
+    Coulomb solves and twoematel, reducedpot, actreduced00), a description of
+    what was timed, and, for a complete evaluation with `want_outputs`, its RHS
+    and twoematel.
+
+    Grids up to 41^3 run the whole evaluation.  Larger workloads time a
+    bounded sample: the Coulomb solves of
+    4 of the reference's n op_tinv batches (one batch = the n densities of one
+    orbital b, coreproject.f90:1042-1081) and the twoematel contractions of n of
+    its n^2 (a1, b1) rows (coreproject.f90:1089-1099), each scaled to the full
+    count, plus the complete RDMs, reducedpot and actreduced00."""
     sys.path.insert(0, str(REPO))
     from oracle import sinc_oracle as orc
-    from oracle.walks_oracle import CIWalks
-    from sincgpu import inputs as inp
+    from sincgpu.inputs import seeded_avector, seeded_orbitals
     sysm = orc.SincSystem(w.numpoints, w.spacing, w.centershift, w.nuccharges)
-    ow = CIWalks(w.numelec, w.nspf, 0)
-    phi = inp.seeded_orbitals(w.numpoints, w.spacing, w.nspf, seed=1)
+    ow, tables = oracle_walks(w)
+    phi = seeded_orbitals(w.numpoints, w.spacing, w.nspf, seed=1)
     a = seeded_avector(ow.numconfig, seed=2)
+    n, G = w.nspf, w.G
+    full = w.numpoints <= 41
     t0 = time.perf_counter()
     den = ow.getdenmat00(a)
     inv = orc.invmatsmooth(den)
     tally = ow.get_tworeducedx(a)
-    _, red = sysm.call_twoe_matel00(phi, phi, workers=threads)
+    t_ci = time.perf_counter() - t0
+    if full:
+        t0 = time.perf_counter()
+        mat, red = sysm.call_twoe_matel00(phi, phi, workers=threads)
+        rp = orc.get_reducedpot(red, tally)
+        rhs = orc.actreduced00(sysm, phi, phi, den, inv, rp)
+        t = t_ci + time.perf_counter() - t0
+        sample = (f"1 complete orbital-RHS evaluation, numpy/scipy restatement of the reference on {threads} host "
+                  f"threads (walk tables: {tables}, set-up)")
+        return t, sample, ({"rhs": rhs, "twoematel": mat} if want_outputs else None)
+    nb = 4
+    red = np.empty((G, n, n), dtype=np.complex128, order="F")
+    t0 = time.perf_counter()
+    for b in range(nb):                                   # coreproject.f90:1042-1081
+        den_b = phi * np.conj(phi[:, b])[:, None]
+        red[:, :, b] = sysm.op_tinv(den_b, workers=threads)
+    t_coul = (time.perf_counter() - t0) * n / nb
+    for b in range(nb, n):                                # values for the timed GEMMs below (not timed)
+        red[:, :, b] = red[:, :, b % nb]
+    R = red.reshape(G, n * n, order="F")
+    mat = np.zeros((n, n, n, n), dtype=np.complex128, order="F")
+    t0 = time.perf_counter()
+    for a1 in range(n):                                   # coreproject.f90:1089-1099, row b1 = 0
+        myden = phi[:, a1] * np.conj(phi[:, 0])
+        mat[a1, 0, :, :] = (R.T @ myden).reshape(n, n, order="F")
+    t_twoe = (time.perf_counter() - t0) * n
+    t0 = time.perf_counter()
     rp = orc.get_reducedpot(red, tally)
     orc.actreduced00(sysm, phi, phi, den, inv, rp)
-    return time.perf_counter() - t0
+    t_rest = time.perf_counter() - t0
+    t = t_ci + t_coul + t_twoe + t_rest
+    sample = (f"bounded sample of one orbital-RHS evaluation, numpy/scipy restatement of the reference on {threads} "
+              f"host threads: RDMs {t_ci:.2f} s, Coulomb solves {nb} of {n} op_tinv batches x {n / nb:g} = "
+              f"{t_coul:.2f} s, twoematel {n} of {n * n} rows x {n} = {t_twoe:.2f} s, reducedpot + actreduced00 "
+              f"{t_rest:.2f} s (walk tables: {tables}, set-up)")
+    return t, sample, None
+
+
+def parity_report(w, outputs, ref):
+    """GPU outputs of the timed evaluation (rank 0's seeded inputs) against the
+    oracle: the live CPU evaluation where it ran completely, else the oracle's
+    results frozen in tests/golden/workload_C.npz (same seeds) for that workload."""
+    def rel(x, y):
+        return float(np.abs(x - y).max() / np.abs(y).max())
+    if ref is not None:
+        return {"against": "oracle (numpy/scipy restatement), same seeded inputs, this run",
+                "rhs_rel_err": rel(outputs["rhs"], ref["rhs"]),
+                "twoematel_rel_err": rel(outputs["twoematel"], ref["twoematel"]), "tolerance": 1e-11}
+    gold_path = REPO / "tests" / "golden" / f"workload_{w.name}.npz"
+    if not gold_path.exists():
+        return None
+    gold = np.load(gold_path)
+    pts = gold["points"]
+    return {"against": f"oracle results frozen in tests/golden/{gold_path.name} (same seeded inputs)",
+            "rhs_rel_err": float(np.abs(outputs["rhs"][pts] - gold["rhs_pts"]).max() / gold["rhs_absmax"]),
+            "rhs_points_compared": int(pts.size) * w.nspf,
+            "twoematel_rel_err": rel(outputs["twoematel"], gold["twoematel"]), "tolerance": 1e-11}
 
 
 def run_reference(args):
@@ -169,7 +253,8 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     for _ in range(max(0, min(args.warmup, 1))):
         cpu_reference_eval(w, threads)
-    ts = [cpu_reference_eval(w, threads) for _ in range(max(1, min(args.steps, 3)))]
+    runs = [cpu_reference_eval(w, threads) for _ in range(max(1, min(args.steps, 3)))]
+    ts = [r[0] for r in runs]
     t = float(np.median(ts))
     v = 1.0 / t
     line = {
@@ -178,9 +263,8 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
         "data": "synthetic", "config": workload_config(w, l2="n/a (CPU)"),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{len(ts)} full orbital-RHS evaluations (median), numpy/scipy restatement "
-                                   f"of the reference on {threads} host threads; the Fortran reference has "
-                                   f"no compiler in this image"},
+                         "sample": f"median of {len(ts)}: {runs[-1][1]}; the Fortran reference has no compiler "
+                                   f"in this image"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -190,22 +274,15 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # this implementation
 # ---------------------------------------------------------------------------
-def main():
-    args = parse()
-    if args.impl == "reference":
-        return run_reference(args)
-    rank, world, local = dist_env()
+def measure(w, args, rank, world, local, dist, extras=True, e2e=True, propagation=True):
+    """Device-timed evaluations of workload `w` (inputs resident, L2 flushed
+    between steps), then, with `extras`, the secondary rates, the precision form,
+    the per-stage profile and roofline, CMF steps/s and the end-to-end rate
+    through the host-array entry.  Returns the numbers and rank 0's outputs."""
     import torch
     from sincgpu import SincProject, WalkTables
-    from sincgpu.inputs import WORKLOADS, seeded_orbitals
+    from sincgpu.inputs import seeded_avector, seeded_orbitals
 
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    w = WORKLOADS[args.config]
     n, G = w.nspf, w.G
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
@@ -236,8 +313,6 @@ def main():
         proj.orbital_rhs_avec_dev(phi, avec, den, inv, tally, mat, red, out)
 
     if args.profile_precision_form:
-        if not args.no_extras:
-            raise SystemExit("--profile-precision-form is a profiling mode: use it with --no-extras")
         proj.set_option("coulomb_fp32", 1)
         proj.set_option("contract_tf32", 1)
     for _ in range(args.warmup):
@@ -267,24 +342,22 @@ def main():
         dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
     total_ms = float(t_local.item())
     ms_step = total_ms / args.steps
-    value = world * args.steps / (total_ms / 1e3)
-
-    if args.no_extras:
-        if rank == 0:
-            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                              "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-                              "gpu_launches": int(launches), "note": "profiling run (--no-extras)"}), flush=True)
+    res = {"value": world * args.steps / (total_ms / 1e3), "ms_per_step": ms_step, "clocks": clk,
+           "gpu_launches": int(launches), "launches_per_step": launches / args.steps,
+           "fft_length": proj.fft_length, "numconfig": nc}
+    if rank == 0 and not args.profile_precision_form:
+        res["outputs"] = {"rhs": out.cpu().numpy().T, "twoematel": mat.cpu().numpy().T.reshape((n,) * 4, order="F"),
+                          "phi": phi_h, "avector": a_h}
+    if not extras:
         proj.close()
-        if dist:
-            dist.barrier()
-            dist.destroy_process_group()
-        return 0
+        return res
 
     # ---- secondary rates: orbital-RHS matvec alone, CI sigma alone ----
-    secondary = secondary_rates(proj, torch, stream, flush, phi, den, inv, red, out, mat, avec, n, G)
+    res["secondary"] = secondary_rates(proj, torch, stream, flush, phi, den, inv, red, out, mat, avec, n, G)
 
-    # ---- precision form: Coulomb passes in FP32, everything else FP64 ----
-    precision = precision_form(proj, torch, stream, flush, step, out, mat, args.steps, world, dist, dev)
+    # ---- precision form: Coulomb passes in FP32, reducedpot 3xTF32 ----
+    res["precision_forms"] = precision_form(proj, torch, stream, flush, step, out, mat, max(3, args.steps), world,
+                                            dist, dev)
 
     # ---- per-kernel times (profiled pass, one stream) for the roofline ----
     # the timed evaluations overlap the CI part, the kinetic contraction and
@@ -292,42 +365,77 @@ def main():
     # are taken with that overlap off so that each stage is timed alone
     proj.set_option("rhs_overlap", 0)
     proj.profile(True)
-    nprof = min(20, args.steps)
+    nprof = max(3, min(20, args.steps))
     for _ in range(nprof):
         flush.zero_()
         step()
     prof = proj.profile_read()
     proj.profile(False)
     proj.set_option("rhs_overlap", 1)
-    roofline = make_roofline(w, prof, nprof, dev, proj.fft_length)
-    evaluation_roofline = eval_roofline(w, prof, nprof, dev, proj.fft_length, ms_step)
+    res["roofline"] = make_roofline(w, prof, nprof, dev, proj.fft_length)
+    res["evaluation_roofline"] = eval_roofline(w, prof, nprof, dev, proj.fft_length, ms_step)
+    res["stage_ms_per_step"] = {k: v[0] / nprof for k, v in prof.items()}
+    res["stage_timing"] = "CUDA events per stage on one stream (rhs_overlap 0); the timed value overlaps them"
 
     # ---- CMF propagation steps/s on the same workload ----
-    propagation = cmf_rate(proj, w, phi, avec, torch, local)
+    if propagation:
+        res["propagation"] = cmf_rate(proj, w, phi, avec, torch, local)
 
     # ---- end to end through the host-array C entry (pinned host buffers) ----
-    e2e = None
-    if not args.no_e2e:
-        e2e = run_e2e(proj, w, phi_h, a_h, args, stream, world, dist)
+    if e2e and not args.no_e2e:
+        res["e2e"] = run_e2e(proj, w, phi_h, a_h, args, stream, world, dist)
+    proj.close()
+    return res
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    if args.profile_precision_form and not args.no_extras:
+        raise SystemExit("--profile-precision-form is a profiling mode: use it with --no-extras")
+    rank, world, local = dist_env()
+    import torch
+    from sincgpu import SincProject  # noqa: F401  (fails loudly without the CUDA library)
+    from sincgpu.inputs import WORKLOADS
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    w = WORKLOADS[args.config]
+    head = measure(w, args, rank, world, local, dist, extras=not args.no_extras)
+    outputs = head.pop("outputs", None)
+
+    if args.no_extras:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
+                              "higher_is_better": True, "gpu_launches": head["gpu_launches"],
+                              "config": workload_config(w), "note": "profiling run (--no-extras)"}), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
 
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "complex128",
         "data": "synthetic (seeded Gaussian-envelope orbitals, seeded normalised A-vector)",
-        "config": workload_config(w), "clocks": clk, "gpu_launches": int(launches),
-        "launches_per_step": launches / args.steps, "fft_length": proj.fft_length, "numconfig": nc,
-        "roofline": roofline, "secondary": secondary, "precision_forms": precision,
-        "propagation": propagation,
-        "stage_ms_per_step": {k: v[0] / nprof for k, v in prof.items()},
-        "stage_timing": "CUDA events per stage on one stream (rhs_overlap 0); the timed value overlaps them",
-        "evaluation_roofline": evaluation_roofline,
+        "config": workload_config(w), **{k: v for k, v in head.items() if k not in ("value", "ms_per_step")},
     }
-    if e2e:
-        line["e2e"] = e2e
-    proj.close()
+    # the 41^3 / 10-orbital workload beside the headline (BASELINE's plain FP64 GPU drop-in)
+    sub_outputs = None
+    if args.config != "B" and not args.no_workload_b:
+        wb = WORKLOADS["B"]
+        sub = measure(wb, args, rank, world, local, dist, extras=True, propagation=True)
+        sub_outputs = sub.pop("outputs", None)
+        line["workload_B"] = {"config": workload_config(wb), **sub}
     if not args.no_batched:
-        line["batched"] = batched_form(torch, local, stream, args.batched_count)
+        line["batched"] = batched_form(torch, local, torch.cuda.current_stream(), args.batched_count)
     if not args.no_served:
         line["served"] = {f: served_form(local, f == "mixed_fp32_coulomb", args.served_count, args.served_steps)
                           for f in ("plain_fp64", "mixed_fp32_coulomb")}
@@ -335,10 +443,15 @@ def main():
         line["served"]["mixed_vs_plain_steps_per_s"] = mx["steps_per_s"] / max(pl["steps_per_s"], 1e-30)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        t = cpu_reference_eval(w, threads)
-        line["cpu_baseline"] = {"value": 1.0 / t, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": "1 full orbital-RHS evaluation of the same workload with the "
-                                          "numpy/scipy restatement of the reference"}
+        t, sample, ref = cpu_reference_eval(w, threads, want_outputs=outputs is not None)
+        line["cpu_baseline"] = {"value": 1.0 / t, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        if outputs is not None:
+            line["parity"] = parity_report(w, outputs, ref)
+        if sub_outputs is not None:
+            tb, sample_b, ref_b = cpu_reference_eval(WORKLOADS["B"], threads, want_outputs=True)
+            line["workload_B"]["cpu_baseline"] = {"value": 1.0 / tb, "unit": UNIT, "cores": threads, "kind": "port",
+                                                  "sample": sample_b}
+            line["workload_B"]["parity"] = parity_report(WORKLOADS["B"], sub_outputs, ref_b)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -611,67 +724,83 @@ def _dgemm_tflops(dev):
     return _DGEMM["v"]
 
 
+def measured_peaks():
+    """HBM bandwidth (GB/s) of this GPU pool from MEASURED_PEAKS.json when the
+    file is present, else the pool's earlier STREAM-copy measurement."""
+    try:
+        peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text())
+        return float(peaks["hbm_gbs"]), "of measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "of fallback (6.65 TB/s STREAM copy measured earlier on this pool; MEASURED_PEAKS.json absent)"
+
+
+def coulomb_pass_work(name, N, P, U):
+    """Algorithmic bytes and FP64 flops of one Coulomb pass over U pair densities.
+    Bytes: each pass reads its input slab and writes its output slab once (16-byte
+    complex values; the z pass reads the real kernel spectrum, 8 P^3 bytes, once
+    per launch).  Flops: 5 L log2 L per transformed line of length L = P (the
+    pruned lines only), the pair products (6 per point) in the x pass and the
+    spectrum multiply (2 per value) in the z pass."""
+    fl = 5.0 * P * math.log2(P)
+    by = {"coul_fwd_x": 16.0 * (2 * N ** 3 + N * N * P) * U,   # phi_a, phi_b in; W1 out
+          "coul_fwd_y": 16.0 * (N * N * P + N * P * P) * U,
+          "coul_z": 32.0 * N * P * P * U + 8.0 * P ** 3,
+          "coul_inv_y": 16.0 * (N * P * P + N * N * P) * U,
+          "coul_inv_x": 16.0 * (N * N * P + N ** 3) * U}[name]
+    lines = {"coul_fwd_x": N * N, "coul_fwd_y": N * P, "coul_z": 2 * P * P, "coul_inv_y": N * P,
+             "coul_inv_x": N * N}[name]
+    extra = {"coul_fwd_x": 6.0 * N ** 3, "coul_z": 2.0 * P ** 3}.get(name, 0.0)
+    return by, (lines * fl + extra) * U
+
+
 def make_roofline(w, prof, nprof, dev, proj_fft_length=None):
-    """Dominant kernel of the step with its algorithmic bytes or flops per launch."""
-    import torch
+    """Dominant kernel of the step (largest summed time in the per-stage profile)
+    with its algorithmic bytes or flops per launch.  Coulomb passes and the
+    element-wise RHS kernels are booked against HBM; the FP64 GEMMs (twoematel,
+    reducedpot, the kinetic contraction: FP64 tensor cores, mma.sync f64) against
+    a cuBLAS DGEMM measured in this run."""
     if not prof:
         return None
     name, (ms, nl) = max(prof.items(), key=lambda kv: kv[1][0])
     per_launch_ms = ms / nl
     n, G, N = w.nspf, w.G, w.numpoints
     U = n * (n + 1) // 2
-    peaks = {}
-    try:
-        peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text())
-    except Exception:
-        pass
-    hbm = peaks.get("hbm_gbs", 6650.0)
-    hbm_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
+    hbm, hbm_src = measured_peaks()
     launches_per_step = nl / nprof
+    base = {"kernel": name, "launch_ms": per_launch_ms, "launches_per_step": launches_per_step,
+            "traffic": TRAFFIC.get((name, N, n)),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, profiles/"
+            if TRAFFIC.get((name, N, n)) else None}
     if name in ("rp_gemm", "twoe_gemm", "ke_xy", "ke_z"):
-        # FP64 contraction: achieved FLOP/s against an in-run cuBLAS DGEMM
         dgemm = _dgemm_tflops(dev)
-        flops = {"rp_gemm": 2.0 * G * 2 * U * 2 * n * n, "twoe_gemm": 2.0 * G * (2 * U) ** 2,
+        flops = {"rp_gemm": 2.0 * G * 2 * U * n * (n + 1), "twoe_gemm": 2.0 * G * (2 * U) ** 2,
                  "ke_xy": 2 * 2 * 2.0 * N ** 3 * N * n, "ke_z": 2 * 2.0 * N ** 3 * N * n}[name] / launches_per_step
         ach = flops / (per_launch_ms / 1e3) / 1e12
-        return {"kernel": name, "bound": "tensor", "achieved": ach, "peak": dgemm, "unit": "TFLOP/s",
-                "frac": ach / dgemm, "traffic": TRAFFIC.get((name, N, n)), "launch_ms": per_launch_ms,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64; the measured-peaks file has no FP64 figure)"}
+        return {**base, "bound": "tensor", "precision": "fp64 (mma.sync f64)", "achieved": ach, "peak": dgemm,
+                "unit": "TFLOP/s", "frac": ach / dgemm,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor cores; "
+                               "MEASURED_PEAKS.json holds no FP64 figure)"}
     P = proj_fft_length
     if name.startswith("coul_"):
-        # FP64 compute bound (ncu: FP64 pipe busy, DRAM a small fraction): algorithmic
-        # flops 5 L log2 L per length-L line (pruned lines only) plus the spectrum
-        # multiply and the pair products, against the in-run FP64 DGEMM
-        fl = 5.0 * P * math.log2(P)
-        lines = {"coul_fwd_x": N * N, "coul_fwd_y": N * P, "coul_z": 2 * P * P, "coul_inv_y": N * P,
-                 "coul_inv_x": N * N}[name]
-        extra = {"coul_fwd_x": 6.0 * N ** 3, "coul_z": 6.0 * P ** 3}.get(name, 0.0)
-        flops = (lines * fl + extra) * U / launches_per_step
+        by, flops = coulomb_pass_work(name, N, P, U)
+        by /= launches_per_step
+        flops /= launches_per_step
+        ach = by / (per_launch_ms / 1e3) / 1e9
         dgemm = _dgemm_tflops(dev)
-        ach = flops / (per_launch_ms / 1e3) / 1e12
-        return {"kernel": name, "bound": "tensor", "compute": "FP64 on CUDA cores", "achieved": ach,
-                "peak": dgemm, "unit": "TFLOP/s", "frac": ach / dgemm, "traffic": TRAFFIC.get((name, N, n)),
-                "launch_ms": per_launch_ms, "launches_per_step": launches_per_step,
-                "peak_source": "FP64 ceiling: cuBLAS DGEMM 8192^3 measured in this run (the measured-peaks file "
-                               "has no FP64 figure)",
-                "flops_per_launch": flops}
-    bytes_per_pair = {
-        "coul_fwd_x": 16.0 * (2 * N ** 3 + N * N * P),
-        "coul_fwd_y": 16.0 * (N * N * P + N * P * P),
-        "coul_z": 16.0 * (2 * N * P * P) + 16.0 * P ** 3,
-        "coul_inv_y": 16.0 * (N * P * P + N * N * P),
-        "coul_inv_x": 16.0 * (N * N * P + N ** 3),
-    }
-    if name in bytes_per_pair:
-        by = bytes_per_pair[name] * U / launches_per_step
-    elif name == "rhs_redpot":
+        fp64 = flops / (per_launch_ms / 1e3) / 1e12
+        return {**base, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "peak_source": hbm_src, "algorithmic_bytes_per_launch": by,
+                "fp64": {"bound": "fp64", "achieved": fp64, "peak": dgemm, "unit": "TFLOP/s",
+                         "frac": fp64 / dgemm, "flops_per_launch": flops,
+                         "peak_source": "cuBLAS DGEMM 8192^3 in this run (FFT butterflies run on the FP64 "
+                                        "CUDA-core pipe, whose peak equals it on B200)"}}
+    if name == "rhs_redpot":
         by = 16.0 * G * (n * n + 3 * n)
     else:
         by = 16.0 * G * n * 2
     ach = by / (per_launch_ms / 1e3) / 1e9
-    return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-            "frac": ach / hbm, "traffic": TRAFFIC.get((name, N, n)), "launch_ms": per_launch_ms,
-            "peak_source": hbm_src}
+    return {**base, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+            "peak_source": hbm_src, "algorithmic_bytes_per_launch": by}
 
 
 def eval_roofline(w, prof, nprof, dev, P, ms_step):
@@ -682,19 +811,12 @@ def eval_roofline(w, prof, nprof, dev, P, ms_step):
         return None
     n, G, N = w.nspf, w.G, w.numpoints
     U = n * (n + 1) // 2
-    try:
-        hbm = json.loads((REPO / "MEASURED_PEAKS.json").read_text())["hbm_gbs"] * 1e9
-    except Exception:
-        hbm = 6650.0e9
+    hbm = measured_peaks()[0] * 1e9
     fp64 = _dgemm_tflops(dev) * 1e12
-    fl = 5.0 * P * math.log2(P)
     stages = {
         # name: (algorithmic bytes, algorithmic flops) per evaluation
-        "coul_fwd_x": (16.0 * (2 * N ** 3 + N * N * P) * U, (N * N * fl + 6.0 * N ** 3) * U),
-        "coul_fwd_y": (16.0 * (N * N * P + N * P * P) * U, N * P * fl * U),
-        "coul_z": ((16.0 * 2 * N * P * P) * U + 16.0 * P ** 3, (2 * P * P * fl + 6.0 * P ** 3) * U),
-        "coul_inv_y": (16.0 * (N * P * P + N * N * P) * U, N * P * fl * U),
-        "coul_inv_x": (16.0 * (N * N * P + N ** 3) * U, N * N * fl * U),
+        **{k: coulomb_pass_work(k, N, P, U) for k in ("coul_fwd_x", "coul_fwd_y", "coul_z", "coul_inv_y",
+                                                      "coul_inv_x")},
         "twoe_gemm": (16.0 * G * (n + 2 * U), 2.0 * G * (2 * U) ** 2),
         "rp_gemm": (8.0 * G * 2 * U + 16.0 * G * n * n, 2.0 * G * 2 * U * n * (n + 1)),
         "ke_xy": (16.0 * G * n * 2, 2 * 2 * 2.0 * N ** 3 * N * n),

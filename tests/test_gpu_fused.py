@@ -119,14 +119,15 @@ def test_avec_reducedpot_mirror_equals_full(li):
     assert err < 1e-13
 
 
-def test_reducedpot_dmma_matches_dfma(built_lib):
+@pytest.mark.parametrize("n", [7, 10])
+def test_reducedpot_dmma_matches_dfma(built_lib, n):
     """The FP64 tensor-core (DMMA) reducedpot and twoematel GEMMs against the
     register-tiled DFMA ones on the same mean-field inputs: both FP64, different
-    summation order."""
+    summation order.  n = 10 runs the widest one-tile instances (twoematel tile
+    R = 7, reducedpot FN = 7 with the fused apply)."""
     import torch
     from oracle import sinc_oracle as orc
     from sincgpu import SincProject, WalkTables
-    n = 7
     p = SincProject(21, 0.4, [[0, 0, 0]], [2.0], n)
     try:
         sysm = orc.SincSystem(21, 0.4, [[0, 0, 0]], [2.0])
@@ -152,3 +153,31 @@ def test_reducedpot_dmma_matches_dfma(built_lib):
         assert err < 1e-13, err
     finally:
         p.close()
+
+
+@pytest.mark.parametrize("n,numelec,ms", [(8, 3, 1), (9, 2, 0), (10, 2, 0)])
+def test_orbital_rhs_avec_wide_column_tiles(built_lib, n, numelec, ms):
+    """The A-vector entry at 8, 9 and 10 orbitals: n(n+1) = 72, 90, 110 half
+    columns, so the fused reducedpot + apply kernel runs its FN = 5, 6, 7
+    instances and twoematel its R = 5, 6, 7 one-tile symmetric instances (the
+    instances behind the 41^3 / 10-orbital benchmark), against the oracle."""
+    from sincgpu import SincProject, WalkTables
+    sysm = orc.SincSystem(15, 0.5, [[0, 0, 2], [0, 0, -2]], [1.0, 2.0])
+    gpu = SincProject(15, 0.5, [[0, 0, 2], [0, 0, -2]], [1.0, 2.0], n)
+    try:
+        gpu.ci_attach(WalkTables(numelec, n, ms))
+        ow = CIWalks(numelec, n, ms)
+        phi = orc.seeded_orbitals(sysm, n, seed=50 + n)
+        rng = np.random.default_rng(60 + n)
+        a = rng.standard_normal(ow.numconfig) + 1j * rng.standard_normal(ow.numconfig)
+        a /= np.linalg.norm(a)
+        den = ow.getdenmat00(a)
+        inv = orc.invmatsmooth(den)
+        tally = ow.get_tworeducedx(a)
+        _, red = sysm.call_twoe_matel00(phi, phi)
+        rp = orc.get_reducedpot(red, tally)
+        ref = orc.actreduced00(sysm, phi, phi, den, inv, rp, ztdpot=0.01)
+        out = gpu.orbital_rhs_avec(phi, a, ztdpot=0.01)
+        assert relerr(out, ref) < TOL
+    finally:
+        gpu.close()

@@ -110,3 +110,22 @@ def test_spin_projector_is_idempotent_symmetric():
     sp = SpinSets(CIWalks(4, 6, 0), 2)
     for p in sp.projectors:
         assert np.abs(p @ p - p).max() < 1e-13 and np.abs(p - p.T).max() == 0.0
+
+
+def test_tables_bit_exact_4e16o_frozen_oracle(built_lib):
+    """The 14400-determinant walk tables of the 81^3 / 16-orbital workload
+    against the oracle's, frozen as SHA-256 digests of each int32 table in
+    tests/golden/workload_C.npz (the pure-Python oracle needs minutes here)."""
+    import hashlib
+    from pathlib import Path
+    from sincgpu import WalkTables
+    gold = np.load(Path(__file__).resolve().parent / "golden" / "workload_C.npz")
+    w = WalkTables(4, 16, 0)
+    try:
+        assert w.numconfig == int(gold["numconfig"])
+        for name, sha, ln in zip(gold["table_names"], gold["table_sha256"], gold["table_len"]):
+            t = np.ascontiguousarray(w.table(str(name)), dtype=np.int32)
+            assert t.size == int(ln), name
+            assert hashlib.sha256(t.tobytes()).hexdigest() == str(sha), name
+    finally:
+        w.close()

@@ -63,6 +63,13 @@ def seeded_orbitals(numpoints: int, spacing: float, nspf: int, seed: int, width:
     return out
 
 
+def seeded_avector(numconfig: int, seed: int):
+    """A-vector with seeded complex-normal coefficients, normalised."""
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal(numconfig) + 1j * rng.standard_normal(numconfig)
+    return a / np.linalg.norm(a)
+
+
 def seeded_hermitian_psd(n: int, seed: int):
     rng = np.random.default_rng(seed)
     a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
