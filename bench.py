@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--profile-precision-form", action="store_true",
                     help="with --no-extras: time the precision form (FP32 Coulomb passes, 3xTF32 "
                          "tensor-core reducedpot) instead of the FP64 form")
+    ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
+                    help="context option for the measured workloads (sincgpu_set_option), e.g. coul_fused=1")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--batched-count", type=int, default=64)
@@ -288,6 +290,9 @@ def measure(w, args, rank, world, local, dist, extras=True, e2e=True, propagatio
     stream = torch.cuda.current_stream()
     proj = SincProject(w.numpoints, w.spacing, w.centershift, w.nuccharges, n, device=local)
     proj.set_stream(stream.cuda_stream)
+    for opt in args.option:
+        name, value = opt.split("=")
+        proj.set_option(name, int(value))
     walks = WalkTables(w.numelec, n, 0)
     proj.ci_attach(walks)
     nc = walks.numconfig

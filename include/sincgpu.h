@@ -190,10 +190,14 @@ int sincgpu_mean_field_dev(sincgpu_ctx* ctx, const double* phi, const double* re
  * twoereduced(totpoints,allsize), enqueued on the context stream.  The FFT
  * scratch is a fixed 64 MiB device array inside the library (held on every GPU
  * that loads it until exit); one density needs 16*(N*N*P + N*P*P) bytes of it
- * (P = sincgpu_fft_length) and larger grids are rejected with SINCGPU_ERANGE.
- * All calls share the array: calls that overlap on the GPU race.  The first
- * call on a device looks up the array's address; make it before any stream
- * capture. */
+ * in the FP64 form and 8*(N*N*P + N*P*P) with the context option coulomb_fp32
+ * (P = sincgpu_fft_length); larger grids are rejected with SINCGPU_ERANGE.
+ * The FP32 form also needs the context's FP32 twiddle and kernel-spectrum
+ * tables, which this entry does not allocate: after setting coulomb_fp32, make
+ * one allocating Coulomb call (e.g. sincgpu_op_tinv) first, else this entry
+ * returns SINCGPU_ESTATE.  All calls share the array: calls that overlap on the
+ * GPU race.  The first call on a device looks up the array's address; make it
+ * before any stream capture. */
 int sincgpu_op_tinv_noalloc_dev(sincgpu_ctx* ctx, const double* twoeden03, double* twoereduced,
                                 int allsize);
 int sincgpu_actreduced_dev(sincgpu_ctx* ctx, int dentimeflag, const double* inspfs,

@@ -116,8 +116,10 @@ class _Slot:
 
 
 class CmfOracle:
-    def __init__(self, sysm, numelec, restrictms, phi, avec, params: CmfParams, spinrestrictval=None):
+    def __init__(self, sysm, numelec, restrictms, phi, avec, params: CmfParams, spinrestrictval=None,
+                 workers=1):
         self.sysm, self.p = sysm, params
+        self.workers = workers          # FFT threads of the Coulomb solves (same transforms)
         n = phi.shape[1]
         self.n = n
         self.ow = CIWalks(numelec, n, restrictms)
@@ -143,7 +145,7 @@ class CmfOracle:
 
     def all_matel(self):
         s, sysm = self.s0, self.sysm
-        s.mat, self.twoereduced = sysm.call_twoe_matel00(s.spfs, s.spfs)
+        s.mat, self.twoereduced = sysm.call_twoe_matel00(s.spfs, s.spfs, workers=self.workers)
         ph = np.conj(s.spfs).T
         pot, ke, z = ph @ sysm.mult_pot(s.spfs), ph @ sysm.mult_ke(s.spfs), ph @ sysm.mult_zdipole(s.spfs)
         s.hops = (self.ow.assemble_doubles(s.mat), self.ow.assemble_singles(pot), self.ow.assemble_singles(ke),

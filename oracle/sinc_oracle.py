@@ -298,9 +298,11 @@ class SincSystem:
         g = self.N
         x = np.asarray(inp, dtype=np.complex128).reshape(g, g, g, -1, order="F")
         K = self.ketot
-        out = np.einsum("lj,lyzm->jyzm", K, x)
-        out = out + np.einsum("lj,xlzm->xjzm", K, x)
-        out = out + np.einsum("lj,xylm->xyjm", K, x)
+        # the three contractions as tensordots (BLAS); same sums as the
+        # reference's per-axis ZGEMMs, summation order aside
+        out = np.tensordot(K, x, axes=([0], [0]))                               # (j, y, z, m)
+        out = out + np.moveaxis(np.tensordot(x, K, axes=([1], [0])), 3, 1)      # (x, j, z, m)
+        out = out + np.moveaxis(np.tensordot(x, K, axes=([2], [0])), 3, 2)      # (x, y, j, m)
         return np.asfortranarray(out).reshape(self.G, -1, order="F")
 
     def mult_pot(self, inp):

@@ -70,3 +70,38 @@ def test_expoavecprop_with_field(ci):
                                    ezfield=ez)
     assert nstep == info["nstep"]
     assert np.abs(w - complexify(w_ref)).max() < 1e-11
+
+
+@pytest.mark.parametrize("nspf", [8, 9, 11], ids=["2x1568", "4x2592", "loop6050"])
+def test_expoavecprop_long_vectors(built_lib, nspf):
+    """4 electrons in 8, 9 and 11 orbitals: 784, 1296 and 3025 determinants, so the
+    real-ified Krylov vectors have 1568 and 2592 entries (the register-resident
+    Gram-Schmidt kernel with two and four values per thread) and 6050 (the
+    looping kernel beyond 4096), against the oracle's DGEXPV."""
+    from sincgpu import SincProject, WalkTables
+    sysm = orc.SincSystem(15, 0.5, [[0, 0, 0]], [2.0])
+    gpu = SincProject(15, 0.5, [[0, 0, 0]], [2.0], nspf)
+    try:
+        gpu.ci_attach(WalkTables(4, nspf, 0))
+        ow = CIWalks(4, nspf, 0)
+        phi = orc.seeded_orbitals(sysm, nspf, seed=33)
+        mat, _ = sysm.call_twoe_matel00(phi, phi)
+        ph = np.conj(phi).T
+        pot, ke, z = ph @ sysm.mult_pot(phi), ph @ sysm.mult_ke(phi), ph @ sysm.mult_zdipole(phi)
+        gpu.assemble_sparsemats(mat, pot, ke, z)
+        xp, xo, xk = ow.assemble_doubles(mat), ow.assemble_singles(pot), ow.assemble_singles(ke)
+        rng = np.random.default_rng(34)
+        a = rng.standard_normal(ow.numconfig) + 1j * rng.standard_normal(ow.numconfig)
+        a /= np.linalg.norm(a)
+        dt, m = 0.05, 12
+        tf = -1j * dt
+        mv = lambda x: realify(tf * ow.sparsesparsemult(complexify(x), xp, xo, xk,  # noqa: E731
+                                                        constant=sysm.nucrepulsion))
+        w_ref, g_ref, info = dgexpv(2 * ow.numconfig, m, 1.0, realify(a), 1e-9, dt, mv,
+                                    lambda u, v: float(u @ v), 1.0, 2 * ow.numconfig - 1)
+        w, g, nstep = gpu.expoavecprop(a, 1.0, krylovdim=m, tol=1e-9, anorm=dt, stepguess=1.0, timefac=tf)
+        assert nstep == info["nstep"]
+        assert g == pytest.approx(g_ref, rel=1e-12)
+        assert np.abs(w - complexify(w_ref)).max() < 1e-11
+    finally:
+        gpu.close()

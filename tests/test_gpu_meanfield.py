@@ -108,8 +108,8 @@ def test_call_twoe_matel00_multitile(built_lib, nspf, general):
 
 
 def test_coulomb_tma_z_pass_matches_plain(h2):
-    """The TMA-staged persistent z pass (default) against the plain z pass on the
-    same densities: same transforms, the kernel spectrum's real part only (its
+    """The TMA-staged persistent z pass (option coul_tma = 1; the automatic choice
+    is the plain pass) against the plain z pass on the same densities: same transforms, the kernel spectrum's real part only (its
     imaginary part is rounding noise), so agreement to 1e-14; no timeouts."""
     sysm, gpu = h2
     rng = np.random.default_rng(7)

@@ -60,3 +60,35 @@ def test_noalloc_rejects_grid_beyond_fixed_scratch(built_lib):
             _call("sincgpu_op_tinv_noalloc_dev", proj._h, _ptr(d), _ptr(o), 1)
     finally:
         proj.close()
+
+
+def test_noalloc_fp32_form(built_lib):
+    """With coulomb_fp32 the entry needs the FP32 tables, which it does not
+    allocate: on a fresh context it refuses (SINCGPU_ESTATE); after one
+    allocating solve it matches the regular FP32 entry, twice in a row."""
+    import torch
+    from sincgpu import SincProject, SincGpuError
+    from sincgpu.capi import _call, _ptr
+
+    N, m = 25, 4
+    G = N ** 3
+    rng = np.random.default_rng(25)
+    dens = np.asfortranarray(rng.standard_normal((G, m)) + 1j * rng.standard_normal((G, m)))
+    d_in = torch.from_numpy(np.ascontiguousarray(dens.T)).cuda()
+    d_out = torch.empty_like(d_in)
+    proj = SincProject(N, 0.4, [[0, 0, 0]], [1.0], 2)
+    try:
+        proj.set_option("coulomb_fp32", 1)
+        with pytest.raises(SincGpuError, match="FP32"):
+            _call("sincgpu_op_tinv_noalloc_dev", proj._h, _ptr(d_in), _ptr(d_out), m)
+        ref = proj.op_tinv(dens)                       # allocating FP32 solve: builds the tables
+        for _ in range(2):
+            d_out.fill_(float("nan"))
+            torch.cuda.synchronize()
+            _call("sincgpu_op_tinv_noalloc_dev", proj._h, _ptr(d_in), _ptr(d_out), m)
+            proj.synchronize()
+            out = d_out.cpu().numpy().T
+            assert np.isfinite(out).all()
+            assert relerr(out, ref) < TOL
+    finally:
+        proj.close()
