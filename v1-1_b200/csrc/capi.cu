@@ -94,7 +94,7 @@ Ctx::~Ctx() {
   if (stream) cudaStreamSynchronize(stream);
   if (rhs_graph) cudaDeviceSynchronize();
   for (void* p : {(void*)d_kevect, (void*)d_ketile, (void*)d_pot, (void*)d_zdip, (void*)d_tcoul, (void*)d_khat,
-                  (void*)d_roots, (void*)d_khat32, (void*)d_roots32})
+                  (void*)d_roots, (void*)d_khat32, (void*)d_roots32, (void*)d_khT, (void*)d_khT32})
     dfree(*this, p);
   ws_fft.release();
   ws_pairs.release();
@@ -363,6 +363,11 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
   if (!strcmp(name, "rp_dmma")) {
     SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "rp_dmma must be 0 or 1");
     h->c.rp_dmma = (int)value;
+    return SINCGPU_OK;
+  }
+  if (!strcmp(name, "coul_fused")) {
+    SG_CHECK(value >= -1 && value <= 1, SINCGPU_EINVAL, "coul_fused must be -1, 0 or 1");
+    h->c.coul_fused = (int)value;
     return SINCGPU_OK;
   }
   if (!strcmp(name, "coul_tma")) {

@@ -29,7 +29,7 @@ struct Workspace {
 enum Stage {
   ST_COUL_FWD_X = 0, ST_COUL_FWD_Y, ST_COUL_Z, ST_COUL_INV_Y, ST_COUL_INV_X,
   ST_TWOE_GEMM, ST_TWOE_FINISH, ST_RP_W, ST_RP_GEMM, ST_KE_XY, ST_KE_Z,
-  ST_RHS_MIX, ST_RHS_REDPOT, ST_RHS_PROJ, ST_CI, ST_OTHER, ST_COUNT
+  ST_RHS_MIX, ST_RHS_REDPOT, ST_RHS_PROJ, ST_CI, ST_OTHER, ST_COUL_YZY, ST_COUNT
 };
 
 struct Prof {
@@ -156,6 +156,8 @@ struct Ctx {
   double2* d_roots = nullptr;   // exp(-2 pi i m / P)              (P)
   float2* d_khat32 = nullptr;   // FP32 copies for the precision form, made on demand
   float2* d_roots32 = nullptr;
+  double* d_khT = nullptr;      // real part of d_khat as [kx][kz][ky], three-pass Coulomb form (on demand)
+  float* d_khT32 = nullptr;
 
   // ---- scratch --------------------------------------------------------------
   Workspace ws_fft;     // W1 + W2 of the Coulomb passes
@@ -181,6 +183,7 @@ struct Ctx {
   int coul_fp32 = 0;    // 1: Coulomb passes in FP32 (precision form), 0: FP64
   int contract_tf32 = 0;  // 1: reducedpot contraction as 3xTF32 on the tensor cores
   int coul_tma = -1;      // TMA-staged persistent z pass: 1 on, 0 off, -1 automatic (off)
+  int coul_fused = 0;     // three-pass Coulomb form (y, z, inverse y per plane on chip): 1 on where it fits, 0 off, -1 automatic
   int rp_dmma = 1;        // 1: FP64 reducedpot GEMM on the FP64 tensor cores (DMMA), 0: DFMA tiles
   int twoe_dmma = 1;      // 1: FP64 twoematel GEMM on the FP64 tensor cores (DMMA), 0: DFMA tiles
   int twoe_tile = 0;      // twoematel tile edge 16R: 0 = least padding, 2..9 = that R
@@ -252,6 +255,8 @@ int choose_plan(Ctx& c);
 int make_khat(Ctx& c);
 // FP32 roots and kernel spectrum (rounded once from the FP64 tables)
 int ensure_fp32_tables(Ctx& c);
+// real kernel spectrum transposed to [kx][kz][ky] (FP64, and FP32 with fp32)
+int ensure_khT(Ctx& c, bool fp32);
 
 // coulomb.cu: R_p = T * (phi1_a conj(phi2_b)) for pairs p=(a_p,b_p).
 // Rpl (device) receives the planar real/imag parts: Rpl[p*G+x] = Re, Rpl[(npair+p)*G+x] = Im.

@@ -73,6 +73,13 @@ const double2* khat_of<double2>(const Ctx& c) { return c.d_khat; }
 template <>
 const float2* khat_of<float2>(const Ctx& c) { return c.d_khat32; }
 
+template <class C>
+static const typename CplxTraits<C>::Real* khT_of(const Ctx& c);
+template <>
+const double* khT_of<double2>(const Ctx& c) { return c.d_khT; }
+template <>
+const float* khT_of<float2>(const Ctx& c) { return c.d_khT32; }
+
 // cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda).
 static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
@@ -113,7 +120,13 @@ template <class C>
 static int coul_run_t(Ctx& c, const double2* src1, const double2* src2, const int* h_pa,
                       const int* h_pb, int npair, double* Rpl, double2* full, bool herm, bool dens) {
   const int N = c.N, P = c.P;
-  const long long per_pair = (long long)sizeof(C) * ((long long)N * N * P + (long long)N * P * P);
+  // three-pass form (plane kernel on chip, no W2) where its plane fits shared memory
+  int fused = 0;
+  if (c.coul_fused != 0 && c.coul_tma <= 0) {
+    int p1 = 0, p2 = 0;
+    if (fft_length_for(P, &p1, &p2) == P) fused = yzy_cluster<C>(p1, p2, N);
+  }
+  const long long per_pair = (long long)sizeof(C) * ((long long)N * N * P + (fused ? 0LL : (long long)N * P * P));
   int chunk = c.coul_chunk;
   if (chunk <= 0) {
     const long long budget = kCoulChunkBudget;
@@ -135,8 +148,13 @@ static int coul_run_t(Ctx& c, const double2* src1, const double2* src2, const in
   ca.roots = roots_of<C>(c);
   ca.khat = khat_of<C>(c);
   ca.W1 = (C*)c.ws_fft.ptr;
-  ca.W2 = ca.W1 + (long long)chunk * N * N * P;
+  ca.W2 = fused ? nullptr : ca.W1 + (long long)chunk * N * N * P;
   ca.npair_total = npair;
+  ca.fused = fused;
+  if (fused) {
+    SG_TRY(ensure_khT(c, sizeof(C) == 8));
+    ca.khT = khT_of<C>(c);
+  }
   // TMA-staged z pass: one map over the chunk's W2 (the last, shorter chunk
   // only addresses its first pairs)
   // automatic choice: the plain pass.  With chunks of a few pairs the staged pass
@@ -145,7 +163,7 @@ static int coul_run_t(Ctx& c, const double2* src1, const double2* src2, const in
   // 4.8 vs 5.4 ms FP64, 2.1 vs 2.5 ms FP32; 81: 0.16 vs 0.18 ms), its three
   // resident CTAs per SM hiding the W2 latency better than two staged ones
   CUtensorMap zmap;
-  const bool want_tma = c.coul_tma > 0;
+  const bool want_tma = c.coul_tma > 0 && !fused;
   const bool use_tma = want_tma && make_zmap<C>(c, ca.W2, chunk, &zmap);
   int* err = nullptr;
   if (use_tma) {

@@ -46,6 +46,8 @@ struct CoulArgs {
   const int* pb;
   int pair0;        // index of the chunk's first pair in the full list
   int npair_total;  // planar output: Re at pair p, Im at npair_total + p
+  int fused;        // 0: five passes (W1, W2); 1, 2, 4, 8: three passes (W1T), plane kernel on clusters of that size
+  const typename CplxTraits<C>::Real* khT;  // real kernel spectrum [kx][kz][ky] (three-pass form)
 };
 
 template <class C>
@@ -323,7 +325,12 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   }
 }
 
-// Launches the five passes for one chunk of np pairs.  With `zmap` (a tensor map
+}  // namespace sincgpu
+#include "coulomb_fused.cuh"
+namespace sincgpu {
+
+// Launches the five passes for one chunk of np pairs (or, with ca.fused, the
+// three passes of coulomb_fused.cuh).  With `zmap` (a tensor map
 // of the chunk's W2 as [pair][z][2 P^2 reals]) the z pass is the TMA-staged
 // persistent kernel, else the plain one.
 template <int P1, int P2, class C>
@@ -338,6 +345,35 @@ int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2*
   // (y passes) and f = ky*P + kx (z pass)
   constexpr int TLZ = lines_for_z<C>(P);
   const int nrow = ceil_div(N * N, TL), ncol = ceil_div(N * P, TL), nzc = ceil_div(P * P, TLZ);
+  if (ca.fused) {
+    {
+      ProfScope ps(c, ST_COUL_FWD_X);
+      if (dens)
+        coul_fwd_xT_t<P1, P2, true, C><<<dim3(nrow, 1, np), nthr, 0, c.stream>>>(src1, nullptr, ca);
+      else
+        coul_fwd_xT_t<P1, P2, false, C><<<dim3(nrow, 1, np), nthr, 0, c.stream>>>(src1, src2, ca);
+      SG_LAUNCHED();
+    }
+    {
+      ProfScope ps(c, ST_COUL_YZY);
+      switch (ca.fused) {
+        case 1: SG_TRY((launch_yzy<P1, P2, C, 1>(c, ca, np, ca.khT))); break;
+        case 2: SG_TRY((launch_yzy<P1, P2, C, 2>(c, ca, np, ca.khT))); break;
+        case 4: SG_TRY((launch_yzy<P1, P2, C, 4>(c, ca, np, ca.khT))); break;
+        default: SG_TRY((launch_yzy<P1, P2, C, 8>(c, ca, np, ca.khT))); break;
+      }
+      SG_LAUNCHED();
+    }
+    {
+      ProfScope ps(c, ST_COUL_INV_X);
+      if (dens)
+        coul_inv_xT_t<P1, P2, true, C><<<dim3(nrow, 1, np), nthr, 0, c.stream>>>(ca, Rpl, full, 0);
+      else
+        coul_inv_xT_t<P1, P2, false, C><<<dim3(nrow, 1, np), nthr, 0, c.stream>>>(ca, Rpl, full, herm ? 1 : 0);
+      SG_LAUNCHED();
+    }
+    return SINCGPU_OK;
+  }
   {
     ProfScope ps(c, ST_COUL_FWD_X);
     if (dens)

@@ -480,11 +480,15 @@ int make_khat(Ctx& c) {
   const int P = c.P;
   const long long P3 = (long long)P * P * P;
   dfree(c, c.d_khat);
-  dfree(c, c.d_khat32);  // FP32 copies follow the FP64 tables
+  dfree(c, c.d_khat32);  // FP32 copies and the transposed spectra follow the FP64 tables
   dfree(c, c.d_roots32);
+  dfree(c, c.d_khT);
+  dfree(c, c.d_khT32);
   c.d_khat = nullptr;
   c.d_khat32 = nullptr;
   c.d_roots32 = nullptr;
+  c.d_khT = nullptr;
+  c.d_khT32 = nullptr;
   SG_TRY(dalloc(c, &c.d_khat, sizeof(double2) * P3));
   embed_kernel<<<ceil_div(P3, 256), 256, 0, c.stream>>>(c.d_khat, c.d_tcoul, c.N, P);
   SG_LAUNCHED();
@@ -529,6 +533,35 @@ int ensure_fp32_tables(Ctx& c) {
     narrow_kernel<<<1, 256, 0, c.stream>>>(c.d_roots32, c.d_roots, c.P);
     SG_LAUNCHED();
   }
+  SG_CUDA(cudaStreamSynchronize(c.stream));
+  return SINCGPU_OK;
+}
+
+// khT[(kx P + kz) P + ky] = Re khat[(kz P + ky) P + kx], and its FP32 rounding
+template <class R>
+__global__ void khat_transpose_kernel(R* __restrict__ out, const double2* __restrict__ in, int P) {
+  const long long P3 = (long long)P * P * P;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < P3;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long kx = i / ((long long)P * P);
+    const long long rem = i - kx * P * P;
+    const long long kz = rem / P, ky = rem - kz * P;
+    out[i] = (R)in[(kz * P + ky) * P + kx].x;
+  }
+}
+
+int ensure_khT(Ctx& c, bool fp32) {
+  if (fp32 ? c.d_khT32 != nullptr : c.d_khT != nullptr) return SINCGPU_OK;  // no stream work once built
+  const long long P3 = (long long)c.P * c.P * c.P;
+  const int grid = (int)std::min<long long>(ceil_div(P3, 256), 148 * 16);
+  if (fp32) {
+    SG_TRY(dalloc(c, &c.d_khT32, sizeof(float) * P3));
+    khat_transpose_kernel<float><<<grid, 256, 0, c.stream>>>(c.d_khT32, c.d_khat, c.P);
+  } else {
+    SG_TRY(dalloc(c, &c.d_khT, sizeof(double) * P3));
+    khat_transpose_kernel<double><<<grid, 256, 0, c.stream>>>(c.d_khT, c.d_khat, c.P);
+  }
+  SG_LAUNCHED();
   SG_CUDA(cudaStreamSynchronize(c.stream));
   return SINCGPU_OK;
 }

@@ -265,7 +265,7 @@ class SincProject:
 
     STAGES = ("coul_fwd_x", "coul_fwd_y", "coul_z", "coul_inv_y", "coul_inv_x", "twoe_gemm",
               "twoe_finish", "rp_w", "rp_gemm", "ke_xy", "ke_z", "rhs_mix", "rhs_redpot",
-              "rhs_proj", "ci", "other")
+              "rhs_proj", "ci", "other", "coul_yzy")
 
     def profile(self, enable: bool = True):
         _call("sincgpu_profile", self._h, 1 if enable else 0)
