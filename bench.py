@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--profile-precision-form", action="store_true",
                     help="with --no-extras: time the precision form (FP32 Coulomb passes, 3xTF32 "
                          "tensor-core reducedpot) instead of the FP64 form")
+    ap.add_argument("--stages", action="store_true",
+                    help="with --no-extras: also time each stage on one stream (per-stage CUDA events)")
     ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
                     help="context option for the measured workloads (sincgpu_set_option), e.g. coul_fused=1")
     ap.add_argument("--no-batched", action="store_true")
@@ -354,6 +356,15 @@ def measure(w, args, rank, world, local, dist, extras=True, e2e=True, propagatio
         res["outputs"] = {"rhs": out.cpu().numpy().T, "twoematel": mat.cpu().numpy().T.reshape((n,) * 4, order="F"),
                           "phi": phi_h, "avector": a_h}
     if not extras:
+        if args.stages:
+            proj.set_option("rhs_overlap", 0)
+            proj.profile(True)
+            for _ in range(3):
+                flush.zero_()
+                step()
+            prof = proj.profile_read()
+            proj.profile(False)
+            res["stage_ms_per_step"] = {k: v[0] / 3 for k, v in prof.items()}
         proj.close()
         return res
 
@@ -419,7 +430,8 @@ def main():
             print(json.dumps({"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
                               "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
                               "higher_is_better": True, "gpu_launches": head["gpu_launches"],
-                              "config": workload_config(w), "note": "profiling run (--no-extras)"}), flush=True)
+                              "config": workload_config(w), "stage_ms_per_step": head.get("stage_ms_per_step"),
+                              "note": "profiling run (--no-extras)"}), flush=True)
         if dist:
             dist.barrier()
             dist.destroy_process_group()
@@ -612,7 +624,8 @@ def batched_form(torch, local, stream, count):
         p.close()
     return {
         "instances": count, "workload": "inputs.batched_instances: odd 21^3-61^3 grids, spacing 0.25-0.4, 1-2 "
-        "nuclei Z=1-3 within +-2 bohr, 2-6 electrons, 4-12 orbitals, <= 4000 determinants, seeded",
+        "nuclei Z=1-3 within +-2 bohr, 2-6 electrons, 4-12 orbitals, full M_s=0 CI (up to 48400 "
+        "determinants), seeded",
         "grid_points_total": int(sum(s["numpoints"] ** 3 for s in inst)),
         "plain_fp64_sequential": {"value": count / (plain_ms / 1e3), "unit": "evals/s", "ms_per_round": plain_ms},
         "batched_fp64_graph": {"value": count / (batched_plain_ms / 1e3), "unit": "evals/s",

@@ -193,10 +193,9 @@ int sincgpu_mean_field_dev(sincgpu_ctx* ctx, const double* phi, const double* re
  * in the FP64 form and 8*(N*N*P + N*P*P) with the context option coulomb_fp32
  * (P = sincgpu_fft_length); larger grids are rejected with SINCGPU_ERANGE.
  * The FP32 form also needs the context's FP32 twiddle and kernel-spectrum
- * tables, which this entry does not allocate: after setting coulomb_fp32, make
- * one allocating Coulomb call (e.g. sincgpu_op_tinv) first, else this entry
- * returns SINCGPU_ESTATE.  All calls share the array: calls that overlap on the
- * GPU race.  The first call on a device looks up the array's address; make it
+ * tables: sincgpu_set_option("coulomb_fp32", 1) allocates them when the option
+ * is set, so this entry itself never does.  All calls share the array: calls
+ * that overlap on the GPU race.  The first call on a device looks up the array's address; make it
  * before any stream capture. */
 int sincgpu_op_tinv_noalloc_dev(sincgpu_ctx* ctx, const double* twoeden03, double* twoereduced,
                                 int allsize);

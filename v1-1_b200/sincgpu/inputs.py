@@ -126,17 +126,18 @@ def _system(rng, nmin, nmax, emin, emax, omin, omax, max_configs):
     ne = int(rng.integers(emin, emax + 1))
     lo = max(omin, (ne + 1) // 2 + 1)
     n = int(rng.integers(lo, omax + 1))
-    while n > lo and ci_size(ne, n) > max_configs:
+    while n > lo and max_configs and ci_size(ne, n) > max_configs:
         n -= 1
     return dict(numpoints=N, spacing=spacing, centershift=tuple(cs), nuccharges=tuple(z), nspf=n, numelec=ne,
                 restrictms=ne % 2)
 
 
-def batched_instances(count: int = 64, seed: int = 2024, max_configs: int = 4000):
+def batched_instances(count: int = 64, seed: int = 2024, max_configs: int | None = None):
     """Instances of the batched form: 21^3-61^3 grids (odd point counts),
     spacing 0.25-0.4, 1-2 nuclei of charge 1-3 within +-2 bohr (snapped), 2-6
-    electrons, 4-12 orbitals, lowest 2Ms; the orbital count is lowered until the
-    full CI has at most `max_configs` determinants (keeps walk-table builds short)."""
+    electrons, 4-12 orbitals, full CI with the lowest 2Ms (up to C(12,3)^2 =
+    48400 determinants); with `max_configs` the orbital count is lowered until
+    the full CI has at most that many determinants."""
     rng = np.random.default_rng(seed)
     return [_system(rng, 21, 61, 2, 6, 4, 12, max_configs) for _ in range(count)]
 
