@@ -54,6 +54,10 @@ def parse():
     ap.add_argument("--profile-precision-form", action="store_true",
                     help="with --no-extras: time the precision form (FP32 Coulomb passes, 3xTF32 "
                          "tensor-core reducedpot) instead of the FP64 form")
+    ap.add_argument("--precision-trajectory", type=int, default=0, metavar="STEPS",
+                    help="instead of the benchmark: STEPS field-free CMF steps of the workload in the FP64 form, "
+                         "the precision form and the precision form with FP64 final mean fields; per-quantity "
+                         "errors against the FP64 form")
     ap.add_argument("--stages", action="store_true",
                     help="with --no-extras: also time each stage on one stream (per-stage CUDA events)")
     ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
@@ -416,6 +420,11 @@ def main():
     from sincgpu.inputs import WORKLOADS
 
     torch.cuda.set_device(local)
+    if args.precision_trajectory:
+        if rank == 0:
+            print(json.dumps(precision_trajectory(WORKLOADS[args.config], args.precision_trajectory, local)),
+                  flush=True)
+        return 0
     dist = None
     if world > 1:
         import datetime
@@ -521,6 +530,87 @@ def precision_form(proj, torch, stream, flush, step, out, mat, steps, world, dis
         proj.set_option("coulomb_fp32", 0)
         proj.set_option("contract_tf32", 0)
     return res
+
+
+def precision_trajectory(w, nsteps, local, dt=0.05):
+    """The precision form along a trajectory: `nsteps` field-free CMF steps of
+    workload `w` from the seeded state, run three ways -- FP64 (the plain form,
+    pinned to the oracle), mixed (FP32 Coulomb passes, 3xTF32 reducedpot) and
+    mixed with the last mean-field build of each step in FP64 (cmf_fp64_last) --
+    with the energy and z dipole of every step; then one orbital-RHS evaluation
+    of the FP64 run's final state in each precision.  Errors are against the
+    FP64 run."""
+    import torch
+    from sincgpu import SincProject, WalkTables
+    from sincgpu.inputs import seeded_avector, seeded_orbitals
+    n, G = w.nspf, w.G
+    dev = torch.device("cuda", local)
+    phi_h = seeded_orbitals(w.numpoints, w.spacing, n, seed=1)
+    variants = {"fp64": {}, "mixed": {"coulomb_fp32": 1, "contract_tf32": 1},
+                "mixed_fp64_last": {"coulomb_fp32": 1, "contract_tf32": 1, "cmf_fp64_last": 1}}
+    runs, final = {}, None
+    for name, opts in variants.items():
+        with SincProject(w.numpoints, w.spacing, w.centershift, w.nuccharges, n, device=local) as p:
+            wt = WalkTables(w.numelec, n, 0).build_spin()
+            p.ci_attach(wt)
+            for k, v in opts.items():
+                p.set_option(k, v)
+            p.cmf_setup(par_timestep=dt)
+            p.cmf_pulses([])
+            a_h = seeded_avector(wt.numconfig, seed=2)
+            e0 = p.cmf_init_dev(torch.from_numpy(np.ascontiguousarray(phi_h.T)).to(dev), torch.from_numpy(a_h).to(dev))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            en, dip = [e0], []
+            for k in range(nsteps):
+                en.append(p.cmf_step(dt * k, dt * (k + 1))["energy"])
+                d, nn = p.cmf_dipole_z()
+                dip.append(d.real / nn)
+            wall = time.perf_counter() - t0
+            runs[name] = {"energy": np.array(en), "dipole": np.array(dip), "ms_per_step": 1e3 * wall / nsteps}
+            if name == "fp64":
+                ph = torch.empty((n, G), dtype=torch.complex128, device=dev)
+                av = torch.empty(wt.numconfig, dtype=torch.complex128, device=dev)
+                p.cmf_state_dev(ph, av)
+                final = (ph, av)
+    # one evaluation of the FP64 run's final state in each precision
+    evals = {}
+    with SincProject(w.numpoints, w.spacing, w.centershift, w.nuccharges, n, device=local) as p:
+        wt = WalkTables(w.numelec, n, 0)
+        p.ci_attach(wt)
+        cx = dict(dtype=torch.complex128, device=dev)
+        bufs = [torch.empty((n, n), **cx), torch.empty((n, n), **cx), torch.empty((n,) * 4, **cx),
+                torch.empty((n,) * 4, **cx), torch.empty((n, n, G), **cx), torch.empty((n, G), **cx)]
+        for name, opts in (("fp64", {}), ("mixed", {"coulomb_fp32": 1, "contract_tf32": 1})):
+            for k in ("coulomb_fp32", "contract_tf32"):
+                p.set_option(k, opts.get(k, 0))
+            p.orbital_rhs_avec_dev(final[0], final[1], *bufs)
+            torch.cuda.synchronize()
+            evals[name] = {"twoematel": bufs[3].clone(), "reducedpot": bufs[4].clone(), "rhs": bufs[5].clone()}
+    ref, mix = evals["fp64"], evals["mixed"]
+    rp_err = ((mix["reducedpot"] - ref["reducedpot"]).abs().amax(dim=2) /
+              ref["reducedpot"].abs().amax(dim=2).clamp_min(1e-300)).cpu().numpy()
+    rhs_err = ((mix["rhs"] - ref["rhs"]).abs().amax(dim=1) / ref["rhs"].abs().amax(dim=1)).cpu().numpy()
+    twoe = float((mix["twoematel"] - ref["twoematel"]).abs().max() / ref["twoematel"].abs().max())
+    e_ref, d_ref = runs["fp64"]["energy"], runs["fp64"]["dipole"]
+    out = {"workload": workload_config(w, l2="n/a")["workload"], "steps": nsteps, "dt_au": dt,
+           "timing": "host wall clock over the steps (each CMF step ends in a device synchronisation)",
+           "fp64_ms_per_step": runs["fp64"]["ms_per_step"], "fp64_energy_first_last": [e_ref[0], e_ref[-1]]}
+    for name in ("mixed", "mixed_fp64_last"):
+        r = runs[name]
+        out[name] = {"ms_per_step": r["ms_per_step"],
+                     "speedup_vs_fp64": runs["fp64"]["ms_per_step"] / r["ms_per_step"],
+                     "energy_dev_max_hartree": float(np.abs(r["energy"] - e_ref).max()),
+                     "energy_dev_last_hartree": float(abs(r["energy"][-1] - e_ref[-1])),
+                     "dipole_z_dev_max_au": float(np.abs(r["dipole"] - d_ref).max()),
+                     "energy_dev_at_steps": {str(k): float(abs(r["energy"][k] - e_ref[k]))
+                                             for k in (1, 10, 50, 100, 200) if k <= nsteps}}
+    out["evaluation_at_final_state"] = {
+        "reduced_potentials_rel_err": {"max": float(rp_err.max()), "median": float(np.median(rp_err)),
+                                       "count": int(rp_err.size),
+                                       "per_potential": "reducedpot(:, k, i): max |mixed - fp64| / max |fp64|"},
+        "rhs_rel_err_per_orbital_max": float(rhs_err.max()), "twoematel_rel_err": twoe}
+    return out
 
 
 def cmf_rate(proj, w, phi, avec, torch, local, nsteps=6):

@@ -85,7 +85,14 @@ int sincgpu_fft_length(sincgpu_ctx* ctx);
  * A-vector orbital-RHS entry runs the RDMs, the density-matrix inverse and the
  * kinetic contraction on a second stream of the context beside the Coulomb
  * passes, then twoematel there beside reducedpot and the apply, joined by
- * events; 0: one stream; bitwise the same). */
+ * events; 0: one stream; bitwise the same); "coul_fused" (1: the Coulomb
+ * solve as three passes, the y, z and inverse-y transforms of each (pair, kx)
+ * plane in one kernel with the plane in shared memory, split over a
+ * thread-block cluster where it does not fit one CTA; 0: five passes through
+ * HBM; results agree to rounding); "cmf_fp64_last" (1: in the precision form,
+ * the last mean-field build of each CMF step and its post-prop reducedpot run
+ * in FP64, so that the energy, the dipole and the next step start from FP64
+ * matrices). */
 int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
 
 /* C(M x N, row-major) = A(M x K, row-major) * B(N x K, row-major)^T on the

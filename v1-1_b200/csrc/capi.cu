@@ -375,6 +375,11 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
     h->c.coul_tma = (int)value;
     return SINCGPU_OK;
   }
+  if (!strcmp(name, "cmf_fp64_last")) {
+    SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "cmf_fp64_last must be 0 or 1");
+    h->c.cmf.fp64_last = value != 0;
+    return SINCGPU_OK;
+  }
   if (!strcmp(name, "contract_tf32")) {
     SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "contract_tf32 must be 0 or 1");
     h->c.contract_tf32 = (int)value;

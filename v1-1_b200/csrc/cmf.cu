@@ -299,6 +299,26 @@ int cmf_init(Ctx& c, const double2* phi, const double2* avec, double* e0) {
   return SINCGPU_OK;
 }
 
+// FP64 Coulomb passes and contractions while alive (the precision form's
+// correction pass), the context's precision options restored after
+struct Fp64Scope {
+  Ctx& c;
+  const int coul, tf32;
+  bool on;
+  Fp64Scope(Ctx& cc, bool enable) : c(cc), coul(cc.coul_fp32), tf32(cc.contract_tf32), on(enable) {
+    if (on) {
+      c.coul_fp32 = 0;
+      c.contract_tf32 = 0;
+    }
+  }
+  ~Fp64Scope() {
+    if (on) {
+      c.coul_fp32 = coul;
+      c.contract_tf32 = tf32;
+    }
+  }
+};
+
 int cmf_step(Ctx& c, double tin, double tout) {
   CmfState& m = c.cmf;
   CIState& s = c.ci;
@@ -327,12 +347,14 @@ int cmf_step(Ctx& c, double tin, double tout) {
   for (int ii = 0; ii < m.p.step_flag; ++ii) {
     SG_TRY(propspfs(c, 1, tin, tout));
     SG_TRY(cmf_prop_avector(c, 1, tin, tout));
+    Fp64Scope fp64(c, m.fp64_last && ii == m.p.step_flag - 1);
     SG_TRY(get_allden(c));
     SG_TRY(all_matel(c));
     SG_TRY(get_reducedpot(c));
   }
   // post-prop (postpropflag=2)
   SG_TRY(cmf_prop_avector(c, 1, tin, tout));
+  Fp64Scope fp64(c, m.fp64_last);
   SG_TRY(get_allden(c));
   SG_TRY(get_reducedpot(c));
   // prop_loop: spin projection, energy

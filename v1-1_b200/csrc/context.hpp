@@ -118,6 +118,9 @@ struct CmfState {
   AvecPropState a;
   double first = 0.0, last = 0.0, energy = 0.0, norm = 0.0, nucdipz = 0.0;
   int orb_iters = 0, avec_iters = 0;
+  // precision form: the last mean-field build of each step (whose matrices give the
+  // energy and dipole and start the next step) and the post-prop reducedpot in FP64
+  bool fp64_last = false;
   std::vector<int> pa, pb;  // pair list of the resident planar reduced potentials
   bool herm = true;
   Workspace ws;
