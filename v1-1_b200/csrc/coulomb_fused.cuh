@@ -166,35 +166,31 @@ __global__ void __launch_bounds__(yzy_bound(P1, P2, CL), yzy_min_blocks<C>(P1, P
     __syncthreads();
   }
 
-  // ---- phase 2: the CTA's columns along z: forward, * kernel spectrum, inverse.
-  // Threads are mapped lines-fastest here (consecutive lanes on consecutive
-  // columns at one position in the line), so that the plane, the exchange and
-  // the kernel spectrum are read at consecutive addresses
+  // ---- phase 2: the CTA's columns along z: forward, * kernel spectrum, inverse
   constexpr int PCmax = (P + CL - 1) / CL;
   const int k0 = r * PCmax, kend = min(P, k0 + PCmax);
-  const int lc = tid % NR, sc = tid / NR;
   const R* kh = khT + (long long)kx * P * P;  // [kz][ky] at this kx
   for (int kb = k0; kb < kend; kb += NR) {
-    const int ky = kb + lc;
+    const int ky = kb + l;
     const bool colok = ky < kend;
 #pragma unroll
     for (int n1 = 0; n1 < P1; ++n1) {
-      const int zz = sc + P2 * n1;
-      a[n1] = (colok && sc < P2 && zz < N) ? *at(zz, ky) : zero;
+      const int zz = s + P2 * n1;
+      a[n1] = (colok && s < P2 && zz < N) ? *at(zz, ky) : zero;
     }
-    dft_in_to_out<P1, P2, false, C, false, true>(a, b, sc, lc, NR, zex, roots);
-    if (colok && sc < P1) {
+    dft_in_to_out<P1, P2, false, C, false, true>(a, b, s, l, NR, zex, roots);
+    if (colok && s < P1) {
 #pragma unroll
       for (int k2 = 0; k2 < P2; ++k2) {
-        const R w = kh[(long long)(sc + P1 * k2) * P + ky];
+        const R w = kh[(long long)(s + P1 * k2) * P + ky];
         b[k2] = CplxTraits<C>::make(b[k2].x * w, b[k2].y * w);
       }
     }
-    dft_out_to_in<P1, P2, true, C, false, true>(b, a, sc, lc, NR, zex, roots);
-    if (colok && sc < P2) {
+    dft_out_to_in<P1, P2, true, C, false, true>(b, a, s, l, NR, zex, roots);
+    if (colok && s < P2) {
 #pragma unroll
       for (int m1 = 0; m1 < P1; ++m1) {
-        const int zz = sc + P2 * m1;
+        const int zz = s + P2 * m1;
         if (zz < N) *at(zz, ky) = a[m1];
       }
     }
