@@ -121,7 +121,11 @@ void sincgpu_server::run(Req& r, Res& out) {
   };
   int rc = sincgpu_create(&ctx, r.N, r.spacing, (int)r.z.size(), r.cs.data(), r.z.data(), r.nspf, 240, 40, 0,
                           device);
-  if (rc == SINCGPU_OK) rc = sincgpu_walks_create(&walks, r.numelec, r.nspf, r.restrictms, 0);
+  // the walk-table build of one request uses its share of the host cores, so that
+  // the other requests' host loops (one synchronisation per Arnoldi step) are not
+  // starved while it runs
+  const int host_threads = std::max(1, (int)std::thread::hardware_concurrency() / std::max(1, max_active));
+  if (rc == SINCGPU_OK) rc = sincgpu_walks_create(&walks, r.numelec, r.nspf, r.restrictms, host_threads);
   if (rc == SINCGPU_OK) rc = sincgpu_walks_spin(walks, r.spinrestrictval);
   if (rc == SINCGPU_OK) rc = sincgpu_ci_attach(ctx, walks);
   const long long G = (long long)r.N * r.N * r.N;
