@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--batched-count", type=int, default=64)
     ap.add_argument("--served-count", type=int, default=24)
     ap.add_argument("--served-steps", type=int, default=10)
+    ap.add_argument("--served-full", action="store_true",
+                    help="served stream at the stated sizes (31^3-81^3 grids, 2-6 electrons, 4-16 orbitals); "
+                         "use with --served-steps 200")
     return ap.parse_args()
 
 
@@ -463,7 +466,8 @@ def main():
     if not args.no_batched:
         line["batched"] = batched_form(torch, local, torch.cuda.current_stream(), args.batched_count)
     if not args.no_served:
-        line["served"] = {f: served_form(local, f == "mixed_fp32_coulomb", args.served_count, args.served_steps)
+        line["served"] = {f: served_form(local, f == "mixed_fp32_coulomb", args.served_count, args.served_steps,
+                                         args.served_full)
                           for f in ("plain_fp64", "mixed_fp32_coulomb")}
         pl, mx = line["served"]["plain_fp64"], line["served"]["mixed_fp32_coulomb"]
         line["served"]["mixed_vs_plain_steps_per_s"] = mx["steps_per_s"] / max(pl["steps_per_s"], 1e-30)
@@ -732,14 +736,19 @@ def batched_form(torch, local, stream, count):
     }
 
 
-def served_form(local, fp32, count, nsteps):
+SERVED_FULL = dict(nmin=31, nmax=81, omax=16, emax=6, max_configs=20000)
+
+
+def served_form(local, fp32, count, nsteps, full=False):
     """Served form: requests (inputs.served_requests) submitted at their Poisson
     arrival offsets to the device-resident request loop; per-step latency
-    percentiles and steps/s over the run."""
+    percentiles and steps/s over the run.  `full`: the stated stream's sizes
+    (31^3-81^3 grids, 2-6 electrons, 4-16 orbitals, full CI up to 20000
+    determinants) instead of the bounded default (21^3-41^3, 2-4, 4-8, 1000)."""
     from types import SimpleNamespace
     from sincgpu.inputs import ci_size, seeded_orbitals, served_requests
     from sincgpu.serve import Server
-    reqs = served_requests(count)
+    reqs = served_requests(count, **(SERVED_FULL if full else {}))
     states = []
     for i, r in enumerate(reqs):
         phi = seeded_orbitals(r["numpoints"], r["spacing"], r["nspf"], seed=300 + i)
@@ -772,8 +781,11 @@ def served_form(local, fp32, count, nsteps):
             "queue_wait_ms_p50": float(np.median(queued)),
             "peak_concurrent": st["peak_active"], "completed": st["completed"], "wall_s": wall,
             "mean_request_s": float(np.mean([len(r["step_ms"]) and r["step_ms"].sum() / 1e3 for r in res])),
-            "workload": "inputs.served_requests: odd 21^3-41^3 grids, 2-4 electrons, 4-8 orbitals, <= 1000 "
-                        "determinants, one sin^2 pulse each (type 2), seeded; the request loop uses 8 worker slots"}
+            "workload": ("inputs.served_requests: odd 31^3-81^3 grids, 2-6 electrons, 4-16 orbitals, <= 20000 "
+                         "determinants" if full else "inputs.served_requests: odd 21^3-41^3 grids, 2-4 electrons, "
+                         "4-8 orbitals, <= 1000 determinants") + ", one sin^2 pulse each (type 2), seeded; the "
+                        "request loop uses 8 worker slots",
+            "requests_detail": [[r["numpoints"], r["nspf"], r["numelec"]] for r in reqs]}
 
 
 def secondary_rates(proj, torch, stream, flush, phi, den, inv, red, out, mat, avec, n, G):

@@ -143,16 +143,19 @@ def batched_instances(count: int = 64, seed: int = 2024, max_configs: int | None
 
 
 def served_requests(count: int = 24, seed: int = 4048, nmax: int = 41, omax: int = 8, emax: int = 4,
-                    max_configs: int = 1000, rate: float = 20.0):
+                    max_configs: int = 1000, rate: float = 20.0, nmin: int = 21):
     """Requests of the served form with Poisson arrival offsets (mean `rate`
     per second) and one linearly polarised sin^2 pulse each (peak field
     0.005-0.17 au, carrier 0.05-1.0 au, envelope 400-1600 au; pulse type 2 with
-    omega = pi / duration and strength = peak / carrier)."""
+    omega = pi / duration and strength = peak / carrier).  Grids of
+    nmin^3-nmax^3 points (odd counts), 2-emax electrons, 4-omax orbitals, the
+    orbital count lowered until the full CI has at most `max_configs`
+    determinants."""
     rng = np.random.default_rng(seed)
     out, t = [], 0.0
     for _ in range(count):
         t += float(rng.exponential(1.0 / rate))
-        s = _system(rng, 21, nmax, 2, emax, 4, omax, max_configs)
+        s = _system(rng, nmin, nmax, 2, emax, 4, omax, max_configs)
         peak = float(rng.uniform(0.005, 0.17))
         w2 = float(rng.uniform(0.05, 1.0))
         dur = float(rng.uniform(400.0, 1600.0))
