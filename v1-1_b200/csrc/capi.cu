@@ -94,7 +94,7 @@ Ctx::~Ctx() {
   if (stream) cudaStreamSynchronize(stream);
   if (rhs_graph) cudaDeviceSynchronize();
   for (void* p : {(void*)d_kevect, (void*)d_ketile, (void*)d_pot, (void*)d_zdip, (void*)d_tcoul, (void*)d_khat,
-                  (void*)d_roots, (void*)d_khat32, (void*)d_roots32, (void*)d_khT, (void*)d_khT32})
+                  (void*)d_roots, (void*)d_khat32, (void*)d_roots32, (void*)d_khT, (void*)d_khT32, (void*)d_khr, (void*)d_khr32})
     dfree(*this, p);
   ws_fft.release();
   ws_pairs.release();

@@ -160,6 +160,10 @@ struct Ctx {
   float2* d_khat32 = nullptr;   // FP32 copies for the precision form, made on demand
   float2* d_roots32 = nullptr;
   double* d_khT = nullptr;      // real part of d_khat as [kx][kz][ky], three-pass Coulomb form (on demand)
+  // real part of d_khat on the octant k <= P/2 of each axis, (P/2+1)^3 values: the
+  // kernel is real and even in each axis, so its spectrum is too (khat(P-k) = khat(k))
+  double* d_khr = nullptr;
+  float* d_khr32 = nullptr;
   float* d_khT32 = nullptr;
 
   // ---- scratch --------------------------------------------------------------

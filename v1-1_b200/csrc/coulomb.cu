@@ -74,6 +74,12 @@ template <>
 const float2* khat_of<float2>(const Ctx& c) { return c.d_khat32; }
 
 template <class C>
+static const typename CplxTraits<C>::Real* khr_of(const Ctx& c);
+template <>
+const double* khr_of<double2>(const Ctx& c) { return c.d_khr; }
+template <>
+const float* khr_of<float2>(const Ctx& c) { return c.d_khr32; }
+template <class C>
 static const typename CplxTraits<C>::Real* khT_of(const Ctx& c);
 template <>
 const double* khT_of<double2>(const Ctx& c) { return c.d_khT; }
@@ -147,6 +153,7 @@ static int coul_run_t(Ctx& c, const double2* src1, const double2* src2, const in
   ca.G = c.G;
   ca.roots = roots_of<C>(c);
   ca.khat = khat_of<C>(c);
+  ca.khr = khr_of<C>(c);
   ca.W1 = (C*)c.ws_fft.ptr;
   ca.W2 = fused ? nullptr : ca.W1 + (long long)chunk * N * N * P;
   ca.npair_total = npair;
@@ -216,6 +223,7 @@ static int coulomb_dens_scratch_t(Ctx& c, const double2* dens, int m, double2* r
   ca.G = c.G;
   ca.roots = roots_of<C>(c);
   ca.khat = khat_of<C>(c);
+  ca.khr = khr_of<C>(c);
   ca.W1 = (C*)scratch;
   ca.W2 = ca.W1 + (size_t)chunk * N * N * P;
   ca.npair_total = m;
@@ -231,7 +239,7 @@ static int coulomb_dens_scratch_t(Ctx& c, const double2* dens, int m, double2* r
 int coulomb_dens_scratch(Ctx& c, const double2* dens, int m, double2* red, double2* scratch,
                          size_t scratch_bytes) {
   if (c.coul_fp32) {
-    SG_CHECK(c.d_khat32 && c.d_roots32, SINCGPU_ESTATE, "FP32 Coulomb tables are missing");
+    SG_CHECK(c.d_khat32 && c.d_roots32 && c.d_khr32, SINCGPU_ESTATE, "FP32 Coulomb tables are missing");
     return coulomb_dens_scratch_t<float2>(c, dens, m, red, scratch, scratch_bytes);
   }
   return coulomb_dens_scratch_t<double2>(c, dens, m, red, scratch, scratch_bytes);

@@ -476,6 +476,21 @@ __global__ void fft_full_axis_kernel(double2* __restrict__ data, FftPlan plan,
   }
 }
 
+// khr[(fz H + fy) H + fx] = Re khat[(fz P + fy) P + fx] for f <= P/2, H = P/2 + 1
+__global__ void khat_octant_kernel(double* __restrict__ out, const double2* __restrict__ in, int P) {
+  const int H = P / 2 + 1;
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)H * H * H) return;
+  const int fx = (int)(i % H), fy = (int)((i / H) % H), fz = (int)(i / ((long long)H * H));
+  out[i] = in[((long long)fz * P + fy) * P + fx].x;
+}
+
+__global__ void narrow_real_kernel(float* __restrict__ out, const double* __restrict__ in, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
 int make_khat(Ctx& c) {
   const int P = c.P;
   const long long P3 = (long long)P * P * P;
@@ -484,6 +499,10 @@ int make_khat(Ctx& c) {
   dfree(c, c.d_roots32);
   dfree(c, c.d_khT);
   dfree(c, c.d_khT32);
+  dfree(c, c.d_khr);
+  dfree(c, c.d_khr32);
+  c.d_khr = nullptr;
+  c.d_khr32 = nullptr;
   c.d_khat = nullptr;
   c.d_khat32 = nullptr;
   c.d_roots32 = nullptr;
@@ -509,6 +528,11 @@ int make_khat(Ctx& c) {
   const double inv = 1.0 / ((double)P * (double)P * (double)P);
   fft_full_axis_kernel<<<g1, 128, sm1, c.stream>>>(c.d_khat, c.plan, c.d_roots, 2, c.tx, inv);
   SG_LAUNCHED();
+  const int H = P / 2 + 1;
+  const long long H3 = (long long)H * H * H;
+  SG_TRY(dalloc(c, &c.d_khr, sizeof(double) * H3));
+  khat_octant_kernel<<<ceil_div(H3, 256), 256, 0, c.stream>>>(c.d_khr, c.d_khat, P);
+  SG_LAUNCHED();
   SG_CUDA(cudaStreamSynchronize(c.stream));
   return SINCGPU_OK;
 }
@@ -520,8 +544,15 @@ __global__ void narrow_kernel(float2* __restrict__ out, const double2* __restric
 }
 
 int ensure_fp32_tables(Ctx& c) {
-  if (c.d_khat32 && c.d_roots32) return SINCGPU_OK;  // no stream work once built (graph capture)
+  if (c.d_khat32 && c.d_roots32 && c.d_khr32) return SINCGPU_OK;  // no stream work once built (graph capture)
   const long long P3 = (long long)c.P * c.P * c.P;
+  if (!c.d_khr32) {
+    const long long H = c.P / 2 + 1, H3 = H * H * H;
+    SG_TRY(dalloc(c, &c.d_khr32, sizeof(float) * H3));
+    narrow_real_kernel<<<std::min<long long>(ceil_div(H3, 256), 148 * 16), 256, 0, c.stream>>>(c.d_khr32, c.d_khr,
+                                                                                               H3);
+    SG_LAUNCHED();
+  }
   if (!c.d_khat32) {
     SG_TRY(dalloc(c, &c.d_khat32, sizeof(float2) * P3));
     narrow_kernel<<<std::min<long long>(ceil_div(P3, 256), 148 * 16), 256, 0, c.stream>>>(c.d_khat32,
