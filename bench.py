@@ -58,6 +58,8 @@ def parse():
                     help="instead of the benchmark: STEPS field-free CMF steps of the workload in the FP64 form, "
                          "the precision form and the precision form with FP64 final mean fields; per-quantity "
                          "errors against the FP64 form")
+    ap.add_argument("--only", choices=["served", "batched"], default=None,
+                    help="run only the served or the batched form and print its object")
     ap.add_argument("--stages", action="store_true",
                     help="with --no-extras: also time each stage on one stream (per-stage CUDA events)")
     ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
@@ -423,6 +425,19 @@ def main():
     from sincgpu.inputs import WORKLOADS
 
     torch.cuda.set_device(local)
+    if args.only:
+        out = {}
+        if args.only == "served":
+            out["served"] = {f: served_form(local, f == "mixed_fp32_coulomb", args.served_count, args.served_steps,
+                                            args.served_full)
+                             for f in ("plain_fp64", "mixed_fp32_coulomb")}
+            pl, mx = out["served"]["plain_fp64"], out["served"]["mixed_fp32_coulomb"]
+            out["served"]["mixed_vs_plain_steps_per_s"] = mx["steps_per_s"] / max(pl["steps_per_s"], 1e-30)
+        else:
+            out["batched"] = batched_form(torch, local, torch.cuda.current_stream(), args.batched_count)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return 0
     if args.precision_trajectory:
         if rank == 0:
             print(json.dumps(precision_trajectory(WORKLOADS[args.config], args.precision_trajectory, local)),
