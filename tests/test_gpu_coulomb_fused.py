@@ -85,3 +85,28 @@ def test_orbital_rhs_avec_fused_workload_b(built_lib):
         assert relerr(o3, o5) < 1e-13
     finally:
         gpu.close()
+
+
+def test_paired_z_pass_162(built_lib):
+    """The z pass with 9 threads per length-162 line (coul_z2 = 1: each thread one
+    18-point and two 9-point sub-transforms) against the plain z pass (18 threads
+    per line) and the oracle, FP64 and FP32."""
+    from sincgpu import SincProject
+    N, d = 81, 0.3
+    sysm = orc.SincSystem(N, d, [[0, 0, 0]], [1.0])
+    gpu = SincProject(N, d, [[0, 0, 0]], [1.0], 2)
+    try:
+        rng = np.random.default_rng(162)
+        dens = rng.standard_normal((sysm.G, 2)) + 1j * rng.standard_normal((sysm.G, 2))
+        for fp32 in (0, 1):
+            gpu.set_option("coulomb_fp32", fp32)
+            gpu.set_option("coul_z2", 0)
+            plain = gpu.op_tinv(dens)
+            gpu.set_option("coul_z2", 1)
+            paired = gpu.op_tinv(dens)
+            assert relerr(paired, plain) < 1e-14
+            if not fp32:
+                assert relerr(paired, sysm.op_tinv(dens, workers=8)) < 1e-11
+        gpu.set_option("coul_z2", 0)
+    finally:
+        gpu.close()

@@ -185,6 +185,93 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_z<C>(P1 * P2),
   }
 }
 
+// CZ for lengths P = P1 * P2 with P1 = 2 P2 (162 = 18 x 9): the plain z pass
+// gives each line max(P1, P2) = P1 threads, and half of them idle in the steps
+// with P2 sub-transforms (the loads, the first forward step, the last inverse
+// step, the stores) while the others wait at the exchange barrier.  Here a line
+// has P2 threads: thread s does sub-transform s of length P1 in those steps and
+// the two sub-transforms s and s + P2 of length P2 in the others, so every
+// thread works in every step and a CTA holds twice the lines for the same
+// threads.  Same arithmetic in the same order as coul_z_t.
+template <int P1, int P2>
+__host__ __device__ constexpr int lines_for_z2() { return 32; }
+
+template <int P1, int P2, class C>
+__global__ void __launch_bounds__(P2 * lines_for_z2<P1, P2>(), 2) coul_z2_t(CoulArgs<C> ca) {
+  static_assert(P1 == 2 * P2, "paired z pass needs P1 = 2 P2");
+  constexpr int P = P1 * P2, TL = lines_for_z2<P1, P2>();
+  extern __shared__ __align__(16) unsigned char z2_raw[];
+  C* roots = reinterpret_cast<C*>(z2_raw);
+  C* ex = roots + P;
+  load_roots(roots, ca.roots, P);
+  const int N = ca.N;
+  const int l = threadIdx.x % TL, s = threadIdx.x / TL;  // s < P2
+  const int p = blockIdx.z, f = blockIdx.x * TL + l;    // column f = ky*P + kx
+  const long long zs = (long long)P * P;
+  const bool col = f < zs;
+  C* base = ca.W2 + (long long)p * N * zs + f;
+  const C zero = CplxTraits<C>::make(0.0, 0.0);
+  auto X = [&](int e) -> C& { return ex[e * TL + l]; };
+  C a[P1], b0[P2], b1[P2];
+#pragma unroll
+  for (int n1 = 0; n1 < P1; ++n1) {
+    const int z = s + P2 * n1;
+    a[n1] = (col && z < N) ? base[z * zs] : zero;
+  }
+  __syncthreads();  // twiddles
+  // forward step 1: sub-transform s of length P1
+  RegFFT<P1, 1, false, C>::run(a, ConstRoots<P, C>{}, P);
+#pragma unroll
+  for (int k1 = 0; k1 < P1; ++k1) {
+    C v = a[k1];
+    if (k1 > 0 && s > 0) v = cmul(v, root<false>(roots, s * k1));
+    X(k1 * P2 + s) = v;
+  }
+  __syncthreads();
+  // forward step 2: sub-transforms t = s and t = s + P2 of length P2
+#pragma unroll
+  for (int n2 = 0; n2 < P2; ++n2) {
+    b0[n2] = X(s * P2 + n2);
+    b1[n2] = X((s + P2) * P2 + n2);
+  }
+  RegFFT<P2, 1, false, C>::run(b0, ConstRoots<P, C>{}, P);
+  RegFFT<P2, 1, false, C>::run(b1, ConstRoots<P, C>{}, P);
+  if (col) {
+    const C* kh = ca.khat + f;
+#pragma unroll
+    for (int k2 = 0; k2 < P2; ++k2) {
+      b0[k2] = cmul(b0[k2], kh[(long long)(s + P1 * k2) * zs]);
+      b1[k2] = cmul(b1[k2], kh[(long long)(s + P2 + P1 * k2) * zs]);
+    }
+  }
+  __syncthreads();  // the exchange is read before the inverse writes it
+  // inverse step 1: sub-transforms t = s and t = s + P2 of length P2
+  RegFFT<P2, 1, true, C>::run(b0, ConstRoots<P, C>{}, P);
+  RegFFT<P2, 1, true, C>::run(b1, ConstRoots<P, C>{}, P);
+#pragma unroll
+  for (int m2 = 0; m2 < P2; ++m2) {
+    C v0 = b0[m2], v1 = b1[m2];
+    if (m2 > 0) {
+      if (s > 0) v0 = cmul(v0, root<true>(roots, s * m2));
+      v1 = cmul(v1, root<true>(roots, (s + P2) * m2));
+    }
+    X(m2 * P1 + s) = v0;
+    X(m2 * P1 + s + P2) = v1;
+  }
+  __syncthreads();
+  // inverse step 2: sub-transform s of length P1; z = s + P2 m1
+#pragma unroll
+  for (int k1 = 0; k1 < P1; ++k1) a[k1] = X(s * P1 + k1);
+  RegFFT<P1, 1, true, C>::run(a, ConstRoots<P, C>{}, P);
+  if (col) {
+#pragma unroll
+    for (int m1 = 0; m1 < P1; ++m1) {
+      const int z = s + P2 * m1;
+      if (z < N) base[z * zs] = a[m1];
+    }
+  }
+}
+
 // CZ with TMA-staged slabs: a persistent CTA walks its tiles of TL consecutive
 // (ky, kx) columns; the tile's N z-planes (an N x TL slab of W2) arrive in shared
 // memory by one tiled bulk tensor load, two tiles ahead of the computation (two
@@ -438,6 +525,17 @@ int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2*
       const int ntf = ceil_div(P * P, TLT), ntiles = ntf * np;
       const int grid = std::min(ntiles, nsm * occ);
       coul_z_tma_t<P1, P2, C><<<grid, S * TLT, dyn, c.stream>>>(ca, *zmap, ntf, ntiles, slab_stride, err);
+    } else if constexpr (P1 == 2 * P2) {
+      if (c.coul_z2) {
+        constexpr int TL2 = lines_for_z2<P1, P2>();
+        const size_t dyn = sizeof(C) * ((size_t)P + (size_t)P * TL2);
+        static const cudaError_t attr = cudaFuncSetAttribute(
+            coul_z2_t<P1, P2, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        SG_CUDA(attr);
+        coul_z2_t<P1, P2, C><<<dim3(ceil_div(P * P, TL2), 1, np), P2 * TL2, dyn, c.stream>>>(ca);
+      } else {
+        coul_z_t<P1, P2, C><<<dim3(nzc, 1, np), S * TLZ, 0, c.stream>>>(ca);
+      }
     } else {
       coul_z_t<P1, P2, C><<<dim3(nzc, 1, np), S * TLZ, 0, c.stream>>>(ca);
     }
