@@ -110,27 +110,3 @@ def test_paired_z_pass_162(built_lib):
         gpu.set_option("coul_z2", 0)
     finally:
         gpu.close()
-
-
-@pytest.mark.parametrize("N,d", [(41, 0.25), (81, 0.3)])
-def test_z_pass_spectrum_reads(built_lib, N, d):
-    """The z pass's three reads of the kernel spectrum (option coul_zspec: 0 the
-    complex P^3 table, 1 its real part, 2 the real part on the octant k <= P/2,
-    the spectrum being real and even in each axis) give the same potentials to
-    rounding, FP64 against the oracle."""
-    from sincgpu import SincProject
-    sysm = orc.SincSystem(N, d, [[0, 0, 0]], [1.0])
-    gpu = SincProject(N, d, [[0, 0, 0]], [1.0], 2)
-    try:
-        rng = np.random.default_rng(N)
-        dens = rng.standard_normal((sysm.G, 2)) + 1j * rng.standard_normal((sysm.G, 2))
-        ref = sysm.op_tinv(dens, workers=8)
-        outs = []
-        for zs in (0, 1, 2):
-            gpu.set_option("coul_zspec", zs)
-            outs.append(gpu.op_tinv(dens))
-            assert relerr(outs[-1], ref) < 1e-11
-        assert relerr(outs[1], outs[0]) < 1e-14 and relerr(outs[2], outs[0]) < 1e-14
-        gpu.set_option("coul_zspec", -1)
-    finally:
-        gpu.close()

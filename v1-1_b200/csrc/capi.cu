@@ -94,7 +94,7 @@ Ctx::~Ctx() {
   if (stream) cudaStreamSynchronize(stream);
   if (rhs_graph) cudaDeviceSynchronize();
   for (void* p : {(void*)d_kevect, (void*)d_ketile, (void*)d_pot, (void*)d_zdip, (void*)d_tcoul, (void*)d_khat,
-                  (void*)d_roots, (void*)d_khat32, (void*)d_roots32, (void*)d_khT, (void*)d_khT32, (void*)d_khr, (void*)d_khr32, (void*)d_khre, (void*)d_khre32})
+                  (void*)d_roots, (void*)d_khat32, (void*)d_roots32, (void*)d_khT, (void*)d_khT32, (void*)d_khr, (void*)d_khr32})
     dfree(*this, p);
   ws_fft.release();
   ws_pairs.release();
@@ -363,11 +363,6 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
   if (!strcmp(name, "rp_dmma")) {
     SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "rp_dmma must be 0 or 1");
     h->c.rp_dmma = (int)value;
-    return SINCGPU_OK;
-  }
-  if (!strcmp(name, "coul_zspec")) {
-    SG_CHECK(value >= -1 && value <= 2, SINCGPU_EINVAL, "coul_zspec must be -1, 0, 1 or 2");
-    h->c.coul_zspec = (int)value;
     return SINCGPU_OK;
   }
   if (!strcmp(name, "coul_z2")) {

@@ -164,8 +164,6 @@ struct Ctx {
   // kernel is real and even in each axis, so its spectrum is too (khat(P-k) = khat(k))
   double* d_khr = nullptr;
   float* d_khr32 = nullptr;
-  double* d_khre = nullptr;     // real part of d_khat, P^3 (on demand)
-  float* d_khre32 = nullptr;
   float* d_khT32 = nullptr;
 
   // ---- scratch --------------------------------------------------------------
@@ -192,7 +190,6 @@ struct Ctx {
   int coul_fp32 = 0;    // 1: Coulomb passes in FP32 (precision form), 0: FP64
   int contract_tf32 = 0;  // 1: reducedpot contraction as 3xTF32 on the tensor cores
   int coul_tma = -1;      // TMA-staged persistent z pass: 1 on, 0 off, -1 automatic (off)
-  int coul_zspec = -1;    // spectrum read of the z pass: 0 complex, 1 real P^3, 2 real octant, -1 automatic
   int coul_z2 = 0;        // z pass with P2 threads per line where P1 = 2 P2 (coul_z2_t): 1 on, 0 off
   int coul_fused = 0;     // three-pass Coulomb form (y, z, inverse y per plane on chip): 1 on where it fits, 0 off, -1 automatic
   int rp_dmma = 1;        // 1: FP64 reducedpot GEMM on the FP64 tensor cores (DMMA), 0: DFMA tiles
@@ -268,8 +265,6 @@ int make_khat(Ctx& c);
 int ensure_fp32_tables(Ctx& c);
 // real kernel spectrum transposed to [kx][kz][ky] (FP64, and FP32 with fp32)
 int ensure_khT(Ctx& c, bool fp32);
-// real part of the kernel spectrum on the full grid, [kz][ky][kx] (FP64, or FP32 with fp32)
-int ensure_khre(Ctx& c, bool fp32);
 
 // coulomb.cu: R_p = T * (phi1_a conj(phi2_b)) for pairs p=(a_p,b_p).
 // Rpl (device) receives the planar real/imag parts: Rpl[p*G+x] = Re, Rpl[(npair+p)*G+x] = Im.

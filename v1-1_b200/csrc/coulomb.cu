@@ -74,12 +74,6 @@ template <>
 const float2* khat_of<float2>(const Ctx& c) { return c.d_khat32; }
 
 template <class C>
-static const typename CplxTraits<C>::Real* khre_of(const Ctx& c);
-template <>
-const double* khre_of<double2>(const Ctx& c) { return c.d_khre; }
-template <>
-const float* khre_of<float2>(const Ctx& c) { return c.d_khre32; }
-template <class C>
 static const typename CplxTraits<C>::Real* khr_of(const Ctx& c);
 template <>
 const double* khr_of<double2>(const Ctx& c) { return c.d_khr; }
@@ -160,13 +154,6 @@ static int coul_run_t(Ctx& c, const double2* src1, const double2* src2, const in
   ca.roots = roots_of<C>(c);
   ca.khat = khat_of<C>(c);
   ca.khr = khr_of<C>(c);
-  // z-pass spectrum: automatic = the octant up to 128 points per line (measured
-  // faster at 81), the complex table beyond (the octant measured slower at 162)
-  ca.zspec = c.coul_zspec >= 0 ? c.coul_zspec : (P <= 128 ? 2 : 0);
-  if (ca.zspec == 1) {
-    SG_TRY(ensure_khre(c, sizeof(C) == 8));
-    ca.khre = khre_of<C>(c);
-  }
   ca.W1 = (C*)c.ws_fft.ptr;
   ca.W2 = fused ? nullptr : ca.W1 + (long long)chunk * N * N * P;
   ca.npair_total = npair;
@@ -237,7 +224,6 @@ static int coulomb_dens_scratch_t(Ctx& c, const double2* dens, int m, double2* r
   ca.roots = roots_of<C>(c);
   ca.khat = khat_of<C>(c);
   ca.khr = khr_of<C>(c);
-  ca.zspec = P <= 128 ? 2 : 0;  // tables built at set-up only (this path allocates nothing)
   ca.W1 = (C*)scratch;
   ca.W2 = ca.W1 + (size_t)chunk * N * N * P;
   ca.npair_total = m;

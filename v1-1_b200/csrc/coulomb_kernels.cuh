@@ -49,8 +49,6 @@ struct CoulArgs {
   int fused;        // 0: five passes (W1, W2); 1, 2, 4, 8: three passes (W1T), plane kernel on clusters of that size
   const typename CplxTraits<C>::Real* khT;  // real kernel spectrum [kx][kz][ky] (three-pass form)
   const typename CplxTraits<C>::Real* khr;  // real kernel spectrum on the octant k <= P/2 ((P/2+1)^3)
-  const typename CplxTraits<C>::Real* khre;  // real kernel spectrum, full P^3 ([kz][ky][kx]), or null
-  int zspec;        // spectrum read of the z pass: 0 complex P^3, 1 real P^3, 2 real octant
 };
 
 template <class C>
@@ -148,10 +146,13 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_z<C>(P1 * P2))
   __syncthreads();
   dft_in_to_out<P1, P2, false, C>(a, b, s, l, TL, ex, roots);
   if (col && s < P1) {
-    using R = typename CplxTraits<C>::Real;
-    if (ca.zspec == 2) {
+    if constexpr (P <= 128) {
       // the spectrum is real and even in each axis: read it on the octant (a table
-      // of (P/2+1)^3 values that stays in L2 while the W2 slab streams through)
+      // of (P/2+1)^3 values that stays in L2 while the W2 slab streams through).
+      // Measured on the 41^3 grid (P = 81): z pass 0.165 -> 0.148 ms; on the 81^3
+      // grid (P = 162) it was slower (4.8 -> 6.7 ms), so longer lines keep the
+      // complex table
+      using R = typename CplxTraits<C>::Real;
       constexpr int H = P / 2 + 1;
       const int ky = f / P, kx = f - ky * P;
       const R* kh = ca.khr + ((ky <= P - ky ? ky : P - ky) * H + (kx <= P - kx ? kx : P - kx));
@@ -159,14 +160,6 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_z<C>(P1 * P2))
       for (int k2 = 0; k2 < P2; ++k2) {
         const int kz = s + P1 * k2;
         const R w = kh[(kz <= P - kz ? kz : P - kz) * H * H];
-        b[k2] = CplxTraits<C>::make(b[k2].x * w, b[k2].y * w);
-      }
-    } else if (ca.zspec == 1) {
-      // the real part on the full grid: half the bytes of the complex table
-      const R* kh = ca.khre + f;
-#pragma unroll
-      for (int k2 = 0; k2 < P2; ++k2) {
-        const R w = kh[(long long)(s + P1 * k2) * zs];
         b[k2] = CplxTraits<C>::make(b[k2].x * w, b[k2].y * w);
       }
     } else {

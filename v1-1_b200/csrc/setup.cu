@@ -501,12 +501,8 @@ int make_khat(Ctx& c) {
   dfree(c, c.d_khT32);
   dfree(c, c.d_khr);
   dfree(c, c.d_khr32);
-  dfree(c, c.d_khre);
-  dfree(c, c.d_khre32);
   c.d_khr = nullptr;
   c.d_khr32 = nullptr;
-  c.d_khre = nullptr;
-  c.d_khre32 = nullptr;
   c.d_khat = nullptr;
   c.d_khat32 = nullptr;
   c.d_roots32 = nullptr;
@@ -597,30 +593,6 @@ int ensure_khT(Ctx& c, bool fp32) {
     khat_transpose_kernel<double><<<grid, 256, 0, c.stream>>>(c.d_khT, c.d_khat, c.P);
   }
   SG_LAUNCHED();
-  SG_CUDA(cudaStreamSynchronize(c.stream));
-  return SINCGPU_OK;
-}
-
-__global__ void real_part_kernel(double* __restrict__ out, const double2* __restrict__ in, long long n) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    out[i] = in[i].x;
-}
-
-int ensure_khre(Ctx& c, bool fp32) {
-  if (fp32 ? c.d_khre32 != nullptr : c.d_khre != nullptr) return SINCGPU_OK;  // no stream work once built
-  const long long P3 = (long long)c.P * c.P * c.P;
-  const int grid = (int)std::min<long long>(ceil_div(P3, 256), 148 * 16);
-  if (!c.d_khre) {
-    SG_TRY(dalloc(c, &c.d_khre, sizeof(double) * P3));
-    real_part_kernel<<<grid, 256, 0, c.stream>>>(c.d_khre, c.d_khat, P3);
-    SG_LAUNCHED();
-  }
-  if (fp32) {
-    SG_TRY(dalloc(c, &c.d_khre32, sizeof(float) * P3));
-    narrow_real_kernel<<<grid, 256, 0, c.stream>>>(c.d_khre32, c.d_khre, P3);
-    SG_LAUNCHED();
-  }
   SG_CUDA(cudaStreamSynchronize(c.stream));
   return SINCGPU_OK;
 }
