@@ -133,10 +133,7 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_z<C>(P1 * P2))
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int l = threadIdx.x % TL, s = threadIdx.x / TL;
-  // pairs run fastest over the grid: the CTAs of one column block for all the
-  // chunk's pairs are resident together, so that block's slice of the kernel
-  // spectrum is read from DRAM once per launch instead of once per pair
-  const int p = blockIdx.x, f = blockIdx.y * TL + l;  // column f = ky*P + kx
+  const int p = blockIdx.z, f = blockIdx.x * TL + l;  // column f = ky*P + kx
   const long long zs = (long long)P * P;
   const bool col = f < zs;
   C* base = ca.W2 + (long long)p * N * zs + f;
@@ -530,10 +527,10 @@ int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2*
         SG_CUDA(attr);
         coul_z2_t<P1, P2, C><<<dim3(ceil_div(P * P, TL2), 1, np), P2 * TL2, dyn, c.stream>>>(ca);
       } else {
-        coul_z_t<P1, P2, C><<<dim3(np, nzc), S * TLZ, 0, c.stream>>>(ca);
+        coul_z_t<P1, P2, C><<<dim3(nzc, 1, np), S * TLZ, 0, c.stream>>>(ca);
       }
     } else {
-      coul_z_t<P1, P2, C><<<dim3(np, nzc), S * TLZ, 0, c.stream>>>(ca);
+      coul_z_t<P1, P2, C><<<dim3(nzc, 1, np), S * TLZ, 0, c.stream>>>(ca);
     }
     SG_LAUNCHED();
   }
