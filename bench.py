@@ -718,9 +718,11 @@ def batched_form(torch, local, stream, count):
         p.set_option("contract_tf32", 1)
         key = (p.N, p.nspf)
         if key in tuned:
-            p.set_option("coul_chunk", tuned[key])
+            for name, v in tuned[key].items():
+                p.set_option(name, v)
         else:
-            tuned[key], _ = p.autotune_rhs(*args_of(b))
+            p.autotune_rhs(*args_of(b))
+            tuned[key] = {name: p.get_option(name) for name in ("coul_chunk", "twoe_tile", "coul_tma")}
         p.rhs_graph_capture(*args_of(b))
     tune_s = time.perf_counter() - t_tune
     batch = Batch([m[0] for m in made])
@@ -745,7 +747,8 @@ def batched_form(torch, local, stream, count):
                                 "rhs_rel_err_max_vs_fp64": rhs_err,
                                 "two_electron_energy_dev_max_hartree": de},
         "mixed_batched_vs_plain_sequential": plain_ms / mixed_ms,
-        "setup_s": setup_s, "autotune_s": tune_s, "autotuned_chunks": len(tuned),
+        "setup_s": setup_s, "autotune_s": tune_s, "autotuned_shapes": len(tuned),
+        "autotuned": {f"{k[0]}^3/{k[1]}": v for k, v in sorted(tuned.items())},
         "timing": "CUDA events on the launching stream, 3 rounds after one warm-up round; each round touches "
                   "several GB (inputs larger than L2)",
     }

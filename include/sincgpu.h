@@ -94,6 +94,8 @@ int sincgpu_fft_length(sincgpu_ctx* ctx);
  * in FP64, so that the energy, the dipole and the next step start from FP64
  * matrices). */
 int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
+/* Current value of an option of sincgpu_set_option (SINCGPU_EINVAL for an unknown name). */
+int sincgpu_get_option(sincgpu_ctx* ctx, const char* name, long long* value);
 
 /* C(M x N, row-major) = A(M x K, row-major) * B(N x K, row-major)^T on the
  * tensor cores (tcgen05 kind::tf32, 3xTF32 split, FP32 accumulation), device
@@ -447,9 +449,13 @@ int sincgpu_batch_create(sincgpu_batch** batch, sincgpu_ctx** ctxs, int n);
 int sincgpu_batch_launch(sincgpu_batch* batch, void* stream);
 int sincgpu_batch_destroy(sincgpu_batch* batch);
 
-/* Autotuner: times the orbital-RHS evaluation for the candidate Coulomb
- * pair-chunk sizes (automatic, all pairs, 1/2, 1/4, 16, 8) and keeps the fastest
- * in the context; returns it and its time. */
+/* Autotuner: times the orbital-RHS evaluation (a warm-up, then the mean of
+ * three) and tunes three launch-shape options in turn, each kept at its fastest
+ * value in the context before the next: the Coulomb pair chunk (automatic, all
+ * pairs, 1/2, 1/4, 16, 8; "coul_chunk"), the twoematel tile edge 16R (automatic,
+ * R = 4..9; "twoe_tile") and the TMA-staged z pass ("coul_tma").  A fixed value
+ * must beat the current one by 2 %.  Returns the chunk and the best time; the
+ * others are read with sincgpu_get_option. */
 int sincgpu_autotune_rhs(sincgpu_ctx* ctx, const double* phi, const double* avector, double* denmat,
                          double* invdenmat, double* reducedpottally, double* twoematel, double* reducedpot,
                          double* outspfs, int* best_chunk, float* best_ms);

@@ -93,6 +93,10 @@ def test_mixed_batch_error_and_autotune(built_lib):
         gp.orbital_rhs_avec_dev(*args(bp))
         chunk, ms = gm.autotune_rhs(*args(bm))
         assert chunk >= 0 and ms > 0
+        # the tuned launch shapes stay in the context
+        assert gm.get_option("coul_chunk") == chunk
+        assert gm.get_option("twoe_tile") in (0, 4, 5, 6, 7, 8, 9)
+        assert gm.get_option("coul_tma") in (-1, 1)
         gm.rhs_graph_capture(*args(bm))
     batch = Batch([m[0] for m in mixed])
     batch.launch()

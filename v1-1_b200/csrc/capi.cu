@@ -326,6 +326,26 @@ int sincgpu_get_tables(sincgpu_ctx* h, double* tempcoulomb, double* pot, double*
 
 int sincgpu_fft_length(sincgpu_ctx* h) { return h ? h->c.P : -1; }
 
+int sincgpu_get_option(sincgpu_ctx* h, const char* name, long long* value) {
+  CTX_CHECK(h);
+  SG_CHECK(name && value, SINCGPU_EINVAL, "null argument");
+  const Ctx& c = h->c;
+  const struct {
+    const char* n;
+    long long v;
+  } opts[] = {{"coul_chunk", c.coul_chunk},       {"coulomb_fp32", c.coul_fp32}, {"contract_tf32", c.contract_tf32},
+              {"coul_tma", c.coul_tma},           {"twoe_tile", c.twoe_tile},    {"orth_fused", c.orth_fused},
+              {"rhs_overlap", c.rhs_overlap},     {"coul_fused", c.coul_fused},  {"coul_z2", c.coul_z2},
+              {"cmf_fp64_last", c.cmf.fp64_last ? 1 : 0}, {"twoe_dmma", c.twoe_dmma}, {"rp_dmma", c.rp_dmma}};
+  for (const auto& o : opts)
+    if (!strcmp(name, o.n)) {
+      *value = o.v;
+      return SINCGPU_OK;
+    }
+  SG_CHECK(false, SINCGPU_EINVAL, "unknown option '%s'", name);
+  return SINCGPU_EINVAL;
+}
+
 int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
   CTX_CHECK(h);
   SG_CHECK(name, SINCGPU_EINVAL, "null option name");

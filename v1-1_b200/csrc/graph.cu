@@ -130,41 +130,78 @@ int sincgpu_autotune_rhs(sincgpu_ctx* h, const double* phi, const double* avecto
   Ctx& c = h->c;
   const int n = c.nspf, npair = n * (n + 1) / 2;
   RhsArgs a{phi, avector, 0.0, -1.0, 0.0, denmat, invdenmat, tally, twoematel, reducedpot, outspfs};
-  std::vector<int> cand = {0, npair, (npair + 1) / 2, (npair + 3) / 4, 16, 8};
-  std::sort(cand.begin(), cand.end());
-  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
   cudaEvent_t e0, e1;
   SG_CUDA(cudaEventCreate(&e0));
   SG_CUDA(cudaEventCreate(&e1));
-  int best = 0;
-  float bms = 1e30f;
-  const int saved = c.coul_chunk;
   int rc = SINCGPU_OK;
-  // pair chunks whose W1/W2 scratch would exceed 512 MiB are not tried
+  // one configuration: a warm-up evaluation (sizes the workspaces), then three timed
+  auto timed = [&](float* ms) -> int {
+    SG_TRY(run_rhs(h, a));
+    cudaEventRecord(e0, c.stream);
+    for (int r = 0; r < 3; ++r) SG_TRY(run_rhs(h, a));
+    cudaEventRecord(e1, c.stream);
+    SG_CUDA(cudaEventSynchronize(e1));
+    cudaEventElapsedTime(ms, e0, e1);
+    *ms /= 3.f;
+    return SINCGPU_OK;
+  };
+  // coordinate descent over three knobs, each kept at its best before the next:
+  // (1) the Coulomb pair chunk (pairs per pass launch); pair chunks whose W1/W2
+  //     scratch would exceed 512 MiB are not tried
+  // (2) the twoematel tile edge 16R (the register block R of the FP64 tensor-core
+  //     GEMM: fewer, larger tiles against less padding and fewer triangle tiles)
+  // (3) the Coulomb z pass plain or with TMA-staged slabs
+  float bms = 1e30f;
+  int best = 0;
+  const int saved_chunk = c.coul_chunk, saved_tile = c.twoe_tile, saved_tma = c.coul_tma;
+  std::vector<int> cand = {0, npair, (npair + 1) / 2, (npair + 3) / 4, 16, 8};
+  std::sort(cand.begin(), cand.end());
+  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
   const size_t csz = c.coul_fp32 ? sizeof(float2) : sizeof(double2);
   const size_t per_pair = csz * ((size_t)c.N * c.N * c.P + (size_t)c.N * c.P * c.P);
   for (int ch : cand) {
     if (ch < 0 || ch > npair) continue;
     if (ch > 0 && per_pair * (size_t)ch > (512ull << 20)) continue;
     c.coul_chunk = ch;
-    if ((rc = run_rhs(h, a)) != SINCGPU_OK) break;  // warm-up (sizes the workspace)
-    cudaEventRecord(e0, c.stream);
-    for (int r = 0; r < 3 && rc == SINCGPU_OK; ++r) rc = run_rhs(h, a);
-    cudaEventRecord(e1, c.stream);
-    cudaEventSynchronize(e1);
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    ms /= 3.f;
-    if (rc != SINCGPU_OK) break;
+    if ((rc = timed(&ms)) != SINCGPU_OK) break;
     if (ms < bms) {
       bms = ms;
       best = ch;
     }
   }
+  if (rc == SINCGPU_OK) {
+    c.coul_chunk = best;
+    int best_tile = 0;
+    for (int t : {4, 5, 6, 7, 8, 9}) {
+      c.twoe_tile = t;
+      float ms = 0.f;
+      if ((rc = timed(&ms)) != SINCGPU_OK) break;
+      if (ms < 0.98f * bms) {  // a fixed tile must beat the automatic one clearly
+        bms = ms;
+        best_tile = t;
+      }
+    }
+    c.twoe_tile = best_tile;
+  }
+  if (rc == SINCGPU_OK) {
+    c.coul_tma = 1;
+    float ms = 0.f;
+    rc = timed(&ms);
+    if (rc == SINCGPU_OK && ms < 0.98f * bms) {
+      bms = ms;
+    } else {
+      c.coul_tma = saved_tma;
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  c.coul_chunk = rc == SINCGPU_OK ? best : saved;
-  if (best_chunk) *best_chunk = best;
+  if (rc != SINCGPU_OK) {
+    c.coul_chunk = saved_chunk;
+    c.twoe_tile = saved_tile;
+    c.coul_tma = saved_tma;
+  }
+  if (best_chunk) *best_chunk = c.coul_chunk;
   if (best_ms) *best_ms = bms;
   return rc;
 }

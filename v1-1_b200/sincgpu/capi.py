@@ -39,6 +39,7 @@ _SIGS = {
     "sincgpu_get_tables": ([_P, _P, _P, _P, _P], _I),
     "sincgpu_fft_length": ([_P], _I),
     "sincgpu_set_option": ([_P, C.c_char_p, _LL], _I),
+    "sincgpu_get_option": ([_P, C.c_char_p, _P], _I),
     "sincgpu_synchronize": ([_P], _I),
     "sincgpu_host_register": ([_P, _LL], _I),
     "sincgpu_host_unregister": ([_P], _I),
@@ -251,6 +252,11 @@ class SincProject:
 
     def set_option(self, name: str, value: int):
         _call("sincgpu_set_option", self._h, name.encode(), int(value))
+
+    def get_option(self, name: str) -> int:
+        v = C.c_longlong(0)
+        _call("sincgpu_get_option", self._h, name.encode(), C.byref(v))
+        return v.value
 
     def synchronize(self):
         _call("sincgpu_synchronize", self._h)
