@@ -66,7 +66,10 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for(P1 * P2)) coul
   load_roots(roots, ca.roots, P);
   const int N = ca.N;
   const int s = threadIdx.x % S, l = threadIdx.x / S;
-  const int p = blockIdx.z, f = blockIdx.x * TL + l;  // row f = z*N + y
+  // pairs run fastest over the grid: the CTAs of one row block for all the
+  // chunk's pairs run together and read the orbitals' rows from L2, so each
+  // orbital is read from DRAM about once per launch instead of once per pair
+  const int p = blockIdx.x, f = blockIdx.y * TL + l;  // row f = z*N + y
   const bool row = f < N * N;
   const long long off = (long long)f * N;
   const double2* s1;
@@ -485,9 +488,9 @@ int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2*
   {
     ProfScope ps(c, ST_COUL_FWD_X);
     if (dens)
-      coul_fwd_x_t<P1, P2, true, C><<<dim3(nrow, 1, np), nthr, 0, c.stream>>>(src1, nullptr, ca);
+      coul_fwd_x_t<P1, P2, true, C><<<dim3(np, nrow), nthr, 0, c.stream>>>(src1, nullptr, ca);
     else
-      coul_fwd_x_t<P1, P2, false, C><<<dim3(nrow, 1, np), nthr, 0, c.stream>>>(src1, src2, ca);
+      coul_fwd_x_t<P1, P2, false, C><<<dim3(np, nrow), nthr, 0, c.stream>>>(src1, src2, ca);
     SG_LAUNCHED();
   }
   {
