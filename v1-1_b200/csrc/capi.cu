@@ -385,6 +385,11 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
     h->c.rp_dmma = (int)value;
     return SINCGPU_OK;
   }
+  if (!strcmp(name, "coul_zwide")) {
+    SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "coul_zwide must be 0 or 1");
+    h->c.coul_zwide = (int)value;
+    return SINCGPU_OK;
+  }
   if (!strcmp(name, "coul_z2")) {
     SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "coul_z2 must be 0 or 1");
     h->c.coul_z2 = (int)value;
