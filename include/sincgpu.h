@@ -92,7 +92,9 @@ int sincgpu_fft_length(sincgpu_ctx* ctx);
  * HBM; results agree to rounding); "cmf_fp64_last" (1: in the precision form,
  * the last mean-field build of each CMF step and its post-prop reducedpot run
  * in FP64, so that the energy, the dipole and the next step start from FP64
- * matrices). */
+ * matrices); "ke_tf32" (1: the per-axis kinetic contraction on the tcgen05
+ * tensor cores, one 3xTF32 GEMM per axis with FP32 accumulation, the precision
+ * form; 0: FP64 tensor cores). */
 int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
 /* Current value of an option of sincgpu_set_option (SINCGPU_EINVAL for an unknown name). */
 int sincgpu_get_option(sincgpu_ctx* ctx, const char* name, long long* value);

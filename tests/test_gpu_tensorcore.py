@@ -71,3 +71,61 @@ def test_reducedpot_tf32_contraction(built_lib):
         assert rhs_err < 1e-6, rhs_err
     finally:
         p.close()
+
+
+@pytest.mark.parametrize("N,d,howmany", [(21, 0.4, 3), (41, 0.25, 2)])
+def test_kinetic_tf32_contraction(built_lib, N, d, howmany):
+    """The kinetic contraction on the tcgen05 tensor cores (option ke_tf32: one
+    3xTF32 GEMM per axis, the lines of the grid against the N x N sine-DVR matrix)
+    against the FP64 tensor-core path and the oracle, within 1e-6 of the largest
+    magnitude; and the orbital RHS with it."""
+    import torch
+    from oracle import sinc_oracle as orc
+    from sincgpu import SincProject
+    p = SincProject(N, d, [[0, 0, 0]], [2.0], howmany)
+    try:
+        sysm = orc.SincSystem(N, d, [[0, 0, 0]], [2.0])
+        phi = orc.seeded_orbitals(sysm, howmany, seed=N)
+        ref = sysm.mult_ke(phi)
+        dphi = torch.from_numpy(np.ascontiguousarray(phi.T)).cuda()
+        out64 = torch.empty_like(dphi)
+        out32 = torch.full_like(dphi, float("nan"))
+        p.mult_ke_dev(dphi, out64, howmany)
+        p.set_option("ke_tf32", 1)
+        p.mult_ke_dev(dphi, out32, howmany)
+        p.set_option("ke_tf32", 0)
+        torch.cuda.synchronize()
+        a64, a32 = out64.cpu().numpy().T, out32.cpu().numpy().T
+        assert np.isfinite(a32).all()
+        assert np.abs(a64 - ref).max() / np.abs(ref).max() < 1e-11
+        err = np.abs(a32 - ref).max() / np.abs(ref).max()
+        print(f"kinetic 3xTF32 N={N}: {err:.3g}")
+        assert err < 1e-6, err
+    finally:
+        p.close()
+
+
+def test_orbital_rhs_with_kinetic_tf32(built_lib):
+    """The orbital RHS (the potential and z-field terms ride in the first axis's
+    epilogue) with ke_tf32 and contract_tf32 against the FP64 form at 1e-6."""
+    from oracle import sinc_oracle as orc
+    from sincgpu import SincProject, WalkTables
+    n = 5
+    p = SincProject(21, 0.4, [[0, 0, 0]], [2.0], n)
+    try:
+        sysm = orc.SincSystem(21, 0.4, [[0, 0, 0]], [2.0])
+        phi = orc.seeded_orbitals(sysm, n, seed=8)
+        w = WalkTables(2, n, 0)
+        p.ci_attach(w)
+        rng = np.random.default_rng(9)
+        av = rng.standard_normal(w.numconfig) + 1j * rng.standard_normal(w.numconfig)
+        av /= np.linalg.norm(av)
+        o64 = p.orbital_rhs_avec(phi, av, ztdpot=0.02)
+        p.set_option("ke_tf32", 1)
+        p.set_option("contract_tf32", 1)
+        o32 = p.orbital_rhs_avec(phi, av, ztdpot=0.02)
+        err = np.abs(o32 - o64).max() / np.abs(o64).max()
+        print(f"orbital RHS, kinetic + reducedpot 3xTF32: {err:.3g}")
+        assert err < 1e-6, err
+    finally:
+        p.close()

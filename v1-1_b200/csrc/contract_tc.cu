@@ -40,6 +40,27 @@ struct RedpotEpi {
   int n;
 };
 
+// Row m of A starts at (m % Mlo) lam + (m / Mlo) lam2 (two-level rows: the lines
+// of a 3-D grid along one axis); element k of the row is k lak further.
+struct ARows {
+  long long lam, Mlo, lam2, lak;
+  __device__ __forceinline__ long long row(long long m) const { return (m % Mlo) * lam + (m / Mlo) * lam2; }
+};
+
+// kinetic epilogue: element (m, j) of one axis's contraction at out[row(m) + j lak]
+// (the same addressing as the input lines); `first` writes it, adding the
+// potential and z-field terms times the input when `extra`, otherwise it adds
+struct KeEpi {
+  double* out;
+  const double* in;
+  ARows ar;
+  int first, extra;
+  const double* pot;
+  const double* zdip;
+  double zfield;
+  long long G;
+};
+
 template <int KC>
 struct TileSmem {
   static constexpr int kA = KC * 128;  // u32 per A tile (hi or lo)
@@ -53,8 +74,8 @@ struct TileSmem {
 // 0-3 stage A (one row per thread), warps 4-7 stage B; every thread issues all of
 // its global loads before the first split, so a warp has KC loads in flight.
 template <int KC>
-__device__ __forceinline__ void stage_tile(uint32_t* base, int NT, const double* __restrict__ A, long long lam,
-                                           long long lak, long long M, long long m0, const double* __restrict__ B,
+__device__ __forceinline__ void stage_tile(uint32_t* base, int NT, const double* __restrict__ A, ARows ar,
+                                           long long M, long long m0, const double* __restrict__ B,
                                            long long lbn, long long lbk, int Ntot, int n0, int K, int k0) {
   uint32_t* Ahi = base;
   uint32_t* Alo = Ahi + TileSmem<KC>::kA;
@@ -63,9 +84,10 @@ __device__ __forceinline__ void stage_tile(uint32_t* base, int NT, const double*
   const int tid = threadIdx.x;
   if (tid < 128) {
     const long long m = m0 + tid;
+    const long long rb = m < M ? ar.row(m) : 0;
     double v[KC];
 #pragma unroll
-    for (int k = 0; k < KC; ++k) v[k] = (m < M && k0 + k < K) ? A[m * lam + (long long)(k0 + k) * lak] : 0.0;
+    for (int k = 0; k < KC; ++k) v[k] = (m < M && k0 + k < K) ? A[rb + (long long)(k0 + k) * ar.lak] : 0.0;
 #pragma unroll
     for (int c = 0; c < KC / 4; ++c) {
       uint4 h, l;
@@ -124,6 +146,28 @@ __device__ __forceinline__ void apply_epi<StoreEpi>(const StoreEpi& e, long long
 }
 
 template <>
+__device__ __forceinline__ void apply_epi<KeEpi>(const KeEpi& e, long long m, long long M, int n, int Ntot,
+                                                 const float (&v)[8]) {
+  if (m >= M) return;
+  const long long rb = e.ar.row(m);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    if (n + j >= Ntot) break;
+    const long long a = rb + (long long)(n + j) * e.ar.lak;
+    if (e.first) {
+      double w = (double)v[j];
+      if (e.extra) {
+        const long long gidx = (a >> 1) % e.G;  // grid point of the complex element
+        w = fma(e.pot[gidx] + e.zfield * e.zdip[gidx], e.in[a], w);
+      }
+      e.out[a] = w;
+    } else {
+      e.out[a] += (double)v[j];
+    }
+  }
+}
+
+template <>
 __device__ __forceinline__ void apply_epi<RedpotEpi>(const RedpotEpi& e, long long m, long long M, int n,
                                                      int Ntot, const float (&v)[8]) {
   if (m >= M) return;
@@ -144,8 +188,7 @@ __device__ __forceinline__ void apply_epi<RedpotEpi>(const RedpotEpi& e, long lo
 }
 
 template <int KC, class Epi>
-__global__ void __launch_bounds__(256) gemm_tf32x3_kernel(const double* __restrict__ A, long long lam,
-                                                          long long lak, long long M,
+__global__ void __launch_bounds__(256) gemm_tf32x3_kernel(const double* __restrict__ A, ARows ar, long long M,
                                                           const double* __restrict__ B, long long lbn,
                                                           long long lbk, int Ntot, int K, int NT,
                                                           uint32_t tmem_cols, Epi epi, int* __restrict__ err) {
@@ -163,7 +206,7 @@ __global__ void __launch_bounds__(256) gemm_tf32x3_kernel(const double* __restri
     umma::mbar_init(&mbar[1], 1);
   }
   const int nch = (K + KC - 1) / KC;
-  stage_tile<KC>(st[0], NT, A, lam, lak, M, m0, B, lbn, lbk, Ntot, n0, K, 0);
+  stage_tile<KC>(st[0], NT, A, ar, M, m0, B, lbn, lbk, Ntot, n0, K, 0);
   umma::fence_smem_to_async();
   umma::fence_before_sync();
   __syncthreads();
@@ -194,7 +237,7 @@ __global__ void __launch_bounds__(256) gemm_tf32x3_kernel(const double* __restri
     if (ch + 1 < nch) {
       // the other stage was read by the MMAs of chunk ch - 1
       if (ch >= 1 && ok) ok = umma::mbar_wait(&mbar[s ^ 1], ((ch - 1) >> 1) & 1, kWaitLimit);
-      if (ok) stage_tile<KC>(st[s ^ 1], NT, A, lam, lak, M, m0, B, lbn, lbk, Ntot, n0, K, (ch + 1) * KC);
+      if (ok) stage_tile<KC>(st[s ^ 1], NT, A, ar, M, m0, B, lbn, lbk, Ntot, n0, K, (ch + 1) * KC);
       umma::fence_smem_to_async();
     }
     umma::fence_before_sync();
@@ -232,8 +275,8 @@ constexpr int kSmemDyn = 224 * 1024;  // dynamic limit (the static mbarriers tak
 // more than its tiles need, so that every descriptor address stays inside the
 // CTA's allocation).
 template <class Epi>
-int launch_tf32x3(Ctx& c, const double* A, long long lam, long long lak, long long M, const double* B,
-                  long long lbn, long long lbk, int Ntot, int K, const Epi& epi, size_t smem_min = 0) {
+int launch_tf32x3(Ctx& c, const double* A, ARows ar, long long M, const double* B, long long lbn, long long lbk,
+                  int Ntot, int K, const Epi& epi, size_t smem_min = 0) {
   SG_CHECK(M >= 1 && Ntot >= 1 && K >= 1, SINCGPU_EINVAL, "empty tensor-core contraction");
   const int ntile = ceil_div(Ntot, 256);
   const int NT = ceil_div(ceil_div(Ntot, ntile), 16) * 16;
@@ -246,8 +289,7 @@ int launch_tf32x3(Ctx& c, const double* A, long long lam, long long lak, long lo
   int* err = nullptr;
   SG_TRY(timeout_flags(c, &err));
   const dim3 grid((unsigned)ceil_div(M, 128), (unsigned)ntile);
-  gemm_tf32x3_kernel<kKC, Epi><<<grid, 256, smem, c.stream>>>(A, lam, lak, M, B, lbn, lbk, Ntot, K, NT, cols, epi,
-                                                              err);
+  gemm_tf32x3_kernel<kKC, Epi><<<grid, 256, smem, c.stream>>>(A, ar, M, B, lbn, lbk, Ntot, K, NT, cols, epi, err);
   SG_LAUNCHED();
   return SINCGPU_OK;
 }
@@ -282,7 +324,31 @@ int tc_error_read(Ctx& c, int* flag) {
 int rp_gemm_tf32(Ctx& c, const double* Rpl, const double* Wm, int K, int NC, const int* d_tmap,
                  double2* reducedpot) {
   RedpotEpi e{reducedpot, c.G, d_tmap, c.nspf};
-  return launch_tf32x3(c, Rpl, 1, c.G, c.G, Wm, 1, NC, NC, K, e);
+  return launch_tf32x3(c, Rpl, ARows{1, c.G, 0, c.G}, c.G, Wm, 1, NC, NC, K, e);
+}
+
+// The per-axis kinetic contraction on the tensor cores (precision form, option
+// ke_tf32): out(.., j, ..) = sum_l K(j, l) in(.., l, ..) along x, y and z, real and
+// imaginary parts as separate lines, one 3xTF32 GEMM per axis (lines x N x N
+// against ketile, FP32 accumulation, FP64 sums across the axes), the potential
+// and z-field terms added in the first axis's epilogue.  Same result as mult_ke to
+// about 1e-7 of the kinetic term.
+int mult_ke_tf32(Ctx& c, const double2* in, double2* out, int howmany, bool extra, double zfield) {
+  const long long N = c.N, NN = N * N, G = c.G;
+  const double* A = reinterpret_cast<const double*>(in);
+  double* O = reinterpret_cast<double*>(out);
+  // line = (re/im, the other two coordinates, orbital); element l along the axis
+  const ARows ax{1, 2, 2 * N, 2}, ay{1, 2 * N, 2 * NN, 2 * N}, az{1, 2 * NN, 2 * G, 2 * NN};
+  const long long M = 2 * NN * howmany;
+  {
+    ProfScope ps(c, ST_KE_XY);
+    SG_TRY(launch_tf32x3(c, A, ax, M, c.d_ketile, c.ke_stride, 1, c.N, c.N,
+                         KeEpi{O, A, ax, 1, extra ? 1 : 0, c.d_pot, c.d_zdip, zfield, G}));
+    SG_TRY(launch_tf32x3(c, A, ay, M, c.d_ketile, c.ke_stride, 1, c.N, c.N,
+                         KeEpi{O, A, ay, 0, 0, nullptr, nullptr, 0.0, G}));
+  }
+  ProfScope ps(c, ST_KE_Z);
+  return launch_tf32x3(c, A, az, M, c.d_ketile, c.ke_stride, 1, c.N, c.N, KeEpi{O, A, az, 0, 0, nullptr, nullptr, 0.0, G});
 }
 
 }  // namespace sincgpu
@@ -308,7 +374,7 @@ extern "C" int sincgpu_gemm_tf32x3_dev(sincgpu_ctx* h, const double* A, const do
   SG_CHECK(M >= 1 && N >= 1 && K >= 1, SINCGPU_EINVAL, "bad sizes");
   SG_TRY(tc_error_reset(c));
   StoreEpi e{C, N, 1};
-  SG_TRY(launch_tf32x3(c, A, K, 1, M, B, K, 1, N, K, e, 200 * 1024));
+  SG_TRY(launch_tf32x3(c, A, ARows{K, M, 0, 1}, M, B, K, 1, N, K, e, 200 * 1024));
   int flag = 0;
   SG_TRY(tc_error_read(c, &flag));
   if (timed_out) *timed_out = flag;

@@ -181,63 +181,6 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_z<C>(P1 * P2))
   }
 }
 
-// CZ with TLW lines per CTA and the exchange in dynamic shared memory (wider
-// column blocks: each z-plane access of a CTA is TLW consecutive values).
-// Otherwise coul_z_t.
-template <int P1, int P2, class C, int TLW>
-__global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * TLW) coul_z_wide_t(CoulArgs<C> ca) {
-  constexpr int P = P1 * P2, TL = TLW;
-  __shared__ C roots[P];
-  extern __shared__ __align__(16) unsigned char zw_raw[];
-  C* ex = reinterpret_cast<C*>(zw_raw);
-  load_roots(roots, ca.roots, P);
-  const int N = ca.N;
-  const int l = threadIdx.x % TL, s = threadIdx.x / TL;
-  const int p = blockIdx.z, f = blockIdx.x * TL + l;  // column f = ky*P + kx
-  const long long zs = (long long)P * P;
-  const bool col = f < zs;
-  C* base = ca.W2 + (long long)p * N * zs + f;
-  C a[P1], b[P2];
-#pragma unroll
-  for (int n1 = 0; n1 < P1; ++n1) {
-    const int z = s + P2 * n1;
-    a[n1] = (col && s < P2 && z < N) ? base[z * zs] : CplxTraits<C>::make(0.0, 0.0);
-  }
-  __syncthreads();
-  dft_in_to_out<P1, P2, false, C>(a, b, s, l, TL, ex, roots);
-  if (col && s < P1) {
-    if constexpr (P <= 128) {
-      // the spectrum is real and even in each axis: read it on the octant (a table
-      // of (P/2+1)^3 values that stays in L2 while the W2 slab streams through).
-      // Measured on the 41^3 grid (P = 81): z pass 0.165 -> 0.148 ms; on the 81^3
-      // grid (P = 162) it was slower (4.8 -> 6.7 ms), so longer lines keep the
-      // complex table
-      using R = typename CplxTraits<C>::Real;
-      constexpr int H = P / 2 + 1;
-      const int ky = f / P, kx = f - ky * P;
-      const R* kh = ca.khr + ((ky <= P - ky ? ky : P - ky) * H + (kx <= P - kx ? kx : P - kx));
-#pragma unroll
-      for (int k2 = 0; k2 < P2; ++k2) {
-        const int kz = s + P1 * k2;
-        const R w = kh[(kz <= P - kz ? kz : P - kz) * H * H];
-        b[k2] = CplxTraits<C>::make(b[k2].x * w, b[k2].y * w);
-      }
-    } else {
-      const C* kh = ca.khat + f;
-#pragma unroll
-      for (int k2 = 0; k2 < P2; ++k2) b[k2] = cmul(b[k2], kh[(long long)(s + P1 * k2) * zs]);
-    }
-  }
-  dft_out_to_in<P1, P2, true, C, false, false>(b, a, s, l, TL, ex, roots);
-  if (col && s < P2) {
-#pragma unroll
-    for (int m1 = 0; m1 < P1; ++m1) {
-      const int z = s + P2 * m1;
-      if (z < N) base[z * zs] = a[m1];
-    }
-  }
-}
-
 // CZ for lengths P = P1 * P2 with P1 = 2 P2 (162 = 18 x 9): the plain z pass
 // gives each line max(P1, P2) = P1 threads, and half of them idle in the steps
 // with P2 sub-transforms (the loads, the first forward step, the last inverse
@@ -586,13 +529,6 @@ int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2*
             coul_z2_t<P1, P2, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
         SG_CUDA(attr);
         coul_z2_t<P1, P2, C><<<dim3(ceil_div(P * P, TL2), 1, np), P2 * TL2, dyn, c.stream>>>(ca);
-      } else if (c.coul_zwide && sizeof(C) == 16) {
-        constexpr int TLW = 32;
-        const size_t dyn = sizeof(C) * (size_t)P * TLW;
-        static const cudaError_t attr = cudaFuncSetAttribute(
-            coul_z_wide_t<P1, P2, C, TLW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-        SG_CUDA(attr);
-        coul_z_wide_t<P1, P2, C, TLW><<<dim3(ceil_div(P * P, TLW), 1, np), S * TLW, dyn, c.stream>>>(ca);
       } else {
         coul_z_t<P1, P2, C><<<dim3(nzc, 1, np), S * TLZ, 0, c.stream>>>(ca);
       }

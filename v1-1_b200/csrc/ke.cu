@@ -172,7 +172,10 @@ __global__ void __launch_bounds__(256) ke_z_kernel(const double2* __restrict__ i
   }
 }
 
+int mult_ke_tf32(Ctx& c, const double2* in, double2* out, int howmany, bool extra, double zfield);  // contract_tc.cu
+
 int mult_ke(Ctx& c, const double2* in, double2* out, int howmany, bool extra, double zfield) {
+  if (c.ke_tf32) return mult_ke_tf32(c, in, out, howmany, extra, zfield);
   const int N = c.N;
   KeArgs ka{};
   ka.N = N;
