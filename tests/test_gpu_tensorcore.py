@@ -22,8 +22,9 @@ def proj(built_lib):
     p.close()
 
 
+@pytest.mark.parametrize("kc", [16, 32])
 @pytest.mark.parametrize("m,n,k", [(128, 16, 8), (300, 40, 37), (1000, 272, 272), (77, 256, 64), (129, 112, 110)])
-def test_gemm_tf32x3_matches_fp64(proj, m, n, k):
+def test_gemm_tf32x3_matches_fp64(proj, m, n, k, kc):
     import torch
     g = torch.Generator().manual_seed(m * 7 + n * 3 + k)
     a = torch.randn(m, k, generator=g, dtype=torch.float64)
@@ -31,7 +32,11 @@ def test_gemm_tf32x3_matches_fp64(proj, m, n, k):
     ref = (a @ b.T).numpy()
     da, db = a.cuda(), b.cuda()
     out = torch.full((m, n), float("nan"), dtype=torch.float64, device="cuda")
-    assert proj.gemm_tf32x3_dev(da, db, out) == 0
+    proj.set_option("tc_kc", kc)
+    try:
+        assert proj.gemm_tf32x3_dev(da, db, out) == 0
+    finally:
+        proj.set_option("tc_kc", 16)
     got = out.cpu().numpy()
     assert np.isfinite(got).all()
     err = np.abs(got - ref).max() / np.abs(ref).max()

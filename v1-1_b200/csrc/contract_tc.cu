@@ -268,30 +268,38 @@ __global__ void __launch_bounds__(256) gemm_tf32x3_kernel(const double* __restri
   if (warp == 0) umma::tmem_dealloc(tmem, tmem_cols);
 }
 
-constexpr int kKC = 16;
 constexpr int kSmemDyn = 224 * 1024;  // dynamic limit (the static mbarriers take the rest of 227 KB)
 
-// smem_min: dynamic shared memory to reserve at least (the self test reserves
-// more than its tiles need, so that every descriptor address stays inside the
-// CTA's allocation).
-template <class Epi>
-int launch_tf32x3(Ctx& c, const double* A, ARows ar, long long M, const double* B, long long lbn, long long lbk,
-                  int Ntot, int K, const Epi& epi, size_t smem_min = 0) {
-  SG_CHECK(M >= 1 && Ntot >= 1 && K >= 1, SINCGPU_EINVAL, "empty tensor-core contraction");
+template <int KC, class Epi>
+int launch_tf32x3_kc(Ctx& c, const double* A, ARows ar, long long M, const double* B, long long lbn, long long lbk,
+                     int Ntot, int K, const Epi& epi, size_t smem_min) {
   const int ntile = ceil_div(Ntot, 256);
   const int NT = ceil_div(ceil_div(Ntot, ntile), 16) * 16;
   const uint32_t cols = NT <= 32 ? 32 : NT <= 64 ? 64 : NT <= 128 ? 128 : 256;
-  const size_t smem = std::max(TileSmem<kKC>::bytes(NT), std::min<size_t>(smem_min, kSmemDyn));
+  const size_t smem = std::max(TileSmem<KC>::bytes(NT), std::min<size_t>(smem_min, kSmemDyn));
+  SG_CHECK(smem <= (size_t)kSmemDyn, SINCGPU_ERANGE, "tensor-core tile needs %zu bytes of shared memory", smem);
   // process-wide attribute, one fixed value (thread-safe static initialisation)
-  static const cudaError_t attr = cudaFuncSetAttribute(gemm_tf32x3_kernel<kKC, Epi>,
+  static const cudaError_t attr = cudaFuncSetAttribute(gemm_tf32x3_kernel<KC, Epi>,
                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDyn);
   SG_CUDA(attr);
   int* err = nullptr;
   SG_TRY(timeout_flags(c, &err));
   const dim3 grid((unsigned)ceil_div(M, 128), (unsigned)ntile);
-  gemm_tf32x3_kernel<kKC, Epi><<<grid, 256, smem, c.stream>>>(A, ar, M, B, lbn, lbk, Ntot, K, NT, cols, epi, err);
+  gemm_tf32x3_kernel<KC, Epi><<<grid, 256, smem, c.stream>>>(A, ar, M, B, lbn, lbk, Ntot, K, NT, cols, epi, err);
   SG_LAUNCHED();
   return SINCGPU_OK;
+}
+
+// smem_min: dynamic shared memory to reserve at least (the self test reserves
+// more than its tiles need, so that every descriptor address stays inside the
+// CTA's allocation).  K chunks of 16 (two CTAs per SM) or, with the context
+// option tc_kc = 32, of 32 (one CTA per SM, twice the MMAs per commit).
+template <class Epi>
+int launch_tf32x3(Ctx& c, const double* A, ARows ar, long long M, const double* B, long long lbn, long long lbk,
+                  int Ntot, int K, const Epi& epi, size_t smem_min = 0) {
+  SG_CHECK(M >= 1 && Ntot >= 1 && K >= 1, SINCGPU_EINVAL, "empty tensor-core contraction");
+  if (c.tc_kc == 32) return launch_tf32x3_kc<32>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);
+  return launch_tf32x3_kc<16>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);
 }
 
 }  // namespace
