@@ -22,9 +22,20 @@ def proj(built_lib):
     p.close()
 
 
-@pytest.mark.parametrize("kc", [16, 32])
+MODES = {"kc16": {"tc_kc": 16, "tc_pipe": 0}, "kc32": {"tc_kc": 32, "tc_pipe": 0},
+         "ring": {"tc_kc": 16, "tc_pipe": 1}}
+
+
+def set_mode(p, mode):
+    for name, v in MODES[mode].items():
+        p.set_option(name, v)
+
+
+@pytest.mark.parametrize("mode", list(MODES))
 @pytest.mark.parametrize("m,n,k", [(128, 16, 8), (300, 40, 37), (1000, 272, 272), (77, 256, 64), (129, 112, 110)])
-def test_gemm_tf32x3_matches_fp64(proj, m, n, k, kc):
+def test_gemm_tf32x3_matches_fp64(proj, m, n, k, mode):
+    """The three forms of the kernel: K chunks of 16 (two CTAs per SM), of 32, and
+    the ring of staged chunks with a separate MMA-issuing warp (tc_pipe)."""
     import torch
     g = torch.Generator().manual_seed(m * 7 + n * 3 + k)
     a = torch.randn(m, k, generator=g, dtype=torch.float64)
@@ -32,11 +43,12 @@ def test_gemm_tf32x3_matches_fp64(proj, m, n, k, kc):
     ref = (a @ b.T).numpy()
     da, db = a.cuda(), b.cuda()
     out = torch.full((m, n), float("nan"), dtype=torch.float64, device="cuda")
-    proj.set_option("tc_kc", kc)
+    set_mode(proj, mode)
     try:
         assert proj.gemm_tf32x3_dev(da, db, out) == 0
     finally:
-        proj.set_option("tc_kc", 16)
+        set_mode(proj, "kc16")
+    assert proj.kernel_timeouts()[0] == 0
     got = out.cpu().numpy()
     assert np.isfinite(got).all()
     err = np.abs(got - ref).max() / np.abs(ref).max()
@@ -44,7 +56,8 @@ def test_gemm_tf32x3_matches_fp64(proj, m, n, k, kc):
     assert err < 5e-6, err
 
 
-def test_reducedpot_tf32_contraction(built_lib):
+@pytest.mark.parametrize("mode", ["kc16", "ring"])
+def test_reducedpot_tf32_contraction(built_lib, mode):
     import torch
     from oracle import sinc_oracle as orc
     from sincgpu import SincProject, WalkTables
@@ -66,8 +79,10 @@ def test_reducedpot_tf32_contraction(built_lib):
         red64 = bufs[4].clone()
         out64 = bufs[5].clone()
         p.set_option("contract_tf32", 1)
+        set_mode(p, mode)
         p.orbital_rhs_avec_dev(phi, av, *bufs)
         p.set_option("contract_tf32", 0)
+        assert p.kernel_timeouts()[0] == 0
         red = bufs[4]
         err = (red - red64).abs().max().item() / red64.abs().max().item()
         rhs_err = (bufs[5] - out64).abs().max().item() / out64.abs().max().item()

@@ -268,6 +268,105 @@ __global__ void __launch_bounds__(256) gemm_tf32x3_kernel(const double* __restri
   if (warp == 0) umma::tmem_dealloc(tmem, tmem_cols);
 }
 
+// Pipelined form of gemm_tf32x3_kernel: the 256 staging threads (warps 0-3: A
+// rows, warps 4-7: B columns) fill a ring of ST stages ahead of the tensor core,
+// and a ninth warp issues the MMAs.  Stage s is handed over by mbarriers: the
+// staging threads arrive on full[s] after their shared-memory stores (with the
+// async-proxy fence), the issuing thread waits on it, issues the stage's MMAs and
+// commits them to empty[s], which the staging threads wait on before refilling
+// the stage.  No block-wide barrier inside the K loop, so global loads of the
+// next stages overlap the MMAs of the current one.  Every wait is bounded; a
+// timeout sets *err and the CTA skips the rest of its work (no hang).
+template <int KC, int ST, class Epi>
+__global__ void __launch_bounds__(288) gemm_tf32x3_ws_kernel(const double* __restrict__ A, ARows ar, long long M,
+                                                             const double* __restrict__ B, long long lbn,
+                                                             long long lbk, int Ntot, int K, int NT,
+                                                             uint32_t tmem_cols, Epi epi, int* __restrict__ err) {
+  extern __shared__ __align__(128) uint32_t tsm[];
+  __shared__ __align__(8) uint64_t full[ST], empty[ST], done;
+  __shared__ uint32_t tmem_base;
+  __shared__ int fail;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const long long m0 = (long long)blockIdx.x * 128;
+  const int n0 = blockIdx.y * NT;
+  const size_t stage_u32 = TileSmem<KC>::bytes(NT) / sizeof(uint32_t) / 2;
+  if (warp == 0) umma::tmem_alloc(&tmem_base, tmem_cols);
+  if (tid == 0) {
+    for (int s = 0; s < ST; ++s) {
+      umma::mbar_init(&full[s], 256);
+      umma::mbar_init(&empty[s], 1);
+    }
+    umma::mbar_init(&done, 1);
+    fail = 0;
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  const int nch = (K + KC - 1) / KC;
+  if (warp < 8) {
+    // staging threads
+    for (int ch = 0; ch < nch; ++ch) {
+      const int s = ch % ST;
+      if (ch >= ST && !umma::mbar_wait(&empty[s], ((ch / ST) - 1) & 1, kWaitLimit)) {
+        atomicExch(&fail, 1);
+        break;
+      }
+      if (fail) break;
+      stage_tile<KC>(tsm + (size_t)s * stage_u32, NT, A, ar, M, m0, B, lbn, lbk, Ntot, n0, K, ch * KC);
+      umma::fence_smem_to_async();
+      umma::mbar_arrive(&full[s]);
+    }
+  } else if (lane == 0) {
+    // the issuing thread
+    const uint32_t idesc = umma::idesc_tf32(128, NT);
+    for (int ch = 0; ch < nch; ++ch) {
+      const int s = ch % ST;
+      if (!umma::mbar_wait(&full[s], (ch / ST) & 1, kWaitLimit)) {
+        atomicExch(&fail, 1);
+        break;
+      }
+      umma::fence_after_sync();
+      const uint32_t a_hi = umma::smem_u32(tsm + (size_t)s * stage_u32);
+      const uint32_t a_lo = a_hi + 4u * TileSmem<KC>::kA;
+      const uint32_t b_hi = a_lo + 4u * TileSmem<KC>::kA;
+      const uint32_t b_lo = b_hi + 4u * KC * NT;
+#pragma unroll
+      for (int ks = 0; ks < KC / 8; ++ks) {
+        const uint32_t ao = ks * 2 * 128 * 16, bo = ks * 2 * NT * 16;
+        const uint64_t ah = umma::desc_kmajor(a_hi + ao, 128 * 16, 128);
+        const uint64_t al = umma::desc_kmajor(a_lo + ao, 128 * 16, 128);
+        const uint64_t bh = umma::desc_kmajor(b_hi + bo, NT * 16, 128);
+        const uint64_t bl = umma::desc_kmajor(b_lo + bo, NT * 16, 128);
+        umma::mma_tf32(tmem, ah, bh, idesc, ch > 0 || ks > 0);
+        umma::mma_tf32(tmem, ah, bl, idesc, true);
+        umma::mma_tf32(tmem, al, bh, idesc, true);
+      }
+      umma::commit(&empty[s]);
+    }
+    umma::commit(&done);  // arrives when every MMA issued above has completed
+  }
+  // everyone: the accumulator is final once `done` completes (bounded)
+  bool ok = umma::mbar_wait(&done, 0, kWaitLimit);
+  __syncthreads();
+  ok = ok && !fail;
+  if (!ok && tid == 0) atomicExch(err, 1);
+  umma::fence_after_sync();
+  if (ok && warp < 8) {
+    const int q = warp & 3, h = warp >> 2;
+    const long long m = m0 + 32 * q + lane;
+    for (int c0 = h * (NT / 2); c0 < (h + 1) * (NT / 2); c0 += 8) {
+      float v[8];
+      umma::tmem_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+      umma::tmem_ld_wait();
+      apply_epi(epi, m, M, n0 + c0, Ntot, v);
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, tmem_cols);
+}
+
 constexpr int kSmemDyn = 224 * 1024;  // dynamic limit (the static mbarriers take the rest of 227 KB)
 
 template <int KC, class Epi>
@@ -290,6 +389,26 @@ int launch_tf32x3_kc(Ctx& c, const double* A, ARows ar, long long M, const doubl
   return SINCGPU_OK;
 }
 
+template <int KC, int ST, class Epi>
+int launch_tf32x3_ws(Ctx& c, const double* A, ARows ar, long long M, const double* B, long long lbn, long long lbk,
+                     int Ntot, int K, const Epi& epi, size_t smem_min) {
+  const int ntile = ceil_div(Ntot, 256);
+  const int NT = ceil_div(ceil_div(Ntot, ntile), 16) * 16;
+  const uint32_t cols = NT <= 32 ? 32 : NT <= 64 ? 64 : NT <= 128 ? 128 : 256;
+  const size_t smem = std::max(ST * TileSmem<KC>::bytes(NT) / 2, std::min<size_t>(smem_min, kSmemDyn));
+  SG_CHECK(smem <= (size_t)kSmemDyn, SINCGPU_ERANGE, "tensor-core stages need %zu bytes of shared memory", smem);
+  static const cudaError_t attr = cudaFuncSetAttribute(gemm_tf32x3_ws_kernel<KC, ST, Epi>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDyn);
+  SG_CUDA(attr);
+  int* err = nullptr;
+  SG_TRY(timeout_flags(c, &err));
+  const dim3 grid((unsigned)ceil_div(M, 128), (unsigned)ntile);
+  gemm_tf32x3_ws_kernel<KC, ST, Epi><<<grid, 288, smem, c.stream>>>(A, ar, M, B, lbn, lbk, Ntot, K, NT, cols, epi,
+                                                                      err);
+  SG_LAUNCHED();
+  return SINCGPU_OK;
+}
+
 // smem_min: dynamic shared memory to reserve at least (the self test reserves
 // more than its tiles need, so that every descriptor address stays inside the
 // CTA's allocation).  K chunks of 16 (two CTAs per SM) or, with the context
@@ -298,6 +417,7 @@ template <class Epi>
 int launch_tf32x3(Ctx& c, const double* A, ARows ar, long long M, const double* B, long long lbn, long long lbk,
                   int Ntot, int K, const Epi& epi, size_t smem_min = 0) {
   SG_CHECK(M >= 1 && Ntot >= 1 && K >= 1, SINCGPU_EINVAL, "empty tensor-core contraction");
+  if (c.tc_pipe) return launch_tf32x3_ws<16, 3>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);
   if (c.tc_kc == 32) return launch_tf32x3_kc<32>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);
   return launch_tf32x3_kc<16>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);
 }

@@ -86,6 +86,12 @@ __device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// One arrival (release: the thread's earlier shared-memory writes are visible to
+// whoever completes a wait on this phase).
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
+}
+
 // Waits for the completion of phase `parity`; gives up after `limit` polls and
 // returns false (the caller records the timeout instead of hanging).
 __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t limit) {
