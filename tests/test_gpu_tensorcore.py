@@ -23,7 +23,8 @@ def proj(built_lib):
 
 
 MODES = {"kc16": {"tc_kc": 16, "tc_pipe": 0}, "kc32": {"tc_kc": 32, "tc_pipe": 0},
-         "ring": {"tc_kc": 16, "tc_pipe": 1}}
+         "ring": {"tc_kc": 16, "tc_pipe": 1}, "ring4": {"tc_kc": 16, "tc_pipe": 2},
+         "ring8": {"tc_kc": 16, "tc_pipe": 3}}
 
 
 def set_mode(p, mode):

@@ -386,7 +386,8 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
     return SINCGPU_OK;
   }
   if (!strcmp(name, "tc_pipe")) {
-    SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "tc_pipe must be 0 or 1");
+    SG_CHECK(value >= 0 && value <= 3, SINCGPU_EINVAL, "tc_pipe must be 0 (two stages, no ring), 1 (ring of 3 x 16), "
+             "2 (4 x 16) or 3 (6 x 8)");
     h->c.tc_pipe = (int)value;
     return SINCGPU_OK;
   }

@@ -417,7 +417,9 @@ template <class Epi>
 int launch_tf32x3(Ctx& c, const double* A, ARows ar, long long M, const double* B, long long lbn, long long lbk,
                   int Ntot, int K, const Epi& epi, size_t smem_min = 0) {
   SG_CHECK(M >= 1 && Ntot >= 1 && K >= 1, SINCGPU_EINVAL, "empty tensor-core contraction");
-  if (c.tc_pipe) return launch_tf32x3_ws<16, 3>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);
+  if (c.tc_pipe == 1) return launch_tf32x3_ws<16, 3>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);
+  if (c.tc_pipe == 2) return launch_tf32x3_ws<16, 4>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);
+  if (c.tc_pipe == 3) return launch_tf32x3_ws<8, 6>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);
   if (c.tc_kc == 32) return launch_tf32x3_kc<32>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);
   return launch_tf32x3_kc<16>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);
 }
