@@ -48,7 +48,7 @@ def test_gemm_tf32x3_matches_fp64(proj, m, n, k, mode):
     try:
         assert proj.gemm_tf32x3_dev(da, db, out) == 0
     finally:
-        set_mode(proj, "kc16")
+        set_mode(proj, "ring")
     assert proj.kernel_timeouts()[0] == 0
     got = out.cpu().numpy()
     assert np.isfinite(got).all()
