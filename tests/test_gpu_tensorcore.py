@@ -24,7 +24,8 @@ def proj(built_lib):
 
 MODES = {"kc16": {"tc_kc": 16, "tc_pipe": 0}, "kc32": {"tc_kc": 32, "tc_pipe": 0},
          "ring": {"tc_kc": 16, "tc_pipe": 1}, "ring4": {"tc_kc": 16, "tc_pipe": 2},
-         "ring8": {"tc_kc": 16, "tc_pipe": 3}}
+         "ring8": {"tc_kc": 16, "tc_pipe": 3}, "bulk": {"tc_kc": 16, "tc_pipe": 4},
+         "bulk5": {"tc_kc": 16, "tc_pipe": 5}}
 
 
 def set_mode(p, mode):
@@ -57,7 +58,7 @@ def test_gemm_tf32x3_matches_fp64(proj, m, n, k, mode):
     assert err < 5e-6, err
 
 
-@pytest.mark.parametrize("mode", ["kc16", "ring"])
+@pytest.mark.parametrize("mode", ["kc16", "ring", "bulk"])
 def test_reducedpot_tf32_contraction(built_lib, mode):
     import torch
     from oracle import sinc_oracle as orc

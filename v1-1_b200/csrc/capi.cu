@@ -83,7 +83,7 @@ int dupload(Ctx& c, void** dst, const void* src, size_t bytes) {
 
 void Ctx::bind_workspaces() {
   for (Workspace* w : {&ws_fft, &ws_pairs, &ws_gemm, &ws_twoe, &ws_rhs, &ws_io, &ws_red, &ws_conv, &ws_state, &ws_ci,
-                       &ws_ci2, &ws_kry, &ws_orb, &ws_tcerr, &cmf.ws})
+                       &ws_ci2, &ws_kry, &ws_orb, &ws_tcerr, &ws_tc, &cmf.ws})
     w->owner = &stream;
 }
 
@@ -110,6 +110,7 @@ Ctx::~Ctx() {
   ws_kry.release();
   ws_orb.release();
   ws_tcerr.release();
+  ws_tc.release();
   cmf.ws.release();
   for (IntCache& ic : icache) dfree(*this, ic.dev);
   if (rhs_exec) cudaGraphExecDestroy(rhs_exec);
@@ -386,8 +387,8 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
     return SINCGPU_OK;
   }
   if (!strcmp(name, "tc_pipe")) {
-    SG_CHECK(value >= 0 && value <= 3, SINCGPU_EINVAL, "tc_pipe must be 0 (two stages, no ring), 1 (ring of 3 x 16), "
-             "2 (4 x 16) or 3 (6 x 8)");
+    SG_CHECK(value >= 0 && value <= 5, SINCGPU_EINVAL, "tc_pipe must be 0 (two stages, no ring), 1 (ring of 3 x 16), "
+             "2 (4 x 16), 3 (6 x 8), 4 or 5 (pre-split operands, bulk copies into 3 or 5 stages)");
     h->c.tc_pipe = (int)value;
     return SINCGPU_OK;
   }

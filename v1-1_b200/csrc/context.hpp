@@ -180,6 +180,7 @@ struct Ctx {
   Workspace ws_kry;         // Krylov basis, Hessenberg, Pade output
   Workspace ws_orb;         // orbital Krylov basis and Jacobian state
   Workspace ws_tcerr;       // timeout flags: [0] tensor-core contractions, [1] TMA z pass
+  Workspace ws_tc;          // pre-split tf32 operand tiles of the bulk-copy tensor-core GEMM
   OrbPropState orb;
   CIState ci;
   CmfState cmf;
@@ -191,7 +192,8 @@ struct Ctx {
   int contract_tf32 = 0;  // 1: reducedpot contraction as 3xTF32 on the tensor cores
   int coul_tma = -1;      // TMA-staged persistent z pass: 1 on, 0 off, -1 automatic (off)
   int tc_pipe = 1;        // tcgen05 3xTF32 GEMM with a staging ring and an MMA-issuing warp: 1: 3 stages of
-                          // K = 16, 2: 4 x 16, 3: 6 x 8; 0: two stages, block barriers
+                          // K = 16, 2: 4 x 16, 3: 6 x 8; 4, 5: pre-split operands moved by bulk copies
+                          // into 3 or 5 stages; 0: two stages, block barriers
   int tc_kc = 16;         // K chunk of the tcgen05 3xTF32 GEMM: 16 or 32
   int ke_tf32 = 0;        // 1: kinetic contraction on the tcgen05 tensor cores, 3xTF32 (precision form)
   int coul_z2 = 0;        // z pass with P2 threads per line where P1 = 2 P2 (coul_z2_t): 1 on, 0 off

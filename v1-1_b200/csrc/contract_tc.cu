@@ -14,6 +14,7 @@
 // R x Gamma) when the context option contract_tf32 is set.
 #include <algorithm>
 #include "context.hpp"
+#include "tma.cuh"
 #include "umma.cuh"
 #include "../../include/sincgpu.h"
 
@@ -367,6 +368,171 @@ __global__ void __launch_bounds__(288) gemm_tf32x3_ws_kernel(const double* __res
   if (warp == 0) umma::tmem_dealloc(tmem, tmem_cols);
 }
 
+// Pre-split operands for the bulk-copy form: each K chunk of each 128-row tile of
+// A (and of each NT-column tile of B) is written once, split into tf32 hi and lo,
+// in the exact shared-memory layout of stage_tile (core matrices, K-major), hi
+// then lo, so that one 1-D bulk copy moves it.  Rows, columns and K beyond the
+// operand are zero.
+// A: block (mt, ch) at u32 offset (mt nch + ch) 2 * 128 KC.
+template <int KC>
+__global__ void __launch_bounds__(128) split_a_tiles_kernel(const double* __restrict__ A, ARows ar, long long M,
+                                                            int K, int nch, uint32_t* __restrict__ out) {
+  const long long mt = blockIdx.x;
+  const int ch = blockIdx.y, r = threadIdx.x;
+  const long long m = mt * 128 + r;
+  const long long rb = m < M ? ar.row(m) : 0;
+  double v[KC];
+#pragma unroll
+  for (int k = 0; k < KC; ++k) {
+    const int kk = ch * KC + k;
+    v[k] = (m < M && kk < K) ? A[rb + (long long)kk * ar.lak] : 0.0;
+  }
+  uint32_t* hi = out + (size_t)(mt * nch + ch) * 2 * 128 * KC;
+  uint32_t* lo = hi + 128 * KC;
+#pragma unroll
+  for (int c = 0; c < KC / 4; ++c) {
+    uint4 h, l;
+    umma::split_tf32(v[4 * c + 0], h.x, l.x);
+    umma::split_tf32(v[4 * c + 1], h.y, l.y);
+    umma::split_tf32(v[4 * c + 2], h.z, l.z);
+    umma::split_tf32(v[4 * c + 3], h.w, l.w);
+    *reinterpret_cast<uint4*>(hi + (c * 128 + r) * 4) = h;
+    *reinterpret_cast<uint4*>(lo + (c * 128 + r) * 4) = l;
+  }
+}
+
+// B: block (nt, ch) at u32 offset (nt nch + ch) 2 NT KC; element (column n, k) =
+// B[n lbn + k lbk].
+template <int KC>
+__global__ void split_b_tiles_kernel(const double* __restrict__ B, long long lbn, long long lbk, int Ntot, int K,
+                                     int NT, int nch, uint32_t* __restrict__ out) {
+  const int nt = blockIdx.x, ch = blockIdx.y;
+  uint32_t* hi = out + (size_t)(nt * nch + ch) * 2 * NT * KC;
+  uint32_t* lo = hi + NT * KC;
+  for (int idx = threadIdx.x; idx < (KC / 4) * NT; idx += blockDim.x) {
+    const int c = idx / NT, r = idx - c * NT;
+    const int n = nt * NT + r;
+    double v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = ch * KC + 4 * c + j;
+      v[j] = (n < Ntot && k < K) ? B[(long long)n * lbn + (long long)k * lbk] : 0.0;
+    }
+    uint4 h, l;
+    umma::split_tf32(v[0], h.x, l.x);
+    umma::split_tf32(v[1], h.y, l.y);
+    umma::split_tf32(v[2], h.z, l.z);
+    umma::split_tf32(v[3], h.w, l.w);
+    *reinterpret_cast<uint4*>(hi + (c * NT + r) * 4) = h;
+    *reinterpret_cast<uint4*>(lo + (c * NT + r) * 4) = l;
+  }
+}
+
+// The bulk-copy form: one thread moves each K chunk of the pre-split A and B tiles
+// into a ring of ST stages with two 1-D bulk copies (announced on the stage's
+// `full` mbarrier with their byte count), another issues the MMAs and commits them
+// to the stage's `empty` mbarrier; four warps read the accumulator back.  Every
+// wait is bounded; on a timeout the CTA records it in *err, waits (bounded) for
+// the copies it issued, frees its tensor memory and returns.
+template <int KC, int ST, class Epi>
+__global__ void __launch_bounds__(128) gemm_tf32x3_bulk_kernel(const uint32_t* __restrict__ As,
+                                                               const uint32_t* __restrict__ Bs, long long M, int Ntot,
+                                                               int nch, int NT, uint32_t tmem_cols, Epi epi,
+                                                               int* __restrict__ err) {
+  extern __shared__ __align__(128) uint32_t tsm[];
+  __shared__ __align__(8) uint64_t full[ST], empty[ST], done;
+  __shared__ uint32_t tmem_base;
+  __shared__ int fail;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const long long mt = blockIdx.x;
+  const int nt = blockIdx.y;
+  const uint32_t a_bytes = 2u * 128u * KC * 4u, b_bytes = 2u * (uint32_t)NT * KC * 4u;
+  const size_t stage_u32 = (a_bytes + b_bytes) / 4;
+  if (warp == 0) umma::tmem_alloc(&tmem_base, tmem_cols);
+  if (tid == 0) {
+    for (int s = 0; s < ST; ++s) {
+      umma::mbar_init(&full[s], 1);
+      umma::mbar_init(&empty[s], 1);
+    }
+    umma::mbar_init(&done, 1);
+    fail = 0;
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  int issued = 0;  // chunks whose copies the producer issued
+  if (tid == 0) {
+    // producer
+    for (int ch = 0; ch < nch; ++ch) {
+      const int s = ch % ST;
+      if (ch >= ST && !umma::mbar_wait(&empty[s], ((ch / ST) - 1) & 1, kWaitLimit)) {
+        atomicExch(&fail, 1);
+        break;
+      }
+      if (fail) break;
+      uint32_t* dst = tsm + (size_t)s * stage_u32;
+      tma::mbar_arrive_expect_tx(&full[s], a_bytes + b_bytes);
+      tma::load_1d(dst, As + (size_t)(mt * nch + ch) * (a_bytes / 4), a_bytes, &full[s]);
+      tma::load_1d(dst + a_bytes / 4, Bs + (size_t)(nt * nch + ch) * (b_bytes / 4), b_bytes, &full[s]);
+      issued = ch + 1;
+    }
+  } else if (tid == 32) {
+    // MMA issue
+    const uint32_t idesc = umma::idesc_tf32(128, NT);
+    for (int ch = 0; ch < nch; ++ch) {
+      const int s = ch % ST;
+      if (!umma::mbar_wait(&full[s], (ch / ST) & 1, kWaitLimit)) {
+        atomicExch(&fail, 1);
+        break;
+      }
+      umma::fence_after_sync();
+      const uint32_t a_hi = umma::smem_u32(tsm + (size_t)s * stage_u32);
+      const uint32_t a_lo = a_hi + 4u * 128u * KC;
+      const uint32_t b_hi = a_hi + a_bytes;
+      const uint32_t b_lo = b_hi + 4u * (uint32_t)NT * KC;
+#pragma unroll
+      for (int ks = 0; ks < KC / 8; ++ks) {
+        const uint32_t ao = ks * 2 * 128 * 16, bo = ks * 2 * NT * 16;
+        const uint64_t ah = umma::desc_kmajor(a_hi + ao, 128 * 16, 128);
+        const uint64_t al = umma::desc_kmajor(a_lo + ao, 128 * 16, 128);
+        const uint64_t bh = umma::desc_kmajor(b_hi + bo, NT * 16, 128);
+        const uint64_t bl = umma::desc_kmajor(b_lo + bo, NT * 16, 128);
+        umma::mma_tf32(tmem, ah, bh, idesc, ch > 0 || ks > 0);
+        umma::mma_tf32(tmem, ah, bl, idesc, true);
+        umma::mma_tf32(tmem, al, bh, idesc, true);
+      }
+      umma::commit(&empty[s]);
+    }
+    umma::commit(&done);
+  }
+  bool ok = umma::mbar_wait(&done, 0, kWaitLimit);
+  __syncthreads();
+  ok = ok && !fail;
+  if (!ok) {
+    if (tid == 0) {
+      atomicExch(err, 1);
+      // the copies of the last ST issued chunks may still be landing: wait for them
+      for (int ch = issued > ST ? issued - ST : 0; ch < issued; ++ch)
+        umma::mbar_wait(&full[ch % ST], (ch / ST) & 1, kWaitLimit);
+    }
+    __syncthreads();
+  }
+  umma::fence_after_sync();
+  if (ok) {
+    const long long m = mt * 128 + 32 * warp + lane;
+    for (int c0 = 0; c0 < NT; c0 += 8) {
+      float v[8];
+      umma::tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+      umma::tmem_ld_wait();
+      apply_epi(epi, m, M, nt * NT + c0, Ntot, v);
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, tmem_cols);
+}
+
 constexpr int kSmemDyn = 224 * 1024;  // dynamic limit (the static mbarriers take the rest of 227 KB)
 
 template <int KC, class Epi>
@@ -409,6 +575,37 @@ int launch_tf32x3_ws(Ctx& c, const double* A, ARows ar, long long M, const doubl
   return SINCGPU_OK;
 }
 
+// Bulk-copy form: pre-split A and B (workspace ws_tc), then the ring kernel.
+template <int KC, int ST, class Epi>
+int launch_tf32x3_bulk(Ctx& c, const double* A, ARows ar, long long M, const double* B, long long lbn,
+                       long long lbk, int Ntot, int K, const Epi& epi) {
+  const int ntile = ceil_div(Ntot, 256);
+  const int NT = ceil_div(ceil_div(Ntot, ntile), 16) * 16;
+  const uint32_t cols = NT <= 32 ? 32 : NT <= 64 ? 64 : NT <= 128 ? 128 : 256;
+  const int nch = ceil_div(K, KC);
+  const long long mtiles = (M + 127) / 128;
+  const size_t a_u32 = (size_t)mtiles * nch * 2 * 128 * KC, b_u32 = (size_t)ntile * nch * 2 * NT * KC;
+  SG_TRY(c.ws_tc.ensure(sizeof(uint32_t) * (a_u32 + b_u32)));
+  uint32_t* As = (uint32_t*)c.ws_tc.ptr;
+  uint32_t* Bs = As + a_u32;
+  SG_CHECK(mtiles < (1LL << 31), SINCGPU_ERANGE, "too many row tiles");
+  split_a_tiles_kernel<KC><<<dim3((unsigned)mtiles, nch), 128, 0, c.stream>>>(A, ar, M, K, nch, As);
+  SG_LAUNCHED();
+  split_b_tiles_kernel<KC><<<dim3(ntile, nch), 256, 0, c.stream>>>(B, lbn, lbk, Ntot, K, NT, nch, Bs);
+  SG_LAUNCHED();
+  const size_t smem = (size_t)ST * (2 * 128 * KC + 2 * NT * KC) * sizeof(uint32_t);
+  SG_CHECK(smem <= (size_t)kSmemDyn, SINCGPU_ERANGE, "tensor-core stages need %zu bytes of shared memory", smem);
+  static const cudaError_t attr = cudaFuncSetAttribute(gemm_tf32x3_bulk_kernel<KC, ST, Epi>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDyn);
+  SG_CUDA(attr);
+  int* err = nullptr;
+  SG_TRY(timeout_flags(c, &err));
+  gemm_tf32x3_bulk_kernel<KC, ST, Epi><<<dim3((unsigned)mtiles, ntile), 128, smem, c.stream>>>(
+      As, Bs, M, Ntot, nch, NT, cols, epi, err);
+  SG_LAUNCHED();
+  return SINCGPU_OK;
+}
+
 // smem_min: dynamic shared memory to reserve at least (the self test reserves
 // more than its tiles need, so that every descriptor address stays inside the
 // CTA's allocation).  K chunks of 16 (two CTAs per SM) or, with the context
@@ -417,6 +614,8 @@ template <class Epi>
 int launch_tf32x3(Ctx& c, const double* A, ARows ar, long long M, const double* B, long long lbn, long long lbk,
                   int Ntot, int K, const Epi& epi, size_t smem_min = 0) {
   SG_CHECK(M >= 1 && Ntot >= 1 && K >= 1, SINCGPU_EINVAL, "empty tensor-core contraction");
+  if (c.tc_pipe == 4) return launch_tf32x3_bulk<16, 3>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi);
+  if (c.tc_pipe == 5) return launch_tf32x3_bulk<16, 5>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi);
   if (c.tc_pipe == 1) return launch_tf32x3_ws<16, 3>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);
   if (c.tc_pipe == 2) return launch_tf32x3_ws<16, 4>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);
   if (c.tc_pipe == 3) return launch_tf32x3_ws<8, 6>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi, smem_min);

@@ -50,6 +50,16 @@ __device__ __forceinline__ void load_3d(void* dst, const CUtensorMap* map, int x
       : "memory");
 }
 
+// 1-D bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from
+// global to shared memory, completed on `mbar` with a transaction count.
+__device__ __forceinline__ void load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(mbar))
+      : "memory");
+}
+
 // generic-proxy accesses to shared memory are ordered before later async-proxy ones
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
