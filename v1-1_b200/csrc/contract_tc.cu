@@ -584,6 +584,10 @@ int launch_tf32x3_bulk(Ctx& c, const double* A, ARows ar, long long M, const dou
   const uint32_t cols = NT <= 32 ? 32 : NT <= 64 ? 64 : NT <= 128 ? 128 : 256;
   const int nch = ceil_div(K, KC);
   const long long mtiles = (M + 127) / 128;
+  if constexpr (ST > 3) {  // wide tiles: fewer stages where ST of them do not fit
+    if ((size_t)ST * (2 * 128 * KC + 2 * NT * KC) * sizeof(uint32_t) > (size_t)kSmemDyn)
+      return launch_tf32x3_bulk<KC, 3>(c, A, ar, M, B, lbn, lbk, Ntot, K, epi);
+  }
   const size_t a_u32 = (size_t)mtiles * nch * 2 * 128 * KC, b_u32 = (size_t)ntile * nch * 2 * NT * KC;
   SG_TRY(c.ws_tc.ensure(sizeof(uint32_t) * (a_u32 + b_u32)));
   uint32_t* As = (uint32_t*)c.ws_tc.ptr;
