@@ -49,7 +49,7 @@ def test_gemm_tf32x3_matches_fp64(proj, m, n, k, mode):
     try:
         assert proj.gemm_tf32x3_dev(da, db, out) == 0
     finally:
-        set_mode(proj, "ring")
+        set_mode(proj, "bulk")
     assert proj.kernel_timeouts()[0] == 0
     got = out.cpu().numpy()
     assert np.isfinite(got).all()

@@ -191,7 +191,7 @@ struct Ctx {
   int coul_fp32 = 0;    // 1: Coulomb passes in FP32 (precision form), 0: FP64
   int contract_tf32 = 0;  // 1: reducedpot contraction as 3xTF32 on the tensor cores
   int coul_tma = -1;      // TMA-staged persistent z pass: 1 on, 0 off, -1 automatic (off)
-  int tc_pipe = 1;        // tcgen05 3xTF32 GEMM with a staging ring and an MMA-issuing warp: 1: 3 stages of
+  int tc_pipe = 4;        // tcgen05 3xTF32 GEMM with a staging ring and an MMA-issuing warp: 1: 3 stages of
                           // K = 16, 2: 4 x 16, 3: 6 x 8; 4, 5: pre-split operands moved by bulk copies
                           // into 3 or 5 stages; 0: two stages, block barriers
   int tc_kc = 16;         // K chunk of the tcgen05 3xTF32 GEMM: 16 or 32
