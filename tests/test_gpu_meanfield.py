@@ -88,14 +88,16 @@ def test_call_twoe_matel00_general(he):
     assert relerr(mat, mat_ref) < TOL
 
 
-@pytest.mark.parametrize("nspf,general", [(12, False), (9, True)])
-def test_call_twoe_matel00_multitile(built_lib, nspf, general):
-    """Pair lists longer than one GEMM tile (2U = 156 hermitian, 2n^2 = 162 general):
-    only the upper-triangle tiles of the symmetric pair matrix are computed and the
-    lower ones mirrored."""
+@pytest.mark.parametrize("nspf,general,symdiag", [(12, False, 0), (12, False, 1), (16, False, 1), (9, True, 1)])
+def test_call_twoe_matel00_multitile(built_lib, nspf, general, symdiag):
+    """Pair lists longer than one GEMM tile (2U = 156 and 272 hermitian, 2n^2 = 162
+    general): only the upper-triangle tiles of the symmetric pair matrix are
+    computed and the lower ones mirrored; with twoe_symdiag the diagonal tiles
+    compute their lower 8 x 8 blocks only (hermitian pairs)."""
     from sincgpu import SincProject
     sysm = orc.SincSystem(21, 0.4, [[0, 0, 0]], [2.0])
     gpu = SincProject(21, 0.4, [[0, 0, 0]], [2.0], nspf)
+    gpu.set_option("twoe_symdiag", symdiag)
     try:
         phi = orc.seeded_orbitals(sysm, nspf, seed=21)
         phi2 = orc.seeded_orbitals(sysm, nspf, seed=22) if general else phi

@@ -337,7 +337,7 @@ int sincgpu_get_option(sincgpu_ctx* h, const char* name, long long* value) {
   } opts[] = {{"coul_chunk", c.coul_chunk},       {"coulomb_fp32", c.coul_fp32}, {"contract_tf32", c.contract_tf32},
               {"coul_tma", c.coul_tma},           {"twoe_tile", c.twoe_tile},    {"orth_fused", c.orth_fused},
               {"rhs_overlap", c.rhs_overlap},     {"coul_fused", c.coul_fused},  {"coul_z2", c.coul_z2},
-              {"cmf_fp64_last", c.cmf.fp64_last ? 1 : 0}, {"ke_tf32", c.ke_tf32}, {"tc_kc", c.tc_kc}, {"tc_pipe", c.tc_pipe}, {"twoe_dmma", c.twoe_dmma}, {"rp_dmma", c.rp_dmma}};
+              {"cmf_fp64_last", c.cmf.fp64_last ? 1 : 0}, {"ke_tf32", c.ke_tf32}, {"tc_kc", c.tc_kc}, {"tc_pipe", c.tc_pipe}, {"twoe_symdiag", c.twoe_symdiag}, {"twoe_dmma", c.twoe_dmma}, {"rp_dmma", c.rp_dmma}};
   for (const auto& o : opts)
     if (!strcmp(name, o.n)) {
       *value = o.v;
@@ -384,6 +384,11 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
   if (!strcmp(name, "rp_dmma")) {
     SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "rp_dmma must be 0 or 1");
     h->c.rp_dmma = (int)value;
+    return SINCGPU_OK;
+  }
+  if (!strcmp(name, "twoe_symdiag")) {
+    SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "twoe_symdiag must be 0 or 1");
+    h->c.twoe_symdiag = (int)value;
     return SINCGPU_OK;
   }
   if (!strcmp(name, "tc_pipe")) {

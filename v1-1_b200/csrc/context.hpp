@@ -200,6 +200,7 @@ struct Ctx {
   int coul_fused = 0;     // three-pass Coulomb form (y, z, inverse y per plane on chip): 1 on where it fits, 0 off, -1 automatic
   int rp_dmma = 1;        // 1: FP64 reducedpot GEMM on the FP64 tensor cores (DMMA), 0: DFMA tiles
   int twoe_dmma = 1;      // 1: FP64 twoematel GEMM on the FP64 tensor cores (DMMA), 0: DFMA tiles
+  int twoe_symdiag = 0;   // 1: multi-tile twoematel computes its diagonal tiles' lower blocks only
   int twoe_tile = 0;      // twoematel tile edge 16R: 0 = least padding, 2..9 = that R
   int orth_fused = 1;     // 1: an orbital Arnoldi step's orthogonalisation in one cooperative launch
   int rhs_overlap = 1;    // 1: the fused orbital-RHS entry runs its CI part and the mix + kinetic

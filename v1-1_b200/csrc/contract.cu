@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(64 * R, 1) twoe_dmma_kernel(const double2* __r
                                                               const int* __restrict__ pa, const int* __restrict__ pb,
                                                               const double* __restrict__ Rpl, int npair, int nspf,
                                                               long long G, int ntn, long long xper,
-                                                              double* __restrict__ part) {
+                                                              double* __restrict__ part, int strict) {
   constexpr int TT = 16 * R;
   constexpr int TS = KT + 4;  // shared-memory row stride (doubles), 4 mod 16
   constexpr int NTH = 64 * R;
@@ -252,12 +252,19 @@ __global__ void __launch_bounds__(64 * R, 1) twoe_dmma_kernel(const double2* __r
   int* sb = sa + TT;
   int* sc = sb + TT;
   const int M = 2 * npair;
-  int tm = 0, rem = blockIdx.x;
-  while (rem >= ntn - tm) {
-    rem -= ntn - tm;
-    ++tm;
+  // tile (tm, tn): SYM CTAs take the diagonal tiles (blockIdx.x = tm = tn); the
+  // others the upper-triangle tiles, the diagonal included unless `strict`
+  int tm = 0, tn = 0;
+  if constexpr (SYM) {
+    tm = tn = blockIdx.x;
+  } else {
+    int rem = blockIdx.x;
+    while (rem >= ntn - tm - strict) {
+      rem -= ntn - tm - strict;
+      ++tm;
+    }
+    tn = tm + strict + rem;
   }
-  const int tn = tm + rem;
   const int m0 = tm * TT, n0 = tn * TT;
   const long long xb = blockIdx.y * xper;
   const long long xe = min(G, xb + xper);
@@ -478,13 +485,13 @@ constexpr int kTwoeSmemMax = 227 * 1024;
 template <int RR, bool SYM, int KT>
 static int launch_twoe_pipe_t(Ctx& c, dim3 grid, size_t bytes, const double2* phi1, const double2* phi2,
                               const int* d_pa, const int* d_pb, const double* Rpl, int npair, int ntn,
-                              long long xper, double* part) {
+                              long long xper, double* part, int strict) {
   // process-wide attribute, one fixed value (thread-safe static initialisation)
   static const cudaError_t attr = cudaFuncSetAttribute(twoe_dmma_kernel<RR, SYM, KT>,
                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, kTwoeSmemMax);
   SG_CUDA(attr);
   twoe_dmma_kernel<RR, SYM, KT><<<grid, 64 * RR, bytes, c.stream>>>(phi1, phi2, d_pa, d_pb, Rpl, npair, c.nspf,
-                                                                     c.G, ntn, xper, part);
+                                                                     c.G, ntn, xper, part, strict);
   return SINCGPU_OK;
 }
 
@@ -493,14 +500,17 @@ static int launch_twoe_pipe_t(Ctx& c, dim3 grid, size_t bytes, const double2* ph
 template <int RR>
 static int launch_twoe_pipe(Ctx& c, dim3 grid, bool sym, const double2* phi1, const double2* phi2,
                             const int* d_pa, const int* d_pb, const double* Rpl, int npair, int ntn,
-                            long long xper, double* part) {
+                            long long xper, double* part, int strict = 0) {
   const size_t b32 = twoe_pipe_smem(RR, 32, c.nspf), b16 = twoe_pipe_smem(RR, 16, c.nspf);
   if (b32 <= (size_t)kTwoeSmemMax)
-    return sym ? launch_twoe_pipe_t<RR, true, 32>(c, grid, b32, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper, part)
+    return sym ? launch_twoe_pipe_t<RR, true, 32>(c, grid, b32, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper, part,
+                                                  0)
                : launch_twoe_pipe_t<RR, false, 32>(c, grid, b32, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper,
-                                                   part);
-  return sym ? launch_twoe_pipe_t<RR, true, 16>(c, grid, b16, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper, part)
-             : launch_twoe_pipe_t<RR, false, 16>(c, grid, b16, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper, part);
+                                                   part, strict);
+  return sym ? launch_twoe_pipe_t<RR, true, 16>(c, grid, b16, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper, part,
+                                                0)
+             : launch_twoe_pipe_t<RR, false, 16>(c, grid, b16, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper, part,
+                                                 strict);
 }
 
 static void pair_lut(int n, const int* pa, const int* pb, int npair, bool herm, std::vector<int>& lut) {
@@ -553,10 +563,18 @@ int twoe_matel(Ctx& c, const double2* phi1, const double2* phi2, const int* h_pa
     const dim3 grid(ntiles, nsplit);
     // the pipelined kernel copies whole complex values (16 bytes)
     const bool pipe = ((uintptr_t)phi1 % 16 == 0) && ((uintptr_t)phi2 % 16 == 0);
-    // one symmetric tile (hermitian pairs): the blocks below its diagonal only
-    sym = pipe && herm && c.twoe_dmma && ntm == 1;
+    // hermitian pairs make the pair matrix symmetric: a diagonal tile needs only
+    // its blocks on and below the diagonal (the SYM kernel); with several tiles
+    // (option twoe_symdiag) the diagonal tiles take that kernel and the strictly
+    // upper ones the full one
+    sym = pipe && herm && c.twoe_dmma && (ntm == 1 || c.twoe_symdiag);
 #define SG_TWOE_LAUNCH(RR, DM)                                                                             \
-  if (DM && pipe) {                                                                                        \
+  if (DM && pipe && sym && ntm > 1) {                                                                      \
+    SG_TRY(launch_twoe_pipe<RR>(c, dim3(ntm, nsplit), true, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper,  \
+                                part));                                                                    \
+    SG_TRY(launch_twoe_pipe<RR>(c, dim3(ntm * (ntm - 1) / 2, nsplit), false, phi1, phi2, d_pa, d_pb, Rpl,   \
+                                npair, ntn, xper, part, 1));                                               \
+  } else if (DM && pipe) {                                                                                 \
     SG_TRY(launch_twoe_pipe<RR>(c, grid, sym, phi1, phi2, d_pa, d_pb, Rpl, npair, ntn, xper, part));        \
   } else {                                                                                                 \
     static const cudaError_t attr = cudaFuncSetAttribute(                                                  \
