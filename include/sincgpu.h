@@ -94,7 +94,11 @@ int sincgpu_fft_length(sincgpu_ctx* ctx);
  * in FP64, so that the energy, the dipole and the next step start from FP64
  * matrices); "ke_tf32" (1: the per-axis kinetic contraction on the tcgen05
  * tensor cores, one 3xTF32 GEMM per axis with FP32 accumulation, the precision
- * form; 0: FP64 tensor cores). */
+ * form; 0: FP64 tensor cores); "rhs_upload_groups" (1..8, default 4: the
+ * host-array orbital-RHS entry copies the orbitals up in that many groups on
+ * a copy stream, and the Coulomb pair loop starts on the pairs of the first
+ * group while the others are in flight; 1: one copy before the evaluation;
+ * bitwise the same). */
 int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
 /* Current value of an option of sincgpu_set_option (SINCGPU_EINVAL for an unknown name). */
 int sincgpu_get_option(sincgpu_ctx* ctx, const char* name, long long* value);
@@ -379,7 +383,11 @@ int sincgpu_orbital_rhs_avec_dev(sincgpu_ctx* ctx, const double* phi, const doub
 
 /* Host-array form: orbitals and A-vector in, orbital RHS out; the mean fields stay
  * on the device.  This is the call a Fortran driver makes per RHS evaluation when
- * it keeps the GPU state between calls. */
+ * it keeps the GPU state between calls.  The copies overlap the evaluation: the
+ * A-vector goes up first (the RDMs start on it), the orbitals in groups (option
+ * "rhs_upload_groups") under the Coulomb pair loop, and the RHS comes down while
+ * twoematel, formed after it, runs; page-locked host buffers let the copies run
+ * asynchronously.  Returns when the RHS is in outspfs. */
 int sincgpu_orbital_rhs_avec(sincgpu_ctx* ctx, const double* phi, const double* avector,
                              double timefac_re, double timefac_im, double ztdpot, double* outspfs);
 
@@ -509,7 +517,12 @@ int sincgpu_cmf_state_dev(sincgpu_ctx* ctx, double* phi, double* avector);
  * and walk tables on the device in its own context and stream until it finishes,
  * so requests arriving while others run join as slots and memory free up and
  * their work overlaps on the device.  Results are deterministic: a request gives
- * the same numbers alone or in a mix. */
+ * the same numbers alone or in a mix.  The server reserves its HBM budget in the
+ * device's stream-ordered memory pool when it is created (the requests' device
+ * allocations come out of that reservation, so that none of them waits in the
+ * driver for new memory while other requests run) and gives it back when it is
+ * destroyed.  A request whose tensor-core contraction or staged Coulomb pass gave
+ * up a bounded wait fails with SINCGPU_ETIMEOUT. */
 typedef struct sincgpu_request {
   int numpoints;
   double spacing;

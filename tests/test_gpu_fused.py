@@ -91,7 +91,8 @@ def test_orbital_rhs_avec_overlap_is_bitwise(li):
 def test_scheduling_options_reject_bad_values(li):
     from sincgpu import SincGpuError
     gpu = li[1]
-    for name, bad in (("rhs_overlap", 2), ("orth_fused", -1), ("twoe_tile", 1), ("twoe_tile", 10)):
+    for name, bad in (("rhs_overlap", 2), ("orth_fused", -1), ("twoe_tile", 1), ("twoe_tile", 10),
+                      ("rhs_upload_groups", 0), ("rhs_upload_groups", 9)):
         with pytest.raises(SincGpuError):
             gpu.set_option(name, bad)
     gpu.set_option("rhs_overlap", 1)

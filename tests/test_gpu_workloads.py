@@ -97,6 +97,25 @@ def test_workload_b_host_entry(wb):
     assert relerr(proj.orbital_rhs_avec(phi, a), ref["rhs"]) < TOL
 
 
+def test_workload_b_host_entry_upload_groups(wb):
+    """The host-array entry copies the orbitals up in groups and starts the
+    Coulomb pairs of the first group while the rest is in flight, and copies the
+    RHS down while it forms twoematel: the same bits as the device entry for any
+    group count (1 = one copy before the evaluation)."""
+    w, proj, walks, phi, a, ref, _ = wb
+    dev = _run_avec_dev(w, proj, walks, phi, a)["rhs"]
+    assert proj.get_option("rhs_upload_groups") == 4
+    try:
+        for g in (1, 3, 4, 8):
+            proj.set_option("rhs_upload_groups", g)
+            assert np.array_equal(proj.orbital_rhs_avec(phi, a), dev), g
+        proj.set_option("rhs_overlap", 0)
+        assert np.array_equal(proj.orbital_rhs_avec(phi, a), dev)
+    finally:
+        proj.set_option("rhs_overlap", 1)
+        proj.set_option("rhs_upload_groups", 4)
+
+
 def test_workload_b_one_stream_same_bits(wb):
     """rhs_overlap = 0 (the order the per-stage profile uses) gives the same bits."""
     w, proj, walks, phi, a, ref, _ = wb
@@ -171,6 +190,13 @@ def test_workload_c_reducedpot_and_rhs(wc):
     assert np.abs(rhs[pts] - gold["rhs_pts"]).max() < TOL * gold["rhs_absmax"]
     assert (np.abs(W.T @ rp - gold["reducedpot_proj"]) / (bound * gold["reducedpot_absmax"])).max() < TOL
     assert (np.abs(W.T @ rhs - gold["rhs_proj"]) / (bound * gold["rhs_absmax"])).max() < TOL
+
+
+def test_workload_c_host_entry(wc):
+    """The end-to-end call at 81^3 (orbitals up in four groups under the Coulomb
+    pair loop, the RHS down under twoematel): the device entry's bits."""
+    w, proj, walks, phi, a, gold, got = wc
+    assert np.array_equal(proj.orbital_rhs_avec(phi, a), got["rhs"])
 
 
 def test_workload_c_reduced_potentials(wc):

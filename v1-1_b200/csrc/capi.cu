@@ -2,6 +2,7 @@
 #include <atomic>
 #include <cstdarg>
 #include <cstring>
+#include <mutex>
 #include <algorithm>
 #include <vector>
 #include <string>
@@ -55,6 +56,30 @@ void Workspace::release() {
   }
   ptr = nullptr;
   bytes = 0;
+}
+
+namespace {
+std::mutex g_pin_mu;
+std::vector<std::pair<size_t, void*>> g_pin_free;
+}  // namespace
+
+int pinned_get(size_t bytes, void** p) {
+  {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    for (auto it = g_pin_free.begin(); it != g_pin_free.end(); ++it)
+      if (it->first == bytes) {
+        *p = it->second;
+        g_pin_free.erase(it);
+        return SINCGPU_OK;
+      }
+  }
+  SG_CUDA(cudaMallocHost(p, bytes));
+  return SINCGPU_OK;
+}
+
+void pinned_put(size_t bytes, void* p) {
+  std::lock_guard<std::mutex> lk(g_pin_mu);
+  g_pin_free.emplace_back(bytes, p);
 }
 
 int dalloc(Ctx& c, void** p, size_t bytes) {
@@ -117,9 +142,12 @@ Ctx::~Ctx() {
   if (rhs_graph) cudaGraphDestroy(rhs_graph);
   ci.release(stream);
   if (side) cudaStreamDestroy(side);
-  if (orb_state_h) cudaFreeHost(orb_state_h);
-  for (cudaEvent_t e : {ev_fork, ev_ci, ev_join, ev_coul, ev_twoe, ev_avec, ev_orb_state})
+  if (orb_state_h) pinned_put(orb_state_bytes, orb_state_h);
+  for (cudaEvent_t e : {ev_fork, ev_ci, ev_join, ev_coul, ev_twoe, ev_rhs, ev_avec, ev_orb_state, ev_entry})
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : ev_up)
+    if (e) cudaEventDestroy(e);
+  if (copy) cudaStreamDestroy(copy);
   if (stream && own_stream) cudaStreamDestroy(stream);
 }
 
@@ -187,18 +215,27 @@ int side_stream(Ctx& c) {
   SG_CUDA(cudaGetDevice(&cur));
   if (cur != c.device) SG_CUDA(cudaSetDevice(c.device));
   cudaError_t e = cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking);
-  for (cudaEvent_t* ev : {&c.ev_fork, &c.ev_ci, &c.ev_join, &c.ev_coul, &c.ev_twoe, &c.ev_avec})
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c.copy, cudaStreamNonBlocking);
+  for (cudaEvent_t* ev : {&c.ev_fork, &c.ev_ci, &c.ev_join, &c.ev_coul, &c.ev_twoe, &c.ev_rhs, &c.ev_avec,
+                          &c.ev_entry})
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+  for (cudaEvent_t& ev : c.ev_up)
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
   if (cur != c.device) cudaSetDevice(cur);
   SG_CUDA(e);
   return SINCGPU_OK;
 }
 
 int mean_field(Ctx& c, const double2* phi, const double2* tally, double2* twoematel, double2* reducedpot,
-               bool tally_herm, cudaEvent_t tally_ready, cudaStream_t side, RpApply* apply) {
+               bool tally_herm, cudaEvent_t tally_ready, cudaStream_t side, RpApply* apply, TwoeDefer* defer) {
   std::vector<int> pa, pb;
   bool herm;
-  if (side && twoematel) {
+  if (defer && !twoematel) {
+    SG_TRY(twoe_core(c, phi, phi, nullptr, nullptr, pa, pb, herm));
+    defer->pa = pa;
+    defer->pb = pb;
+    defer->herm = herm;
+  } else if (side && twoematel) {
     // twoematel feeds nothing below, so it runs on `side` beside reducedpot and the
     // apply; the pair tables both read are uploaded here first (on this stream)
     SG_TRY(twoe_core(c, phi, phi, nullptr, nullptr, pa, pb, herm));
@@ -223,6 +260,18 @@ int mean_field(Ctx& c, const double2* phi, const double2* tally, double2* twoema
   if (tally_ready) SG_CUDA(cudaStreamWaitEvent(c.stream, tally_ready, 0));
   return reduced_pot(c, (const double*)c.ws_red.ptr, pa.data(), pb.data(), (int)pa.size(), herm, tally,
                      reducedpot, tally_herm, apply);
+}
+
+int twoe_deferred(Ctx& c, const double2* phi, const TwoeDefer& defer, double2* twoematel, cudaEvent_t after,
+                  cudaStream_t side) {
+  SG_CUDA(cudaStreamWaitEvent(side, after, 0));
+  const cudaStream_t main_stream = c.stream;
+  c.stream = side;
+  const int rc = twoe_matel(c, phi, phi, defer.pa.data(), defer.pb.data(), (int)defer.pa.size(),
+                            (const double*)c.ws_red.ptr, defer.herm, twoematel);
+  c.stream = main_stream;
+  SG_CUDA(cudaEventRecord(c.ev_twoe, side));
+  return rc;
 }
 
 int orbital_rhs(Ctx& c, const double2* phi, const double2* tally, const double2* denmat, const double2* invdenmat,
@@ -337,7 +386,7 @@ int sincgpu_get_option(sincgpu_ctx* h, const char* name, long long* value) {
   } opts[] = {{"coul_chunk", c.coul_chunk},       {"coulomb_fp32", c.coul_fp32}, {"contract_tf32", c.contract_tf32},
               {"coul_tma", c.coul_tma},           {"twoe_tile", c.twoe_tile},    {"orth_fused", c.orth_fused},
               {"rhs_overlap", c.rhs_overlap},     {"coul_fused", c.coul_fused},  {"coul_z2", c.coul_z2},
-              {"cmf_fp64_last", c.cmf.fp64_last ? 1 : 0}, {"ke_tf32", c.ke_tf32}, {"tc_kc", c.tc_kc}, {"tc_pipe", c.tc_pipe}, {"twoe_symdiag", c.twoe_symdiag}, {"twoe_dmma", c.twoe_dmma}, {"rp_dmma", c.rp_dmma}};
+              {"cmf_fp64_last", c.cmf.fp64_last ? 1 : 0}, {"rhs_upload_groups", c.up_groups}, {"ke_tf32", c.ke_tf32}, {"tc_kc", c.tc_kc}, {"tc_pipe", c.tc_pipe}, {"twoe_symdiag", c.twoe_symdiag}, {"twoe_dmma", c.twoe_dmma}, {"rp_dmma", c.rp_dmma}};
   for (const auto& o : opts)
     if (!strcmp(name, o.n)) {
       *value = o.v;
@@ -364,6 +413,12 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
   if (!strcmp(name, "rhs_overlap")) {
     SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "rhs_overlap must be 0 or 1");
     h->c.rhs_overlap = (int)value;
+    return SINCGPU_OK;
+  }
+  if (!strcmp(name, "rhs_upload_groups")) {
+    SG_CHECK(value >= 1 && value <= Ctx::kUpGroups, SINCGPU_EINVAL, "rhs_upload_groups must be 1..%d",
+             Ctx::kUpGroups);
+    h->c.up_groups = (int)value;
     return SINCGPU_OK;
   }
   if (!strcmp(name, "orth_fused")) {

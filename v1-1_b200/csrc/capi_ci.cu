@@ -208,22 +208,28 @@ int sincgpu_sparseconfigmult_dev(sincgpu_ctx* h, const double* in, double* out, 
 namespace {
 // avec_ready (or nullptr): the A-vector reached the device before the orbitals (the
 // host-array entry), so the side stream's RDMs start on it while the orbitals are
-// still being copied; the mix and kinetic contraction wait for the orbitals
+// still being copied; the mix and kinetic contraction wait for the orbitals.
+// host_out (or nullptr): the host-array entry's RHS buffer; the RHS is copied there
+// as soon as it is final, and twoematel, which that entry does not return, is formed
+// on the side stream while the copy runs
 int orbital_rhs_avec_impl(sincgpu_ctx* h, const double* phi, const double* avector, double tre, double tim,
                           double ztdpot, double* denmat, double* invdenmat, double* tally, double* twoematel,
-                          double* reducedpot, double* out, cudaEvent_t avec_ready) {
+                          double* reducedpot, double* out, cudaEvent_t avec_ready, double* host_out = nullptr) {
   SG_CHECK(phi && avector && denmat && invdenmat && tally && reducedpot && out, SINCGPU_EINVAL,
            "null argument");
   SG_CHECK(out != phi, SINCGPU_EINVAL, "out must not alias phi");
   Ctx& c = h->c;
   const double2 *P = (const double2*)phi, *A = (const double2*)avector;
   const double2 tf = make_double2(tre, tim);
+  const size_t bout = sizeof(double2) * (size_t)c.G * c.nspf;
   if (!c.rhs_overlap) {
     SG_TRY(sincgpu_getdenmat_dev(h, avector, denmat, invdenmat, 1e-10));
     SG_TRY(sincgpu_get_tworeducedx_dev(h, avector, avector, tally));
     // the 2-RDM of one A-vector: reducedpot(x,i,k) = conj reducedpot(x,k,i)
-    return orbital_rhs(c, P, (const double2*)tally, (const double2*)denmat, (const double2*)invdenmat, tf, ztdpot,
-                       (double2*)twoematel, (double2*)reducedpot, (double2*)out, true);
+    SG_TRY(orbital_rhs(c, P, (const double2*)tally, (const double2*)denmat, (const double2*)invdenmat, tf, ztdpot,
+                       (double2*)twoematel, (double2*)reducedpot, (double2*)out, true));
+    if (host_out) SG_CUDA(cudaMemcpyAsync(host_out, out, bout, cudaMemcpyDeviceToHost, c.stream));
+    return SINCGPU_OK;
   }
   // The RDMs, the density-matrix inverse, the mix with denmat and the kinetic
   // contraction depend on the A-vector or the orbitals alone: they run on the
@@ -243,7 +249,7 @@ int orbital_rhs_avec_impl(sincgpu_ctx* h, const double* phi, const double* avect
     SG_TRY(ci_denmat(c, A, (double2*)denmat, (double2*)invdenmat, 1e-10));
     SG_TRY(ci_tally(c, A, A, (double2*)tally));
     SG_CUDA(cudaEventRecord(c.ev_ci, c.side));
-    if (avec_ready) SG_CUDA(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
+    if (avec_ready) SG_CUDA(cudaStreamWaitEvent(c.side, c.up_n ? c.ev_up[c.up_n - 1] : c.ev_fork, 0));
     return actreduced_pre(c, P, (const double2*)denmat, ztdpot);
   }();
   c.stream = main_stream;
@@ -257,14 +263,22 @@ int orbital_rhs_avec_impl(sincgpu_ctx* h, const double* phi, const double* avect
   double2 *S = nullptr, *T = nullptr, *part = nullptr;
   int rc = actreduced_temps(c, &S, &T, &part);
   RpApply ap{P, S, (const double2*)invdenmat, tf, T, c.ev_join, false, P, part};
+  const bool deferred = host_out && twoematel;
+  TwoeDefer defer;
   if (rc == SINCGPU_OK)
-    rc = mean_field(c, P, (const double2*)tally, (double2*)twoematel, (double2*)reducedpot, true, c.ev_ci,
-                    twoematel ? c.side : nullptr, &ap);
+    rc = mean_field(c, P, (const double2*)tally, deferred ? nullptr : (double2*)twoematel, (double2*)reducedpot,
+                    true, c.ev_ci, twoematel ? c.side : nullptr, &ap, deferred ? &defer : nullptr);
   SG_CUDA(cudaStreamWaitEvent(c.stream, c.ev_join, 0));
-  const int rc2 = rc == SINCGPU_OK ? actreduced_post(c, P, P, (const double2*)invdenmat,
-                                                     (const double2*)reducedpot, tf, 1, 1, (double2*)out, ap.done,
-                                                     ap.done)
-                                   : rc;
+  int rc2 = rc == SINCGPU_OK ? actreduced_post(c, P, P, (const double2*)invdenmat, (const double2*)reducedpot, tf,
+                                               1, 1, (double2*)out, ap.done, ap.done)
+                             : rc;
+  if (rc2 == SINCGPU_OK && host_out) {
+    // the RHS is final: its copy to the host overlaps the deferred twoematel (issued
+    // first: a copy to pageable memory returns only when it is done)
+    SG_CUDA(cudaEventRecord(c.ev_rhs, c.stream));
+    if (deferred) rc2 = twoe_deferred(c, P, defer, (double2*)twoematel, c.ev_rhs, c.side);
+    SG_CUDA(cudaMemcpyAsync(host_out, out, bout, cudaMemcpyDeviceToHost, c.stream));
+  }
   // twoematel (side stream) joins last
   if (twoematel) SG_CUDA(cudaStreamWaitEvent(c.stream, c.ev_twoe, 0));
   return rc2;
@@ -335,14 +349,46 @@ int sincgpu_orbital_rhs_avec(sincgpu_ctx* h, const double* phi, const double* av
   double* dtal = (double*)p;
   p += pad(b4);
   double* dmat = (double*)p;
-  // the A-vector first: the RDMs start on it while the orbitals are copied
+  // the A-vector first: the RDMs start on it while the orbitals are copied.  With
+  // rhs_upload_groups > 1 the orbitals go up in groups on the copy stream and the
+  // Coulomb pair loop starts on the first group while the others are in flight
   if (c.rhs_overlap) SG_TRY(side_stream(c));
   SG_TRY(up(c, da, avector, ba));
   if (c.rhs_overlap) SG_CUDA(cudaEventRecord(c.ev_avec, c.stream));
-  SG_TRY(up(c, dphi, phi, bphi));
-  SG_TRY(orbital_rhs_avec_impl(h, dphi, da, tre, tim, ztdpot, dden, dinv, dtal, dmat, (double*)c.ws_state.ptr,
-                               dout, c.rhs_overlap ? c.ev_avec : nullptr));
-  SG_TRY(down(c, outspfs, dout, bphi));
+  int ng = 0;
+  if (c.rhs_overlap && c.up_groups > 1 && n > 1) {
+    // group ends ceil(n (g + 1) / groups), repeated ends dropped
+    for (int g = 0; g < c.up_groups; ++g) {
+      const int e = (n * (g + 1) + c.up_groups - 1) / c.up_groups;
+      if (ng == 0 || e > c.up_end[ng - 1]) c.up_end[ng++] = e;
+    }
+  }
+  if (ng > 1) {
+    // the copies wait for everything issued so far (workspace growth included)
+    SG_CUDA(cudaEventRecord(c.ev_entry, c.stream));
+    SG_CUDA(cudaStreamWaitEvent(c.copy, c.ev_entry, 0));
+    const size_t borb = sizeof(double2) * (size_t)c.G;
+    for (int g = 0, b = 0; g < ng; b = c.up_end[g++]) {
+      SG_CUDA(cudaMemcpyAsync((char*)dphi + borb * b, (const char*)phi + borb * b, borb * (c.up_end[g] - b),
+                              cudaMemcpyHostToDevice, c.copy));
+      SG_CUDA(cudaEventRecord(c.ev_up[g], c.copy));
+    }
+    c.up_n = ng;
+  } else {
+    SG_TRY(up(c, dphi, phi, bphi));
+  }
+  const int rc = orbital_rhs_avec_impl(h, dphi, da, tre, tim, ztdpot, dden, dinv, dtal, dmat,
+                                       (double*)c.ws_state.ptr, dout, c.rhs_overlap ? c.ev_avec : nullptr, outspfs);
+  if (c.up_n) {
+    // the last group is joined here too, whatever the evaluation did
+    c.up_n = 0;
+    cudaStreamWaitEvent(c.stream, c.ev_up[ng - 1], 0);
+  }
+  if (rc != SINCGPU_OK) {
+    // no copy may still use the caller's buffers once this returns
+    cudaStreamSynchronize(c.stream);
+    return rc;
+  }
   SG_CUDA(cudaStreamSynchronize(c.stream));
   return SINCGPU_OK;
 }

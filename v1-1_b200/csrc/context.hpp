@@ -207,9 +207,22 @@ struct Ctx {
                           //    contraction on `side`, beside the Coulomb passes and twoematel
   cudaStream_t side = nullptr;  // the second stream of the fused orbital-RHS entry (own, non-blocking;
                                 //   made with its events on first use, side_stream)
-  cudaEvent_t ev_fork = nullptr, ev_ci = nullptr, ev_join = nullptr, ev_coul = nullptr, ev_twoe = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_ci = nullptr, ev_join = nullptr, ev_coul = nullptr, ev_twoe = nullptr,
+              ev_rhs = nullptr;
   cudaEvent_t ev_avec = nullptr;  // host-array entry: the A-vector is on the device
+  // host-array orbital-RHS entry: the orbitals are copied in up to kUpGroups groups on
+  // `copy` (made with its events by side_stream); while that entry runs, up_n > 0 and
+  // orbital index < up_end[g] is on the device once ev_up[g] has fired, and the
+  // Coulomb pair loop waits for each group before the pairs that need it
+  static constexpr int kUpGroups = 8;
+  int up_groups = 4;      // option rhs_upload_groups (1: one copy before the evaluation)
+  cudaStream_t copy = nullptr;
+  cudaEvent_t ev_up[kUpGroups] = {};
+  cudaEvent_t ev_entry = nullptr;
+  int up_n = 0;
+  int up_end[kUpGroups] = {};
   void* orb_state_h = nullptr;    // page-locked copy of the orbital Krylov state (orbprop.cu)
+  size_t orb_state_bytes = 0;
   cudaEvent_t ev_orb_state = nullptr;
   Prof prof;
 
@@ -312,14 +325,29 @@ int reduced_pot_full(Ctx& c, const double2* twoereduced, const double2* tally, d
 
 // capi.cu: twoematel + reducedpot of one orbital set, and that followed by
 // actreduced00 (tally_herm: see reduced_pot)
+// Small page-locked host blocks, recycled across contexts: pinning and unpinning
+// are driver calls that can take milliseconds while other contexts' threads run
+int pinned_get(size_t bytes, void** p);
+void pinned_put(size_t bytes, void* p);
 // creates c.side and the fork/join events on the context's device if not yet made
 int side_stream(Ctx& c);
 // tally_ready: when set, reducedpot waits for it (the tally is written on another
 // stream); side: when set, twoematel runs on that stream after the Coulomb passes
 // and c.ev_twoe marks its end (the caller joins it)
+// defer: when set (and twoematel null), the pair lists the twoematel GEMM needs are
+// kept there and twoe_deferred forms twoematel later from the same reduced potentials
+struct TwoeDefer {
+  std::vector<int> pa, pb;
+  bool herm = false;
+};
 int mean_field(Ctx& c, const double2* phi, const double2* tally, double2* twoematel, double2* reducedpot,
                bool tally_herm, cudaEvent_t tally_ready = nullptr, cudaStream_t side = nullptr,
-               RpApply* apply = nullptr);
+               RpApply* apply = nullptr, TwoeDefer* defer = nullptr);
+// twoematel of a deferred mean-field build on `side` once `after` has fired; c.ev_twoe
+// marks its end (the caller joins it).  The reduced potentials in c.ws_red must
+// still be the build's.
+int twoe_deferred(Ctx& c, const double2* phi, const TwoeDefer& defer, double2* twoematel, cudaEvent_t after,
+                  cudaStream_t side);
 int orbital_rhs(Ctx& c, const double2* phi, const double2* tally, const double2* denmat, const double2* invdenmat,
                 double2 timefac, double ztdpot, double2* twoematel, double2* reducedpot, double2* out,
                 bool tally_herm);

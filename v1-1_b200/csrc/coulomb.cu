@@ -177,13 +177,31 @@ static int coul_run_t(Ctx& c, const double2* src1, const double2* src2, const in
     SG_TRY(timeout_flags(c, &err));
     err += 1;
   }
-  for (int p0 = 0; p0 < npair; p0 += chunk) {
-    const int np = std::min(chunk, npair - p0);
+  // orbitals arriving in groups (host-array entry): the hermitian pair list is
+  // b-major (a <= b), so the pairs of orbitals below e are its first e (e + 1) / 2;
+  // a chunk never crosses a group's end and the first chunk of each group waits for it
+  const bool grouped = !dens && herm && c.up_n > 0;
+  auto pairs_below = [](int e) { return e * (e + 1) / 2; };
+  int g = -1;
+  for (int p0 = 0; p0 < npair;) {
+    int np = std::min(chunk, npair - p0);
+    if (grouped) {
+      int gg = 0;
+      while (gg < c.up_n - 1 && pairs_below(c.up_end[gg]) <= p0) ++gg;
+      if (gg != g) {
+        SG_CUDA(cudaStreamWaitEvent(c.stream, c.ev_up[gg], 0));
+        g = gg;
+      }
+      np = std::max(1, std::min(np, pairs_below(c.up_end[gg]) - p0));
+    }
     ca.pair0 = p0;
     ca.pa = d_pa ? d_pa + p0 : nullptr;
     ca.pb = d_pb ? d_pb + p0 : nullptr;
     SG_TRY(coul_dispatch(c, ca, np, dens, src1, src2, Rpl, full, herm, use_tma ? &zmap : nullptr, err));
+    p0 += np;
   }
+  // every group has been waited for (the last group ends at the last orbital)
+  if (grouped && g != c.up_n - 1) SG_CUDA(cudaStreamWaitEvent(c.stream, c.ev_up[c.up_n - 1], 0));
   return SINCGPU_OK;
 }
 

@@ -425,10 +425,12 @@ int orb_work(Ctx& c, int m, OrbWork& o) {
   return SINCGPU_OK;
 }
 
-// page-locked host copy of OrbKryState and its event, made once per context
+// page-locked host copy of OrbKryState and its event, made once per context (the
+// block comes from the process's recycled page-locked blocks)
 int orb_state_host(Ctx& c, OrbKryState** h) {
   if (!c.orb_state_h) {
-    SG_CUDA(cudaMallocHost(&c.orb_state_h, sizeof(OrbKryState)));
+    SG_TRY(pinned_get(sizeof(OrbKryState), &c.orb_state_h));
+    c.orb_state_bytes = sizeof(OrbKryState);
     SG_CUDA(cudaEventCreateWithFlags(&c.ev_orb_state, cudaEventDisableTiming));
   }
   *h = static_cast<OrbKryState*>(c.orb_state_h);

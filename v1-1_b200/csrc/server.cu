@@ -174,6 +174,17 @@ void sincgpu_server::run(Req& r, Res& out) {
     out.norm = nn;
   }
   if (rc == SINCGPU_OK) {
+    // a tensor-core contraction or a staged Coulomb pass that gave up a bounded
+    // wait has left a wrong result behind: the request fails
+    int flags[2] = {0, 0};
+    rc = sincgpu_kernel_timeouts(ctx, flags);
+    if (rc == SINCGPU_OK && (flags[0] || flags[1])) {
+      set_error("a %s gave up a bounded wait during the request",
+                flags[0] ? "tensor-core contraction" : "staged Coulomb pass");
+      rc = SINCGPU_ETIMEOUT;
+    }
+  }
+  if (rc == SINCGPU_OK) {
     double d[2], nn;
     rc = sincgpu_cmf_dipole_z(ctx, d, &nn);
     out.dipole = nn > 0 ? d[0] / nn : 0.0;
@@ -257,16 +268,34 @@ int sincgpu_server_create(sincgpu_server** out, int device, long long hbm_budget
   SG_CHECK(out && max_active >= 1 && max_active <= 64, SINCGPU_EINVAL, "bad argument");
   SG_CUDA(cudaSetDevice(device));
   // memory cached in the stream-ordered pool by earlier contexts counts as free
-  cudaMemPool_t pool;
+  cudaMemPool_t pool = nullptr;
   if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
     SG_CUDA(cudaDeviceSynchronize());
     cudaMemPoolTrimTo(pool, 0);
+  } else {
+    pool = nullptr;
   }
   size_t fr = 0, tot = 0;
   SG_CUDA(cudaMemGetInfo(&fr, &tot));
   auto s = std::make_unique<sincgpu_server>();
   s->device = device;
   s->budget = hbm_budget > 0 ? std::min<long long>(hbm_budget, (long long)fr) : (long long)(0.85 * fr);
+  // The budget is reserved in the stream-ordered pool up front: the requests'
+  // device allocations are then carved out of memory the pool already holds.
+  // Growing the pool maps new physical memory in a driver call that can take tens
+  // of milliseconds, during which the other requests' host threads stalled.
+  if (pool) {
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    cudaStream_t st = nullptr;
+    void* p = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess) {
+      if (cudaMallocFromPoolAsync(&p, (size_t)s->budget, pool, st) == cudaSuccess) cudaFreeAsync(p, st);
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+    cudaGetLastError();
+  }
   s->max_active = max_active;
   s->t0 = now_ms();
   for (int i = 0; i < max_active; ++i) s->workers.emplace_back([p = s.get()] { p->worker(); });
@@ -407,6 +436,12 @@ int sincgpu_server_destroy(sincgpu_server* s) {
   }
   s->cv_work.notify_all();
   for (auto& t : s->workers) t.join();
+  // the pool gives the reservation back (what live contexts hold stays theirs)
+  cudaMemPool_t pool;
+  if (cudaSetDevice(s->device) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess &&
+      cudaDeviceSynchronize() == cudaSuccess)
+    cudaMemPoolTrimTo(pool, 0);
+  cudaGetLastError();
   delete s;
   return SINCGPU_OK;
 }
