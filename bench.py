@@ -864,6 +864,13 @@ TRAFFIC = {
     ("ke_z", 41, 10): 22090000,
 }
 
+# DRAM bytes per pair of a Coulomb z launch on the 81^3 grid (P = 162), from one
+# ncu capture of an 8-pair launch (coul_chunk=8; the full 40-pair launches hold
+# more than the capture size allows): (774.5 + 245.3) MB / 8 pairs.  Every term
+# (W2 slab read and written, the complex spectrum re-read per pair) grows with the
+# pairs, so a launch's traffic is this times its pairs.
+TRAFFIC_PER_PAIR = {("coul_z", 81, 16): 127475000}
+
 _DGEMM = {}
 
 
@@ -928,10 +935,16 @@ def make_roofline(w, prof, nprof, dev, proj_fft_length=None):
     U = n * (n + 1) // 2
     hbm, hbm_src = measured_peaks()
     launches_per_step = nl / nprof
+    traffic, src = TRAFFIC.get((name, N, n)), None
+    if traffic:
+        src = "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, profiles/"
+    elif TRAFFIC_PER_PAIR.get((name, N, n)):
+        # the average launch: the U pair solves over the launches of one evaluation
+        traffic = TRAFFIC_PER_PAIR[(name, N, n)] * U / launches_per_step
+        src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of an 8-pair launch, scaled to the average "
+               "launch's pairs, profiles/")
     base = {"kernel": name, "launch_ms": per_launch_ms, "launches_per_step": launches_per_step,
-            "traffic": TRAFFIC.get((name, N, n)),
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, profiles/"
-            if TRAFFIC.get((name, N, n)) else None}
+            "traffic": traffic, "traffic_source": src}
     if name in ("rp_gemm", "twoe_gemm", "ke_xy", "ke_z"):
         dgemm = _dgemm_tflops(dev)
         flops = {"rp_gemm": 2.0 * G * 2 * U * n * (n + 1), "twoe_gemm": 2.0 * G * (2 * U) ** 2,

@@ -33,3 +33,19 @@ def test_measured_peaks_source(tmp_path, monkeypatch):
     (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"hbm_gbs": 6531.0}))
     v, src = bench.measured_peaks()
     assert v == 6531.0 and "measured" in src
+
+
+def test_roofline_of_z_pass_81(monkeypatch):
+    """The headline workload's z pass (4 launches per evaluation over 136 pairs):
+    booked against HBM with the algorithmic bytes of the average launch, and the
+    ncu traffic of the 8-pair capture scaled to that launch's 34 pairs."""
+    from sincgpu.inputs import WORKLOADS
+    monkeypatch.setattr(bench, "_dgemm_tflops", lambda dev: 35.0)
+    nprof = 5
+    prof = {"coul_z": (4 * 1.2 * nprof, 4 * nprof), "coul_fwd_y": (1.45 * nprof, 4 * nprof)}
+    r = bench.make_roofline(WORKLOADS["C"], prof, nprof, None, 162)
+    assert r["kernel"] == "coul_z" and r["bound"] == "hbm" and r["launches_per_step"] == 4
+    assert r["algorithmic_bytes_per_launch"] == bench.coulomb_pass_work("coul_z", 81, 162, 136)[0] / 4
+    assert r["traffic"] == 127475000 * 136 / 4
+    assert math.isclose(r["frac"], r["algorithmic_bytes_per_launch"] / 1.2e-3 / 1e9 / r["peak"])
+    assert r["fp64"]["bound"] == "fp64"
