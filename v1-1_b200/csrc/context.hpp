@@ -16,6 +16,11 @@ namespace sincgpu {
 // Device bytes of Coulomb pass intermediates (W1 + W2) per pair chunk when the
 // chunk size is automatic.
 constexpr long long kCoulChunkBudget = 2LL << 30;
+// values in the real kernel-spectrum table d_khr for FFT length P (octant up to 128)
+inline long long khr_len(int P) {
+  const long long H = P / 2 + 1;
+  return P <= 128 ? H * H * H : (long long)P * P * P;
+}
 
 struct Workspace {
   void* ptr = nullptr;
@@ -160,8 +165,9 @@ struct Ctx {
   float2* d_khat32 = nullptr;   // FP32 copies for the precision form, made on demand
   float2* d_roots32 = nullptr;
   double* d_khT = nullptr;      // real part of d_khat as [kx][kz][ky], three-pass Coulomb form (on demand)
-  // real part of d_khat on the octant k <= P/2 of each axis, (P/2+1)^3 values: the
-  // kernel is real and even in each axis, so its spectrum is too (khat(P-k) = khat(k))
+  // real part of d_khat (the kernel is real and even in each axis, so its spectrum
+  // is too: khat(P-k) = khat(k)): for P <= 128 on the octant k <= P/2 of each axis,
+  // (P/2+1)^3 values; for longer lengths the full P^3 table (khr_len(P) values)
   double* d_khr = nullptr;
   float* d_khr32 = nullptr;
   float* d_khT32 = nullptr;

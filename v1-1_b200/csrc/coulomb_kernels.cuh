@@ -48,7 +48,7 @@ struct CoulArgs {
   int npair_total;  // planar output: Re at pair p, Im at npair_total + p
   int fused;        // 0: five passes (W1, W2); 1, 2, 4, 8: three passes (W1T), plane kernel on clusters of that size
   const typename CplxTraits<C>::Real* khT;  // real kernel spectrum [kx][kz][ky] (three-pass form)
-  const typename CplxTraits<C>::Real* khr;  // real kernel spectrum on the octant k <= P/2 ((P/2+1)^3)
+  const typename CplxTraits<C>::Real* khr;  // real kernel spectrum: the octant k <= P/2 ((P/2+1)^3) for P <= 128, else all P^3
 };
 
 template <class C>
@@ -153,8 +153,8 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_z<C>(P1 * P2))
       // the spectrum is real and even in each axis: read it on the octant (a table
       // of (P/2+1)^3 values that stays in L2 while the W2 slab streams through).
       // Measured on the 41^3 grid (P = 81): z pass 0.165 -> 0.148 ms; on the 81^3
-      // grid (P = 162) it was slower (4.8 -> 6.7 ms), so longer lines keep the
-      // complex table
+      // grid (P = 162) it was slower (4.8 -> 6.7 ms), so longer lines read the
+      // real part of the whole table (below)
       using R = typename CplxTraits<C>::Real;
       constexpr int H = P / 2 + 1;
       const int ky = f / P, kx = f - ky * P;
@@ -166,9 +166,16 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_z<C>(P1 * P2))
         b[k2] = CplxTraits<C>::make(b[k2].x * w, b[k2].y * w);
       }
     } else {
-      const C* kh = ca.khat + f;
+      // longer lines: the real spectrum over the whole table, P^3 values with the
+      // indexing of the complex one (P = 162: 34 MB, half the complex table's DRAM
+      // re-reads per pair; z pass 4.80 -> 4.44 ms per evaluation on the 81^3 grid)
+      using R = typename CplxTraits<C>::Real;
+      const R* kh = ca.khr + f;
 #pragma unroll
-      for (int k2 = 0; k2 < P2; ++k2) b[k2] = cmul(b[k2], kh[(long long)(s + P1 * k2) * zs]);
+      for (int k2 = 0; k2 < P2; ++k2) {
+        const R w = kh[(long long)(s + P1 * k2) * zs];
+        b[k2] = CplxTraits<C>::make(b[k2].x * w, b[k2].y * w);
+      }
     }
   }
   dft_out_to_in<P1, P2, true, C, false, false>(b, a, s, l, TL, ex, roots);
@@ -233,11 +240,14 @@ __global__ void __launch_bounds__(P2 * lines_for_z2<P1, P2>(), 2) coul_z2_t(Coul
   RegFFT<P2, 1, false, C>::run(b0, ConstRoots<P, C>{}, P);
   RegFFT<P2, 1, false, C>::run(b1, ConstRoots<P, C>{}, P);
   if (col) {
-    const C* kh = ca.khat + f;
+    // the real spectrum over the whole table, as coul_z_t reads it at these lengths
+    using R = typename CplxTraits<C>::Real;
+    const R* kh = ca.khr + f;
 #pragma unroll
     for (int k2 = 0; k2 < P2; ++k2) {
-      b0[k2] = cmul(b0[k2], kh[(long long)(s + P1 * k2) * zs]);
-      b1[k2] = cmul(b1[k2], kh[(long long)(s + P2 + P1 * k2) * zs]);
+      const R w0 = kh[(long long)(s + P1 * k2) * zs], w1 = kh[(long long)(s + P2 + P1 * k2) * zs];
+      b0[k2] = CplxTraits<C>::make(b0[k2].x * w0, b0[k2].y * w0);
+      b1[k2] = CplxTraits<C>::make(b1[k2].x * w1, b1[k2].y * w1);
     }
   }
   __syncthreads();  // the exchange is read before the inverse writes it
@@ -521,7 +531,8 @@ int coul_launch(Ctx& c, const CoulArgs<C>& ca, int np, bool dens, const double2*
       const int ntf = ceil_div(P * P, TLT), ntiles = ntf * np;
       const int grid = std::min(ntiles, nsm * occ);
       coul_z_tma_t<P1, P2, C><<<grid, S * TLT, dyn, c.stream>>>(ca, *zmap, ntf, ntiles, slab_stride, err);
-    } else if constexpr (P1 == 2 * P2) {
+    } else if constexpr (P1 == 2 * P2 && P > 128) {
+      // (the paired pass reads the whole real spectrum table, built above 128)
       if (c.coul_z2) {
         constexpr int TL2 = lines_for_z2<P1, P2>();
         const size_t dyn = sizeof(C) * ((size_t)P + (size_t)P * TL2);

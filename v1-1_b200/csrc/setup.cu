@@ -477,9 +477,14 @@ __global__ void fft_full_axis_kernel(double2* __restrict__ data, FftPlan plan,
 }
 
 // khr[(fz H + fy) H + fx] = Re khat[(fz P + fy) P + fx] for f <= P/2, H = P/2 + 1
-__global__ void khat_octant_kernel(double* __restrict__ out, const double2* __restrict__ in, int P) {
-  const int H = P / 2 + 1;
+// (P <= 128), or khr[i] = Re khat[i] over the whole table (longer lengths)
+__global__ void khat_real_kernel(double* __restrict__ out, const double2* __restrict__ in, int P) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (P > 128) {
+    if (i < (long long)P * P * P) out[i] = in[i].x;
+    return;
+  }
+  const int H = P / 2 + 1;
   if (i >= (long long)H * H * H) return;
   const int fx = (int)(i % H), fy = (int)((i / H) % H), fz = (int)(i / ((long long)H * H));
   out[i] = in[((long long)fz * P + fy) * P + fx].x;
@@ -528,10 +533,9 @@ int make_khat(Ctx& c) {
   const double inv = 1.0 / ((double)P * (double)P * (double)P);
   fft_full_axis_kernel<<<g1, 128, sm1, c.stream>>>(c.d_khat, c.plan, c.d_roots, 2, c.tx, inv);
   SG_LAUNCHED();
-  const int H = P / 2 + 1;
-  const long long H3 = (long long)H * H * H;
-  SG_TRY(dalloc(c, &c.d_khr, sizeof(double) * H3));
-  khat_octant_kernel<<<ceil_div(H3, 256), 256, 0, c.stream>>>(c.d_khr, c.d_khat, P);
+  const long long nkr = khr_len(P);
+  SG_TRY(dalloc(c, &c.d_khr, sizeof(double) * nkr));
+  khat_real_kernel<<<ceil_div(nkr, 256), 256, 0, c.stream>>>(c.d_khr, c.d_khat, P);
   SG_LAUNCHED();
   SG_CUDA(cudaStreamSynchronize(c.stream));
   return SINCGPU_OK;
@@ -547,10 +551,10 @@ int ensure_fp32_tables(Ctx& c) {
   if (c.d_khat32 && c.d_roots32 && c.d_khr32) return SINCGPU_OK;  // no stream work once built (graph capture)
   const long long P3 = (long long)c.P * c.P * c.P;
   if (!c.d_khr32) {
-    const long long H = c.P / 2 + 1, H3 = H * H * H;
-    SG_TRY(dalloc(c, &c.d_khr32, sizeof(float) * H3));
-    narrow_real_kernel<<<std::min<long long>(ceil_div(H3, 256), 148 * 16), 256, 0, c.stream>>>(c.d_khr32, c.d_khr,
-                                                                                               H3);
+    const long long nkr = khr_len(c.P);
+    SG_TRY(dalloc(c, &c.d_khr32, sizeof(float) * nkr));
+    narrow_real_kernel<<<std::min<long long>(ceil_div(nkr, 256), 148 * 16), 256, 0, c.stream>>>(c.d_khr32, c.d_khr,
+                                                                                               nkr);
     SG_LAUNCHED();
   }
   if (!c.d_khat32) {
