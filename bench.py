@@ -866,10 +866,10 @@ TRAFFIC = {
 
 # DRAM bytes per pair of a Coulomb z launch on the 81^3 grid (P = 162), from one
 # ncu capture of an 8-pair launch (coul_chunk=8; the full 40-pair launches hold
-# more than the capture size allows): (774.5 + 245.3) MB / 8 pairs.  Every term
-# (W2 slab read and written, the complex spectrum re-read per pair) grows with the
-# pairs, so a launch's traffic is this times its pairs.
-TRAFFIC_PER_PAIR = {("coul_z", 81, 16): 127475000}
+# more than the capture size allows): (360.6 + 226.2) MB / 8 pairs.  The W2 slab
+# read and written grows with the pairs (the real spectrum stays in L2), so a
+# launch's traffic is this times its pairs.
+TRAFFIC_PER_PAIR = {("coul_z", 81, 16): 73350000}
 
 _DGEMM = {}
 

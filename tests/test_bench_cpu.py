@@ -46,6 +46,6 @@ def test_roofline_of_z_pass_81(monkeypatch):
     r = bench.make_roofline(WORKLOADS["C"], prof, nprof, None, 162)
     assert r["kernel"] == "coul_z" and r["bound"] == "hbm" and r["launches_per_step"] == 4
     assert r["algorithmic_bytes_per_launch"] == bench.coulomb_pass_work("coul_z", 81, 162, 136)[0] / 4
-    assert r["traffic"] == 127475000 * 136 / 4
+    assert r["traffic"] == 73350000 * 136 / 4
     assert math.isclose(r["frac"], r["algorithmic_bytes_per_launch"] / 1.2e-3 / 1e9 / r["peak"])
     assert r["fp64"]["bound"] == "fp64"
