@@ -110,3 +110,26 @@ def test_paired_z_pass_162(built_lib):
         gpu.set_option("coul_z2", 0)
     finally:
         gpu.close()
+
+
+def test_tma_z_pass_162(built_lib):
+    """The TMA-staged z pass (coul_tma = 1) at length 162, where both it and the
+    plain pass read the real spectrum over the whole table: agreement to 1e-14,
+    the oracle to 1e-11, no timeouts (FP64 and FP32 against FP64)."""
+    from sincgpu import SincProject
+    N, d = 81, 0.3
+    sysm = orc.SincSystem(N, d, [[0, 0, 0]], [1.0])
+    gpu = SincProject(N, d, [[0, 0, 0]], [1.0], 2)
+    try:
+        rng = np.random.default_rng(164)
+        dens = rng.standard_normal((sysm.G, 2)) + 1j * rng.standard_normal((sysm.G, 2))
+        plain = gpu.op_tinv(dens)
+        gpu.set_option("coul_tma", 1)
+        staged = gpu.op_tinv(dens)
+        assert relerr(staged, plain) < 1e-14
+        assert relerr(staged, sysm.op_tinv(dens, workers=8)) < 1e-11
+        gpu.set_option("coulomb_fp32", 1)
+        assert relerr(gpu.op_tinv(dens), plain) < 1e-5
+        assert gpu.kernel_timeouts() == [0, 0]
+    finally:
+        gpu.close()

@@ -324,9 +324,16 @@ __global__ void __launch_bounds__((P1 > P2 ? P1 : P2) * lines_for_ztma<C>(P1 * P
     const bool col = f < zs;
     R kh[P2];
     if (col && s < P1) {
-      const R* khr = reinterpret_cast<const R*>(ca.khat + f);
+      if constexpr (P > 128) {
+        // the real table over all P^3 frequencies (built at these lengths)
+        const R* khr = ca.khr + f;
 #pragma unroll
-      for (int k2 = 0; k2 < P2; ++k2) kh[k2] = khr[2 * (long long)(s + P1 * k2) * zs];
+        for (int k2 = 0; k2 < P2; ++k2) kh[k2] = khr[(long long)(s + P1 * k2) * zs];
+      } else {
+        const R* khr = reinterpret_cast<const R*>(ca.khat + f);
+#pragma unroll
+        for (int k2 = 0; k2 < P2; ++k2) kh[k2] = khr[2 * (long long)(s + P1 * k2) * zs];
+      }
     }
     const bool arrived = tma::mbar_wait(&full[b], (i >> 1) & 1, kLimit);
     if (__syncthreads_or(!arrived)) {
