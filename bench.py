@@ -375,6 +375,7 @@ def measure(w, args, rank, world, local, dist, extras=True, e2e=True, propagatio
                 step()
             prof = proj.profile_read()
             proj.profile(False)
+            proj.set_option("rhs_overlap", 1)
             res["stage_ms_per_step"] = {k: v[0] / 3 for k, v in prof.items()}
         if args.e2e:
             res["e2e"] = run_e2e(proj, w, phi_h, a_h, args, stream, world, dist)

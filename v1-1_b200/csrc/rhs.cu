@@ -486,7 +486,10 @@ int actreduced_post(Ctx& c, const double2* phi, const double2* proj, const doubl
       dots_reduce_kernel<<<n * n, 128, 0, c.stream>>>(part, ceil_div(G, DCH), n * n, D);
       SG_LAUNCHED();
     } else {
-      SG_TRY(launch_dots(c, proj, T, D, part));
+      // above 10 orbitals no GEMM epilogue forms 64-point partials, so the dots
+      // take 256-point blocks (a quarter of the partials; 81^3, 16 orbitals: the
+      // 64-point form took 0.27 ms)
+      SG_TRY(launch_dots(c, proj, T, D, part, n > 10));
     }
     project_kernel<<<bt, tile_for(n), smem_mix(n), c.stream>>>(T, proj, D, n, G, out);
     SG_LAUNCHED();
