@@ -58,8 +58,9 @@ def parse():
                     help="instead of the benchmark: STEPS field-free CMF steps of the workload in the FP64 form, "
                          "the precision form and the precision form with FP64 final mean fields; per-quantity "
                          "errors against the FP64 form")
-    ap.add_argument("--only", choices=["served", "batched"], default=None,
-                    help="run only the served or the batched form and print its object")
+    ap.add_argument("--only", choices=["served", "batched", "propagation"], default=None,
+                    help="run only the served or the batched form, or the CMF steps of the workload, and print "
+                         "its object")
     ap.add_argument("--stages", action="store_true",
                     help="with --no-extras: also time each stage on one stream (per-stage CUDA events)")
     ap.add_argument("--e2e", action="store_true",
@@ -438,6 +439,8 @@ def main():
                              for f in ("plain_fp64", "mixed_fp32_coulomb")}
             pl, mx = out["served"]["plain_fp64"], out["served"]["mixed_fp32_coulomb"]
             out["served"]["mixed_vs_plain_steps_per_s"] = mx["steps_per_s"] / max(pl["steps_per_s"], 1e-30)
+        elif args.only == "propagation":
+            out["propagation"] = propagation_only(WORKLOADS[args.config], local, args.steps)
         else:
             out["batched"] = batched_form(torch, local, torch.cuda.current_stream(), args.batched_count)
         if rank == 0:
@@ -657,6 +660,23 @@ def cmf_rate(proj, w, phi, avec, torch, local, nsteps=6):
             float(np.mean([r["orb_iters"] for r in res])), "sigma_products_per_step":
             float(np.mean([r["avec_iters"] for r in res])), "per_step_ms": ms,
             "timing": "host wall clock around each step (each step ends in a device synchronisation)"}
+
+
+def propagation_only(w, local, nsteps):
+    """CMF steps of workload `w` alone (rank 0's seeded inputs; `nsteps` timed steps
+    after one warm-up step), for profiling the propagation."""
+    import torch
+    from sincgpu import SincProject
+    from sincgpu.inputs import ci_size, seeded_avector, seeded_orbitals
+    phi_h = seeded_orbitals(w.numpoints, w.spacing, w.nspf, seed=1)
+    a_h = seeded_avector(ci_size(w.numelec, w.nspf), seed=2)
+    proj = SincProject(w.numpoints, w.spacing, w.centershift, w.nuccharges, w.nspf, device=local)
+    try:
+        phi = torch.from_numpy(np.ascontiguousarray(phi_h.T)).cuda(local)
+        avec = torch.from_numpy(np.ascontiguousarray(a_h)).cuda(local)
+        return cmf_rate(proj, w, phi, avec, torch, local, nsteps=nsteps)
+    finally:
+        proj.close()
 
 
 def batched_form(torch, local, stream, count):

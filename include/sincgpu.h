@@ -98,7 +98,10 @@ int sincgpu_fft_length(sincgpu_ctx* ctx);
  * host-array orbital-RHS entry copies the orbitals up in that many groups on
  * a copy stream, and the Coulomb pair loop starts on the pairs of the first
  * group while the others are in flight; 1: one copy before the evaluation;
- * bitwise the same). */
+ * bitwise the same); "kry_cluster" (1, default: the A-vector Krylov's
+ * Gram-Schmidt step on vectors longer than 4096 reals runs on a cluster of 8
+ * CTAs with the dot products summed through distributed shared memory; 0: one
+ * CTA; results agree to rounding). */
 int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
 /* Current value of an option of sincgpu_set_option (SINCGPU_EINVAL for an unknown name). */
 int sincgpu_get_option(sincgpu_ctx* ctx, const char* name, long long* value);

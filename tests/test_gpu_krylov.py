@@ -72,15 +72,18 @@ def test_expoavecprop_with_field(ci):
     assert np.abs(w - complexify(w_ref)).max() < 1e-11
 
 
-@pytest.mark.parametrize("nspf", [8, 9, 11], ids=["2x1568", "4x2592", "loop6050"])
-def test_expoavecprop_long_vectors(built_lib, nspf):
+@pytest.mark.parametrize("nspf,cluster", [(8, 1), (9, 1), (11, 1), (11, 0)],
+                         ids=["2x1568", "4x2592", "cluster6050", "loop6050"])
+def test_expoavecprop_long_vectors(built_lib, nspf, cluster):
     """4 electrons in 8, 9 and 11 orbitals: 784, 1296 and 3025 determinants, so the
     real-ified Krylov vectors have 1568 and 2592 entries (the register-resident
-    Gram-Schmidt kernel with two and four values per thread) and 6050 (the
-    looping kernel beyond 4096), against the oracle's DGEXPV."""
+    Gram-Schmidt kernel with two and four values per thread) and 6050 (beyond 4096:
+    the cluster kernel, one value per thread, or with kry_cluster = 0 the looping
+    single-CTA kernel), against the oracle's DGEXPV."""
     from sincgpu import SincProject, WalkTables
     sysm = orc.SincSystem(15, 0.5, [[0, 0, 0]], [2.0])
     gpu = SincProject(15, 0.5, [[0, 0, 0]], [2.0], nspf)
+    gpu.set_option("kry_cluster", cluster)
     try:
         gpu.ci_attach(WalkTables(4, nspf, 0))
         ow = CIWalks(4, nspf, 0)
@@ -103,5 +106,38 @@ def test_expoavecprop_long_vectors(built_lib, nspf):
         assert nstep == info["nstep"]
         assert g == pytest.approx(g_ref, rel=1e-12)
         assert np.abs(w - complexify(w_ref)).max() < 1e-11
+    finally:
+        gpu.close()
+
+
+@pytest.mark.parametrize("nspf", [13, 14], ids=["cluster2x12168", "cluster4x16562"])
+def test_expoavecprop_cluster_vs_one_cta(built_lib, nspf):
+    """4 electrons in 13 and 14 orbitals (6084 and 8281 determinants: 12168 and 16562
+    reals, the cluster Gram-Schmidt kernel with two and four values per thread)
+    against the single-CTA kernel (kry_cluster = 0, checked against the oracle
+    above): the same Krylov steps, the propagated vector to 1e-12 (the two differ
+    in the shape of each dot product's sum only).  The Hamiltonian is the
+    library's own on seeded orbitals."""
+    from sincgpu import SincProject, WalkTables
+    sysm = orc.SincSystem(13, 0.5, [[0, 0, 0]], [2.0])
+    gpu = SincProject(13, 0.5, [[0, 0, 0]], [2.0], nspf)
+    try:
+        wt = WalkTables(4, nspf, 0)
+        gpu.ci_attach(wt)
+        phi = orc.seeded_orbitals(sysm, nspf, seed=35)
+        mat, _ = gpu.call_twoe_matel00(phi)
+        pot, ke, z = gpu.onebody_matel(phi)
+        gpu.assemble_sparsemats(mat, pot, ke, z)
+        rng = np.random.default_rng(36)
+        a = rng.standard_normal(wt.numconfig) + 1j * rng.standard_normal(wt.numconfig)
+        a /= np.linalg.norm(a)
+        dt, m = 0.05, 12
+        out = {}
+        for cl in (0, 1):
+            gpu.set_option("kry_cluster", cl)
+            out[cl] = gpu.expoavecprop(a, 1.0, krylovdim=m, tol=1e-9, anorm=dt, stepguess=1.0, timefac=-1j * dt)
+        assert out[0][2] == out[1][2]
+        assert out[1][1] == pytest.approx(out[0][1], rel=1e-12)
+        assert np.abs(out[1][0] - out[0][0]).max() < 1e-12
     finally:
         gpu.close()

@@ -386,7 +386,7 @@ int sincgpu_get_option(sincgpu_ctx* h, const char* name, long long* value) {
   } opts[] = {{"coul_chunk", c.coul_chunk},       {"coulomb_fp32", c.coul_fp32}, {"contract_tf32", c.contract_tf32},
               {"coul_tma", c.coul_tma},           {"twoe_tile", c.twoe_tile},    {"orth_fused", c.orth_fused},
               {"rhs_overlap", c.rhs_overlap},     {"coul_fused", c.coul_fused},  {"coul_z2", c.coul_z2},
-              {"cmf_fp64_last", c.cmf.fp64_last ? 1 : 0}, {"rhs_upload_groups", c.up_groups}, {"ke_tf32", c.ke_tf32}, {"tc_kc", c.tc_kc}, {"tc_pipe", c.tc_pipe}, {"twoe_symdiag", c.twoe_symdiag}, {"twoe_dmma", c.twoe_dmma}, {"rp_dmma", c.rp_dmma}};
+              {"cmf_fp64_last", c.cmf.fp64_last ? 1 : 0}, {"rhs_upload_groups", c.up_groups}, {"kry_cluster", c.kry_cluster}, {"ke_tf32", c.ke_tf32}, {"tc_kc", c.tc_kc}, {"tc_pipe", c.tc_pipe}, {"twoe_symdiag", c.twoe_symdiag}, {"twoe_dmma", c.twoe_dmma}, {"rp_dmma", c.rp_dmma}};
   for (const auto& o : opts)
     if (!strcmp(name, o.n)) {
       *value = o.v;
@@ -413,6 +413,11 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
   if (!strcmp(name, "rhs_overlap")) {
     SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "rhs_overlap must be 0 or 1");
     h->c.rhs_overlap = (int)value;
+    return SINCGPU_OK;
+  }
+  if (!strcmp(name, "kry_cluster")) {
+    SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "kry_cluster must be 0 or 1");
+    h->c.kry_cluster = (int)value;
     return SINCGPU_OK;
   }
   if (!strcmp(name, "rhs_upload_groups")) {

@@ -209,6 +209,7 @@ struct Ctx {
   int twoe_symdiag = 0;   // 1: multi-tile twoematel computes its diagonal tiles' lower blocks only
   int twoe_tile = 0;      // twoematel tile edge 16R: 0 = least padding, 2..9 = that R
   int orth_fused = 1;     // 1: an orbital Arnoldi step's orthogonalisation in one cooperative launch
+  int kry_cluster = 1;    // 1: A-vector Gram-Schmidt beyond 4096 reals on a cluster of CTAs (0: one CTA)
   int rhs_overlap = 1;    // 1: the fused orbital-RHS entry runs its CI part and the mix + kinetic
                           //    contraction on `side`, beside the Coulomb passes and twoematel
   cudaStream_t side = nullptr;  // the second stream of the fused orbital-RHS entry (own, non-blocking;

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <vector>
+#include <cooperative_groups.h>
 #include "context.hpp"
 
 namespace sincgpu {
@@ -148,6 +149,106 @@ __global__ void __launch_bounds__(kKryThreads) kry_mgs_reg_kernel(double* __rest
     const long long k = threadIdx.x + (long long)e * blockDim.x;
     if (k < n) p[k] = brk ? x[e] : x[e] * inv;
   }
+}
+
+// kry_mgs_reg_kernel over a thread-block cluster of kMgsCluster CTAs, for vectors
+// longer than one CTA holds in registers (n > 4 kKryThreads): CTA r of the cluster
+// keeps the slice [r S, r S + S) of p in registers (S = ceil(n / kMgsCluster),
+// E elements per thread), each projection's dot is summed per CTA (block_sum) and
+// then over the cluster's partials in rank order through distributed shared memory
+// (so every CTA gets the same value, and the sums have a fixed shape), one cluster
+// barrier per sum (the partials alternate between two slots).  The modified
+// Gram-Schmidt order of expokit.f90:2327-2346 is kept; only the shape of each sum
+// differs from the single-CTA kernels.  A single CTA took 0.37 ms per call at
+// 28800 reals (14400 determinants): its loads of V sat behind one SM's bandwidth.
+constexpr int kMgsCluster = 8;
+
+template <int E>
+__global__ void __launch_bounds__(kKryThreads) kry_mgs_cluster_kernel(double* __restrict__ V, long long n, int j,
+                                                                      double* __restrict__ Hm, int mh,
+                                                                      double break_tol, KryState* st) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  __shared__ double red[33];
+  __shared__ double cpart[2];
+  if (st->mbrk) return;  // the same value in every CTA of the cluster
+  const long long S = (n + kMgsCluster - 1) / kMgsCluster;
+  const long long lo = (long long)cl.block_rank() * S, hi = min(n, lo + S);
+  double* p = V + (long long)(j + 1) * n;
+  int nsum = 0;
+  // sum over the cluster: this CTA's block sum, then the kMgsCluster partials in rank order
+  auto cluster_sum = [&](double v) {
+    const double b = block_sum(v, red);
+    const int slot = nsum++ & 1;
+    if (threadIdx.x == 0) cpart[slot] = b;
+    cl.sync();
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < kMgsCluster; ++q) t += *cl.map_shared_rank(&cpart[slot], q);
+    return t;
+  };
+  double x[E], a[E], an[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const long long k = lo + threadIdx.x + (long long)e * blockDim.x;
+    x[e] = k < hi ? p[k] : 0.0;
+    a[e] = k < hi ? V[k] : 0.0;
+    an[e] = 0.0;
+  }
+  for (int i = 0; i <= j; ++i) {
+    if (i < j) {
+      const double* vn = V + (long long)(i + 1) * n;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const long long k = lo + threadIdx.x + (long long)e * blockDim.x;
+        an[e] = k < hi ? vn[k] : 0.0;
+      }
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) s += a[e] * x[e];  // zero outside the slice
+    const double hij = cluster_sum(s);
+#pragma unroll
+    for (int e = 0; e < E; ++e) x[e] -= hij * a[e];
+    if (cl.block_rank() == 0 && threadIdx.x == 0) Hm[(long long)j * mh + i] = hij;
+#pragma unroll
+    for (int e = 0; e < E; ++e) a[e] = an[e];
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int e = 0; e < E; ++e) s += x[e] * x[e];
+  const double h = sqrt(cluster_sum(s));
+  const bool brk = h <= break_tol;
+  if (cl.block_rank() == 0 && threadIdx.x == 0) {
+    if (brk) st->mbrk = j + 1;
+    else Hm[(long long)j * mh + j + 1] = h;
+  }
+  const double inv = 1.0 / h;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const long long k = lo + threadIdx.x + (long long)e * blockDim.x;
+    if (k < hi) p[k] = brk ? x[e] : x[e] * inv;
+  }
+  cl.sync();  // no CTA leaves while another may still read its partials
+}
+
+template <int E>
+static int launch_mgs_cluster(Ctx& c, double* V, long long n, int j, double* Hm, int mh, double break_tol,
+                              KryState* st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(kMgsCluster, 1, 1);
+  cfg.blockDim = dim3(kKryThreads, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = c.stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = kMgsCluster;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  SG_CUDA(cudaLaunchKernelEx(&cfg, kry_mgs_cluster_kernel<E>, V, n, j, Hm, mh, break_tol, st));
+  return SINCGPU_OK;
 }
 
 __global__ void __launch_bounds__(kKryThreads) kry_avnorm_kernel(const double* __restrict__ p, long long n,
@@ -430,6 +531,16 @@ int expv_avector(Ctx& c, const double2* v, double2* w, double t, double2 timefac
         kry_mgs_reg_kernel<2><<<1, kKryThreads, 0, c.stream>>>(V, n, j, Hm, mh, break_tol, dst);
       else if (n <= 4 * kKryThreads)
         kry_mgs_reg_kernel<4><<<1, kKryThreads, 0, c.stream>>>(V, n, j, Hm, mh, break_tol, dst);
+      else if (!c.kry_cluster)
+        kry_mgs_kernel<<<1, kKryThreads, 0, c.stream>>>(V, n, j, Hm, mh, break_tol, dst);
+      else if (n <= 1LL * kMgsCluster * kKryThreads)
+        SG_TRY(launch_mgs_cluster<1>(c, V, n, j, Hm, mh, break_tol, dst));
+      else if (n <= 2LL * kMgsCluster * kKryThreads)
+        SG_TRY(launch_mgs_cluster<2>(c, V, n, j, Hm, mh, break_tol, dst));
+      else if (n <= 4LL * kMgsCluster * kKryThreads)
+        SG_TRY(launch_mgs_cluster<4>(c, V, n, j, Hm, mh, break_tol, dst));
+      else if (n <= 8LL * kMgsCluster * kKryThreads)
+        SG_TRY(launch_mgs_cluster<8>(c, V, n, j, Hm, mh, break_tol, dst));
       else
         kry_mgs_kernel<<<1, kKryThreads, 0, c.stream>>>(V, n, j, Hm, mh, break_tol, dst);
       SG_LAUNCHED();
