@@ -101,7 +101,10 @@ int sincgpu_fft_length(sincgpu_ctx* ctx);
  * bitwise the same); "kry_cluster" (1, default: the A-vector Krylov's
  * Gram-Schmidt step on vectors longer than 4096 reals runs on a cluster of 8
  * CTAs with the dot products summed through distributed shared memory; 0: one
- * CTA; results agree to rounding). */
+ * CTA; results agree to rounding); "orb_blendq" (1, default: an orbital Krylov
+ * call with two mean-field slots folds their reduced potentials and density
+ * matrices into one blended potential once, and each Jacobian product reads
+ * that; 0: each product reads both slots; results agree to rounding). */
 int sincgpu_set_option(sincgpu_ctx* ctx, const char* name, long long value);
 /* Current value of an option of sincgpu_set_option (SINCGPU_EINVAL for an unknown name). */
 int sincgpu_get_option(sincgpu_ctx* ctx, const char* name, long long* value);

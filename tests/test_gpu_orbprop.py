@@ -119,6 +119,29 @@ def test_orthogonalisation_fused_is_bitwise(system):
     assert outs[0][1] == outs[1][1] and outs[0][2] == outs[1][2]
 
 
+def test_blended_potential_matches_per_slot(system):
+    """The Jacobian reading one blended reduced potential Q and matrix M, formed
+    once per call (orb_blendq = 1, the default), against the per-slot blend
+    (orb_blendq = 0): the same Krylov steps and saved state, the propagated
+    orbitals to 1e-12 (the same algebra, summed in another order)."""
+    import torch
+    sysm, gpu, phi, slots, dslots = system
+    outs = []
+    try:
+        for bq in (1, 0):
+            gpu.set_option("orb_blendq", bq)
+            gpu.orbprop_setup(5, 12, 1.2, 0.002)
+            d = dev(torch, phi)
+            iters = [gpu.expospfprop_dev(d, dslots[0], dslots[1], t, t + 0.08, t, t + 0.08, True, expotol=1e-9)
+                     for t in (0.0, 0.08)]
+            outs.append((host(d), iters, gpu.orbprop_state()))
+    finally:
+        gpu.set_option("orb_blendq", 1)
+    assert outs[0][1] == outs[1][1]
+    assert outs[0][2]["thisexpodim"] == outs[1][2]["thisexpodim"]
+    assert np.abs(outs[0][0] - outs[1][0]).max() < 1e-12 * np.abs(outs[1][0]).max()
+
+
 def test_expospfprop_rejects_bad_setup(system):
     from sincgpu import SincGpuError
     gpu = system[1]

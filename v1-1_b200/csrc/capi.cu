@@ -108,7 +108,7 @@ int dupload(Ctx& c, void** dst, const void* src, size_t bytes) {
 
 void Ctx::bind_workspaces() {
   for (Workspace* w : {&ws_fft, &ws_pairs, &ws_gemm, &ws_twoe, &ws_rhs, &ws_io, &ws_red, &ws_conv, &ws_state, &ws_ci,
-                       &ws_ci2, &ws_kry, &ws_orb, &ws_tcerr, &ws_tc, &cmf.ws})
+                       &ws_ci2, &ws_kry, &ws_orb, &ws_tcerr, &ws_tc, &ws_bq, &cmf.ws})
     w->owner = &stream;
 }
 
@@ -136,6 +136,7 @@ Ctx::~Ctx() {
   ws_orb.release();
   ws_tcerr.release();
   ws_tc.release();
+  ws_bq.release();
   cmf.ws.release();
   for (IntCache& ic : icache) dfree(*this, ic.dev);
   if (rhs_exec) cudaGraphExecDestroy(rhs_exec);
@@ -386,7 +387,7 @@ int sincgpu_get_option(sincgpu_ctx* h, const char* name, long long* value) {
   } opts[] = {{"coul_chunk", c.coul_chunk},       {"coulomb_fp32", c.coul_fp32}, {"contract_tf32", c.contract_tf32},
               {"coul_tma", c.coul_tma},           {"twoe_tile", c.twoe_tile},    {"orth_fused", c.orth_fused},
               {"rhs_overlap", c.rhs_overlap},     {"coul_fused", c.coul_fused},  {"coul_z2", c.coul_z2},
-              {"cmf_fp64_last", c.cmf.fp64_last ? 1 : 0}, {"rhs_upload_groups", c.up_groups}, {"kry_cluster", c.kry_cluster}, {"ke_tf32", c.ke_tf32}, {"tc_kc", c.tc_kc}, {"tc_pipe", c.tc_pipe}, {"twoe_symdiag", c.twoe_symdiag}, {"twoe_dmma", c.twoe_dmma}, {"rp_dmma", c.rp_dmma}};
+              {"cmf_fp64_last", c.cmf.fp64_last ? 1 : 0}, {"rhs_upload_groups", c.up_groups}, {"kry_cluster", c.kry_cluster}, {"orb_blendq", c.orb_blendq}, {"ke_tf32", c.ke_tf32}, {"tc_kc", c.tc_kc}, {"tc_pipe", c.tc_pipe}, {"twoe_symdiag", c.twoe_symdiag}, {"twoe_dmma", c.twoe_dmma}, {"rp_dmma", c.rp_dmma}};
   for (const auto& o : opts)
     if (!strcmp(name, o.n)) {
       *value = o.v;
@@ -413,6 +414,11 @@ int sincgpu_set_option(sincgpu_ctx* h, const char* name, long long value) {
   if (!strcmp(name, "rhs_overlap")) {
     SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "rhs_overlap must be 0 or 1");
     h->c.rhs_overlap = (int)value;
+    return SINCGPU_OK;
+  }
+  if (!strcmp(name, "orb_blendq")) {
+    SG_CHECK(value == 0 || value == 1, SINCGPU_EINVAL, "orb_blendq must be 0 or 1");
+    h->c.orb_blendq = (int)value;
     return SINCGPU_OK;
   }
   if (!strcmp(name, "kry_cluster")) {

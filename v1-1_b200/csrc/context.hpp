@@ -187,6 +187,7 @@ struct Ctx {
   Workspace ws_orb;         // orbital Krylov basis and Jacobian state
   Workspace ws_tcerr;       // timeout flags: [0] tensor-core contractions, [1] TMA z pass
   Workspace ws_tc;          // pre-split tf32 operand tiles of the bulk-copy tensor-core GEMM
+  Workspace ws_bq;          // blended reduced potential Q and matrix M of an orbital Krylov call
   OrbPropState orb;
   CIState ci;
   CmfState cmf;
@@ -210,6 +211,7 @@ struct Ctx {
   int twoe_tile = 0;      // twoematel tile edge 16R: 0 = least padding, 2..9 = that R
   int orth_fused = 1;     // 1: an orbital Arnoldi step's orthogonalisation in one cooperative launch
   int kry_cluster = 1;    // 1: A-vector Gram-Schmidt beyond 4096 reals on a cluster of CTAs (0: one CTA)
+  int orb_blendq = 1;     // 1: the orbital Jacobian reads one blended reduced potential (0: both slots')
   int rhs_overlap = 1;    // 1: the fused orbital-RHS entry runs its CI part and the mix + kinetic
                           //    contraction on `side`, beside the Coulomb passes and twoematel
   cudaStream_t side = nullptr;  // the second stream of the fused orbital-RHS entry (own, non-blocking;
@@ -413,6 +415,17 @@ bool actreduced_blend2_fits(int n);  // its shared memory (n <= 20)
 int actreduced_blend2(Ctx& c, const double2* x, const double2* const* denmat, const double2* const* invdenmat,
                       const double2* const* redpot, const double* facs, double2 timefac, double zfield,
                       double2* out);
+// The same blend with the slots folded once per orbital Krylov call: the
+// propagation's blend factors and mean fields are fixed during the call, so
+// A = timefac (Y M + sum_k x_k Q(:, k, :)) with M = sum_s f_s D_s I_s and
+// Q(x, k, i) = sum_s f_s sum_j V_s(x, k, j) I_s(j, i); blendq_prepare forms Q and M
+// in c.ws_bq (one pass over both slots' reducedpot), after which each product
+// reads one reduced potential instead of two.  Same algebra as actreduced_blend2,
+// rounding differs.
+bool actreduced_blendq_fits(int n);
+int blendq_prepare(Ctx& c, const double2* const* denmat, const double2* const* invdenmat,
+                   const double2* const* redpot, const double* facs);
+int actreduced_blendq(Ctx& c, const double2* x, double2 timefac, double zfield, double2* out);
 int actreduced_mix_ke(Ctx& c, const double2* denmat);
 // D(j,i) = <P_j|T_i> over the grid (split-K, deterministic); part holds
 // orbital_dots_scratch(c) * nspf^2 partial sums

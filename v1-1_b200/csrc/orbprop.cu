@@ -377,6 +377,7 @@ struct OrbWork {
   OrbKryState* st;
   int* ns;
   unsigned* gbar;  // lv_arnoldi_orth_kernel's grid barrier (count, generation)
+  bool blendq = false;  // the unprojected blends read the prepared Q and M (blendq_prepare)
 };
 
 size_t al256(size_t b) { return (b + 255) / 256 * 256; }
@@ -439,8 +440,10 @@ int orb_state_host(Ctx& c, OrbKryState** h) {
 
 // blended unprojected (proj == nullptr) or projected actreduced00 over the slots
 int blend_actreduced(Ctx& c, const double2* x, const double2* proj, const MeanFieldSlot* slots,
-                     const double* facs, int nslot, double2 timefac, double ez, double2* tmp, double2* out) {
+                     const double* facs, int nslot, double2 timefac, double ez, double2* tmp, double2* out,
+                     bool blendq = false) {
   const long long len = c.G * c.nspf;
+  if (blendq && nslot == 2 && !proj) return actreduced_blendq(c, x, timefac, ez, out);
   if (nslot == 2 && !proj && actreduced_blend2_fits(c.nspf)) {
     const double2* den[2] = {slots[0].denmat, slots[1].denmat};
     const double2* inv[2] = {slots[0].invdenmat, slots[1].invdenmat};
@@ -463,7 +466,7 @@ int blend_actreduced(Ctx& c, const double2* x, const double2* proj, const MeanFi
 
 int jacoperate(Ctx& c, OrbWork& o, const double2* x, const MeanFieldSlot* slots, const double* facs, int nslot,
                double2 timefac, double ez, double2* y) {
-  SG_TRY(blend_actreduced(c, x, nullptr, slots, facs, nslot, timefac, ez, o.tmp, o.T));
+  SG_TRY(blend_actreduced(c, x, nullptr, slots, facs, nslot, timefac, ez, o.tmp, o.T, o.blendq));
   SG_TRY(orbital_dots(c, o.jv, o.T, o.M1, o.dpart));   // <jacvect|T>
   SG_TRY(orbital_dots(c, x, o.jvo, o.M2, o.dpart));    // <x|jacvectout>
   return jac_combine(c, o.T, o.jv, o.M1, o.M2, x, o.D2, y);
@@ -531,7 +534,16 @@ int expospfprop(Ctx& c, double2* phi, const MeanFieldSlot* slots, double tin, do
   // jacinit: jacvect = phi, jacvectout = blend (gridtime, 1-gridtime) of the
   // unprojected actreduced at midtime; D2 = <jacvect|jacvectout>
   SG_CUDA(cudaMemcpyAsync(o.jv, phi, sizeof(double2) * nv, cudaMemcpyDeviceToDevice, c.stream));
-  SG_TRY(blend_actreduced(c, o.jv, nullptr, slots, facs, nslot, timefac, ez, o.tmp, o.jvo));
+  // with two slots the blend factors and mean fields are fixed for this call: fold
+  // the slots' reduced potentials and density matrices once
+  if (nslot == 2 && c.orb_blendq && actreduced_blendq_fits(n)) {
+    const double2* den[2] = {slots[0].denmat, slots[1].denmat};
+    const double2* inv[2] = {slots[0].invdenmat, slots[1].invdenmat};
+    const double2* rp[2] = {slots[0].reducedpot, slots[1].reducedpot};
+    SG_TRY(blendq_prepare(c, den, inv, rp, facs));
+    o.blendq = true;
+  }
+  SG_TRY(blend_actreduced(c, o.jv, nullptr, slots, facs, nslot, timefac, ez, o.tmp, o.jvo, o.blendq));
   SG_TRY(orbital_dots(c, o.jv, o.jvo, o.D2, o.dpart));
   // u = spf_linear_derivs(midtime, phi)
   SG_TRY(blend_actreduced(c, o.jv, o.jv, slots, facs, nslot, timefac, ez, o.tmp, o.u));

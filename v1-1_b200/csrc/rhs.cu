@@ -138,6 +138,85 @@ __global__ void __launch_bounds__(TXO * kMaxOrbRhs) blend2_kernel(
   if (ok) out[(long long)ii * G + x] = res;
 }
 
+// M(j,i) = sum_s f_s sum_l D_s(j,l) I_s(l,i): one thread per element (n*n <= 1024)
+__global__ void blendq_m_kernel(const double2* __restrict__ D0, const double2* __restrict__ D1,
+                                const double2* __restrict__ I0, const double2* __restrict__ I1, double f0, double f1,
+                                int n, double2* __restrict__ M) {
+  const int e = threadIdx.x;
+  if (e >= n * n) return;
+  const int j = e % n, i = e / n;
+  double2 a0 = make_double2(0.0, 0.0), a1 = make_double2(0.0, 0.0);
+  for (int l = 0; l < n; ++l) {
+    cfma(a0, D0[j + n * l], I0[l + n * i]);
+    cfma(a1, D1[j + n * l], I1[l + n * i]);
+  }
+  M[e] = make_double2(fma(f1, a1.x, f0 * a0.x), fma(f1, a1.y, f0 * a0.y));
+}
+
+// Q(x,k,i) = sum_s sum_j V_s(x,k,j) (f_s I_s(j,i)), reducedpot layout (x fastest,
+// then k, then i): per tile of TXO points the rows V_s(., k, j) of one k are staged
+// (warp j loads row j of both slots), then warp i forms Q(., k, i)
+__global__ void __launch_bounds__(TXO * kMaxOrbRhs) blendq_build_kernel(
+    const double2* __restrict__ V0, const double2* __restrict__ V1, const double2* __restrict__ I0,
+    const double2* __restrict__ I1, double f0, double f1, int n, long long G, double2* __restrict__ Q) {
+  extern __shared__ double2 rsm[];
+  double2* sJ = rsm;             // [2][n*n]
+  double2* sV = sJ + 2 * n * n;  // [2][n][TXO]
+  const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
+  for (int e = tid; e < n * n; e += TXO * blockDim.y) {
+    const double2 a = I0[e], b = I1[e];
+    sJ[e] = make_double2(f0 * a.x, f0 * a.y);
+    sJ[n * n + e] = make_double2(f1 * b.x, f1 * b.y);
+  }
+  const long long x = blockIdx.x * (long long)TXO + lx;
+  const bool ok = x < G;
+  for (int k = 0; k < n; ++k) {
+    __syncthreads();  // the previous k's rows are used (and sJ is staged)
+    for (int j = ty; j < n; j += blockDim.y) {
+      const long long o = (long long)(k + n * j) * G + x;
+      sV[j * TXO + lx] = ok ? V0[o] : make_double2(0.0, 0.0);
+      sV[(n + j) * TXO + lx] = ok ? V1[o] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    if (ok) {
+      for (int i = ty; i < n; i += blockDim.y) {
+        double2 a = make_double2(0.0, 0.0);
+        for (int j = 0; j < n; ++j) cfma(a, sV[j * TXO + lx], sJ[j + n * i]);
+        for (int j = 0; j < n; ++j) cfma(a, sV[(n + j) * TXO + lx], sJ[n * n + j + n * i]);
+        Q[(long long)(k + n * i) * G + x] = a;
+      }
+    }
+  }
+}
+
+// out(x,i) = timefac (sum_j Y(x,j) M(j,i) + sum_k Q(x,k,i) xin(x,k))
+__global__ void __launch_bounds__(TXO * kMaxOrbRhs) blendq_apply_kernel(
+    const double2* __restrict__ xin, const double2* __restrict__ Y, const double2* __restrict__ Q,
+    const double2* __restrict__ M, double2 timefac, int n, long long G, double2* __restrict__ out) {
+  extern __shared__ double2 rsm[];
+  double2* sM = rsm;            // n*n
+  double2* sx = sM + n * n;     // n x TXO
+  double2* sy = sx + n * TXO;   // n x TXO
+  const int lx = threadIdx.x, ty = threadIdx.y, tid = ty * TXO + lx;
+  for (int e = tid; e < n * n; e += TXO * blockDim.y) sM[e] = M[e];
+  const long long x = blockIdx.x * (long long)TXO + lx;
+  const bool ok = x < G;
+  for (int j = ty; j < n; j += blockDim.y) {
+    sx[j * TXO + lx] = ok ? xin[(long long)j * G + x] : make_double2(0.0, 0.0);
+    sy[j * TXO + lx] = ok ? Y[(long long)j * G + x] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  if (!ok) return;
+  for (int i = ty; i < n; i += blockDim.y) {
+    double2 a = make_double2(0.0, 0.0);
+    for (int j = 0; j < n; ++j) cfma(a, sy[j * TXO + lx], sM[j + n * i]);
+    const double2* Qi = Q + (long long)n * i * G + x;
+#pragma unroll 4
+    for (int k = 0; k < n; ++k) cfma(a, Qi[(long long)k * G], sx[k * TXO + lx]);
+    out[(long long)i * G + x] = cmul(timefac, a);
+  }
+}
+
 // partial[blk][j + n*i] = sum_{x in blk} conj(P_j(x)) T_i(x); block blk covers
 // DCH consecutive points, warp w the rows j = w, w + (warps per block), ...
 // BL points per block: 64 (DCH) where the reducedpot GEMM's epilogue forms the same
@@ -293,7 +372,8 @@ int rhs_attrs() {
     for (const void* k : {(const void*)mix_kernel, (const void*)redpot_kernel, (const void*)dots_kernel<DCH>,
                           (const void*)dots_kernel<4 * DCH>,
                           (const void*)project_kernel, (const void*)jac_combine_kernel,
-                          (const void*)blend2_kernel}) {
+                          (const void*)blend2_kernel, (const void*)blendq_build_kernel,
+                          (const void*)blendq_apply_kernel}) {
       const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmemMax);
       if (e != cudaSuccess) return e;
     }
@@ -451,6 +531,45 @@ int actreduced_blend2(Ctx& c, const double2* x, const double2* const* denmat, co
   blend2_kernel<<<ceil_div(c.G, TXO), tile_for(n), sm, c.stream>>>(x, t.Y, redpot[0], redpot[1], denmat[0],
                                                                     denmat[1], invdenmat[0], invdenmat[1], timefac,
                                                                     facs[0], facs[1], n, c.G, out);
+  SG_LAUNCHED();
+  return SINCGPU_OK;
+}
+
+size_t smem_bq_build(int n) { return sizeof(double2) * (2 * (size_t)n * n + 2 * (size_t)n * TXO); }
+size_t smem_bq_apply(int n) { return sizeof(double2) * ((size_t)n * n + 2 * (size_t)n * TXO); }
+
+bool actreduced_blendq_fits(int n) {
+  return n <= kMaxOrbRhs && smem_bq_build(n) <= (size_t)kRhsSmemMax && smem_bq_apply(n) <= (size_t)kRhsSmemMax;
+}
+
+int blendq_prepare(Ctx& c, const double2* const* denmat, const double2* const* invdenmat,
+                   const double2* const* redpot, const double* facs) {
+  const int n = c.nspf;
+  SG_CHECK(actreduced_blendq_fits(n), SINCGPU_ERANGE, "blended reduced potential: at most %d orbitals", kMaxOrbRhs);
+  SG_TRY(rhs_attrs());
+  const size_t nq = (size_t)c.G * n * n;
+  SG_TRY(c.ws_bq.ensure(sizeof(double2) * (nq + (size_t)n * n)));
+  double2* Q = (double2*)c.ws_bq.ptr;
+  ProfScope ps(c, ST_RHS_REDPOT);
+  blendq_m_kernel<<<1, 1024, 0, c.stream>>>(denmat[0], denmat[1], invdenmat[0], invdenmat[1], facs[0], facs[1], n,
+                                            Q + nq);
+  SG_LAUNCHED();
+  blendq_build_kernel<<<ceil_div(c.G, TXO), tile_for(n), smem_bq_build(n), c.stream>>>(
+      redpot[0], redpot[1], invdenmat[0], invdenmat[1], facs[0], facs[1], n, c.G, Q);
+  SG_LAUNCHED();
+  return SINCGPU_OK;
+}
+
+int actreduced_blendq(Ctx& c, const double2* x, double2 timefac, double zfield, double2* out) {
+  RhsTemps t;
+  SG_TRY(rhs_temps(c, t));
+  const int n = c.nspf;
+  const double2* Q = (const double2*)c.ws_bq.ptr;
+  SG_CHECK(Q, SINCGPU_ESTATE, "blended reduced potential not prepared");
+  SG_TRY(mult_ke(c, x, t.Y, n, true, zfield));
+  ProfScope ps(c, ST_RHS_REDPOT);
+  blendq_apply_kernel<<<ceil_div(c.G, TXO), tile_for(n), smem_bq_apply(n), c.stream>>>(
+      x, t.Y, Q, Q + (size_t)c.G * n * n, timefac, n, c.G, out);
   SG_LAUNCHED();
   return SINCGPU_OK;
 }

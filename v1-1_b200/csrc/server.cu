@@ -77,7 +77,7 @@ long long estimate_bytes(const Req& r) {
   long long P = 2 * r.N;  // upper bound of the padded length
   long long b = 0;
   b += 16 * G * n * (2 + 25);                 // orbitals (2 slots) + Krylov basis and Jacobian state
-  b += 16 * G * n * n * 3;                    // reducedpot (2 slots) + scratch
+  b += 16 * G * n * n * 4;                    // reducedpot (2 slots), their blend for the Jacobian, scratch
   b += 8 * 2 * npair * G;                     // planar reduced potentials
   b += std::min(sincgpu::kCoulChunkBudget, npair * 16 * (r.N * r.N * P + r.N * P * P));  // Coulomb W1/W2 chunk
   b += 16 * P * P * P;                        // kernel spectrum
